@@ -1,0 +1,170 @@
+"""ORACLE -- test infrastructure only.
+
+ctypes wrapper around ``oracle/_build/liboracle.so`` (the CPU FP64
+restatement in ``oracle.cpp``).  Imported only by ``tests/``,
+``__graft_entry__.smoke()`` (as the checker) and ``bench.py``'s CPU-baseline
+leg.  The product package never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+TABLE = os.path.join(os.path.dirname(HERE), "openmolcas_b200", "rys", "rys_table.bin")
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        d, i, vp = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
+        L.or_load_rys.argtypes = [C.c_char_p]
+        L.or_rys_rw.argtypes = [C.c_int, C.c_int, d, d, d]
+        L.or_sph_matrix.argtypes = [C.c_int, d]
+        L.or_basis_create.restype = vp
+        L.or_basis_create.argtypes = [C.c_int, d, i, i, i, i, d, d]
+        L.or_basis_free.argtypes = [vp]
+        L.or_nbf.argtypes = [vp]
+        L.or_eri_quartet.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, d]
+        L.or_schwarz.argtypes = [vp, d]
+        L.or_eri_full.argtypes = [vp, C.c_double, d]
+        L.or_rs_count.restype = C.c_int64
+        L.or_rs_count.argtypes = [vp]
+        L.or_rs_list.argtypes = [vp, i, i, i]
+        L.or_eri_diag.argtypes = [vp, d]
+        L.or_cholesky.argtypes = [vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, i, i, i, d, i]
+        L.or_cho_jk.argtypes = [vp, d, C.c_int, d, C.c_int, d, d]
+        L.or_grad.argtypes = [vp, d, C.c_double, d]
+        rc = L.or_load_rys(TABLE.encode())
+        if rc != 0:
+            raise RuntimeError(f"oracle: cannot load Rys table ({rc})")
+        _lib = L
+    return _lib
+
+
+def _p(a, t=C.c_double):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def rys_rw(n, T):
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    x = np.empty((T.size, n))
+    w = np.empty((T.size, n))
+    lib().or_rys_rw(n, T.size, _p(T), _p(x), _p(w))
+    return x, w
+
+
+def sph_matrix(l):
+    nc = (l + 1) * (l + 2) // 2
+    out = np.empty(nc * (2 * l + 1))
+    lib().or_sph_matrix(l, _p(out))
+    return out.reshape(2 * l + 1, nc).T
+
+
+class Oracle:
+    """One basis on the CPU oracle."""
+
+    def __init__(self, mol):
+        self.mol = mol
+        xyz, l, npr, nco, at, ex, cf = mol.flat()
+        self._keep = (xyz, l, npr, nco, at, ex, cf)
+        self.h = lib().or_basis_create(len(l), _p(xyz), _p(l, C.c_int), _p(npr, C.c_int), _p(nco, C.c_int),
+                                       _p(at, C.c_int), _p(ex), _p(cf))
+        self.nbf = lib().or_nbf(self.h)
+        self.nshell = len(l)
+
+    def __del__(self):
+        try:
+            lib().or_basis_free(self.h)
+        except Exception:
+            pass
+
+    def quartet_shape(self, i, j, k, l):
+        sh = self.mol.shells
+        nijkl = sh[i].ncontr * sh[j].ncontr * sh[k].ncontr * sh[l].ncontr
+        return (sh[l].ncomp, sh[k].ncomp, sh[j].ncomp, sh[i].ncomp, nijkl)
+
+    def eri_quartet(self, i, j, k, l):
+        """(ij|kl) block in reference layout, returned as flat Fortran-order array."""
+        shp = self.quartet_shape(i, j, k, l)
+        out = np.empty(int(np.prod(shp)))
+        lib().or_eri_quartet(self.h, i, j, k, l, _p(out))
+        return out
+
+    def schwarz(self):
+        t = np.empty(self.nshell * self.nshell)
+        lib().or_schwarz(self.h, _p(t))
+        return t.reshape(self.nshell, self.nshell)
+
+    def eri_full(self, cutint=0.0):
+        n = self.nbf
+        out = np.empty(n ** 4)
+        lib().or_eri_full(self.h, cutint, _p(out))
+        return out.reshape(n, n, n, n)
+
+    def rs_list(self):
+        n = lib().or_rs_count(self.h)
+        a = np.empty(n, np.int32)
+        b = np.empty(n, np.int32)
+        sp = np.empty(n, np.int32)
+        lib().or_rs_list(self.h, _p(a, C.c_int), _p(b, C.c_int), _p(sp, C.c_int))
+        return a, b, sp
+
+    def eri_diag(self):
+        n = lib().or_rs_count(self.h)
+        d = np.empty(n)
+        lib().or_eri_diag(self.h, _p(d))
+        return d
+
+    def cholesky(self, thrcom=1e-6, span=1e-2, minqual=50, maxqual=100, maxvec=None):
+        nrs = lib().or_rs_count(self.h)
+        if maxvec is None:
+            maxvec = min(nrs, 20 * self.nbf)
+        L = np.zeros(nrs * maxvec)
+        piv = np.zeros(maxvec, np.int32)
+        pas = np.zeros(maxvec, np.int32)
+        M = C.c_int(0)
+        npass = C.c_int(0)
+        rc = lib().or_cholesky(self.h, thrcom, span, minqual, maxqual, maxvec, C.byref(M), _p(piv, C.c_int),
+                               _p(pas, C.c_int), _p(L), C.byref(npass))
+        if rc != 0:
+            raise RuntimeError(f"oracle cholesky failed rc={rc}")
+        m = M.value
+        return dict(L=L[: nrs * m].reshape(m, nrs).T.copy(), piv=piv[:m].copy(), pass_of=pas[:m].copy(),
+                    M=m, npass=npass.value)
+
+    def cho_jk(self, L, Cm):
+        nrs, M = L.shape
+        Lf = np.asfortranarray(L)
+        Cf = np.asfortranarray(Cm, dtype=np.float64)
+        n = self.nbf
+        J = np.empty(n * n)
+        K = np.empty(n * n)
+        lib().or_cho_jk(self.h, _p(Lf), M, _p(Cf), Cf.shape[1], _p(J), _p(K))
+        return J.reshape(n, n, order="F"), K.reshape(n, n, order="F")
+
+    def grad(self, D, cutint=0.0):
+        Dc = np.ascontiguousarray(D, dtype=np.float64)
+        g = np.empty(3 * self.mol.natom)
+        lib().or_grad(self.h, _p(Dc), cutint, _p(g))
+        return g.reshape(-1, 3)
+
+
+def energy_from_full(eri, D):
+    """E = 1/2 tr(DJ) - 1/4 tr(DK) from a full ERI tensor."""
+    J = np.einsum("abcd,cd->ab", eri, D)
+    K = np.einsum("acbd,cd->ab", eri, D)
+    return 0.5 * np.sum(D * J) - 0.25 * np.sum(D * K), J, K
