@@ -1,0 +1,255 @@
+// C ABI of libmolgpu: handle, basis, Schwarz bounds, batched ERIs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "../../include/molgpu.h"
+#include "mg_internal.h"
+
+struct mg_handle {
+  mg::Handle h;
+};
+
+namespace mg {
+size_t eri_smem_plan(int nab, int ncd, int max_accd, int max_nef, int max_tmp, int& NP);
+int eri_launch_class(Handle* h, const EriItem* d_items, int nitems, int nab, int ncd, int NP, size_t smem, double* out,
+                     cudaStream_t st);
+
+// Accumulator budget (doubles) of one work item: nc * nef <= this.
+static const int kAccBudget = 12288;
+
+struct EriClass {
+  int nab, ncd, begin, count, NP;
+  size_t smem;
+};
+
+// Split quartets into work items grouped by (la+lb, lc+ld) class.
+int build_eri_items(Handle* h, const int32_t* q4, int64_t nq, const int64_t* offsets, std::vector<EriItem>& items,
+                    std::vector<EriClass>& classes) {
+  std::map<int, std::vector<EriItem>> byc;
+  std::map<int, int> mx_acc, mx_nef, mx_tmp;
+  const int ns = h->sh.size();
+  for (int64_t t = 0; t < nq; ++t) {
+    const int i = q4[4 * t], j = q4[4 * t + 1], k = q4[4 * t + 2], l = q4[4 * t + 3];
+    if (i < 0 || j < 0 || k < 0 || l < 0 || i >= ns || j >= ns || k >= ns || l >= ns || i < j || k < l) {
+      h->err = "mg_eri_quartets: shell indices out of range or non-canonical pair (need i>=j, k>=l)";
+      return MG_ERR_ARG;
+    }
+    const DPair& P = h->pairs[pair_id(i, j)];
+    const DPair& Q = h->pairs[pair_id(k, l)];
+    const int nab = P.la + P.lb, ncd = Q.la + Q.lb;
+    const int nef = P.ne * Q.ne;
+    const int nijkl = P.nci * P.ncj * Q.nci * Q.ncj;
+    const int chunk = std::max(1, kAccBudget / nef);
+    const int key = nab * 8 + ncd;
+    for (int c0 = 0; c0 < nijkl; c0 += chunk) {
+      EriItem it;
+      it.p = pair_id(i, j);
+      it.q = pair_id(k, l);
+      it.c0 = c0;
+      it.c1 = std::min(nijkl, c0 + chunk);
+      it.out_off = offsets[t];
+      byc[key].push_back(it);
+      const int nc = it.c1 - it.c0;
+      mx_acc[key] = std::max(mx_acc[key], nc * nef);
+      mx_nef[key] = std::max(mx_nef[key], nef);
+      mx_tmp[key] = std::max(mx_tmp[key], nc * P.nsa * P.nsb * Q.ne);
+    }
+  }
+  items.clear();
+  classes.clear();
+  for (auto& kv : byc) {
+    EriClass c;
+    c.nab = kv.first / 8;
+    c.ncd = kv.first % 8;
+    c.begin = items.size();
+    c.count = kv.second.size();
+    c.smem = eri_smem_plan(c.nab, c.ncd, mx_acc[kv.first], mx_nef[kv.first], mx_tmp[kv.first], c.NP);
+    if (c.NP < 1) {
+      h->err = "mg_eri_quartets: class does not fit in shared memory";
+      return MG_ERR_ARG;
+    }
+    items.insert(items.end(), kv.second.begin(), kv.second.end());
+    classes.push_back(c);
+  }
+  return 0;
+}
+
+int run_eri_items(Handle* h, const std::vector<EriItem>& items, const std::vector<EriClass>& classes, double* d_out,
+                  cudaStream_t st) {
+  if (items.empty()) return 0;
+  EriItem* d_items = (EriItem*)ws_get(h, sizeof(EriItem) * items.size(), st);
+  if (!d_items) { h->err = "workspace allocation failed"; return MG_ERR_MEMORY; }
+  cudaMemcpyAsync(d_items, items.data(), sizeof(EriItem) * items.size(), cudaMemcpyHostToDevice, st);
+  for (const EriClass& c : classes) {
+    // grid.x limit is 2^31-1: split very long classes anyway for safety
+    for (int b = 0; b < c.count; b += (1 << 30)) {
+      int n = std::min(c.count - b, 1 << 30);
+      if (eri_launch_class(h, d_items + c.begin + b, n, c.nab, c.ncd, c.NP, c.smem, d_out, st)) {
+        h->err = std::string("ERI kernel launch failed: ") + cudaGetErrorString(cudaGetLastError());
+        return MG_ERR_CUDA;
+      }
+    }
+  }
+  return 0;
+}
+
+}  // namespace mg
+
+using namespace mg;
+
+extern "C" {
+
+int mg_create(const char* rys_table_path, int device, mg_handle** out) {
+  if (!out || !rys_table_path) return MG_ERR_ARG;
+  *out = nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) return MG_ERR_CUDA;
+  mg_handle* H = new mg_handle;
+  H->h.device = device;
+  int rc = load_rys_table(&H->h, rys_table_path);
+  if (rc) {
+    delete H;
+    return MG_ERR_ARG;
+  }
+  *out = H;
+  return 0;
+}
+
+static void free_basis(Handle* h) {
+  cudaFree(h->d_pairs); cudaFree(h->d_prim); cudaFree(h->d_coef); cudaFree(h->d_hrr); cudaFree(h->d_tmax);
+  h->d_pairs = nullptr; h->d_prim = nullptr; h->d_coef = nullptr; h->d_hrr = nullptr; h->d_tmax = nullptr;
+  h->tmax.clear();
+}
+
+int mg_destroy(mg_handle* H) {
+  if (!H) return 0;
+  Handle* h = &H->h;
+  cudaSetDevice(h->device);
+  free_basis(h);
+  cudaFree(h->d_rys);
+  if (h->ws.ptr) cudaFree(h->ws.ptr);
+  delete H;
+  return 0;
+}
+
+const char* mg_last_error(mg_handle* H) { return H ? H->h.err.c_str() : "null handle"; }
+
+int mg_set_basis(mg_handle* H, int nshell, const double* xyz, const int* l, const int* nprim, const int* ncontr,
+                 const int* atom, const double* exps, const double* coefs) {
+  if (!H || nshell < 1) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  cudaSetDevice(h->device);
+  free_basis(h);
+  h->sh.clear();
+  size_t pe = 0, pc = 0;
+  int off = 0, natom = 0, lmax = 0;
+  for (int s = 0; s < nshell; ++s) {
+    if (l[s] < 0 || l[s] > MG_MAX_L || nprim[s] < 1 || ncontr[s] < 1 || atom[s] < 0) {
+      h->err = "mg_set_basis: unsupported shell (need 0<=l<=3, nprim>=1, ncontr>=1)";
+      return MG_ERR_ARG;
+    }
+    ShellH sh;
+    for (int x = 0; x < 3; ++x) sh.A[x] = xyz[3 * s + x];
+    sh.l = l[s]; sh.np = nprim[s]; sh.nc = ncontr[s]; sh.atom = atom[s];
+    sh.ncomp = ncomp(sh.l);
+    sh.e.assign(exps + pe, exps + pe + sh.np);
+    sh.c.assign(coefs + pc, coefs + pc + (size_t)sh.np * sh.nc);
+    pe += sh.np;
+    pc += (size_t)sh.np * sh.nc;
+    sh.off = off;
+    off += sh.nc * sh.ncomp;
+    natom = std::max(natom, sh.atom + 1);
+    lmax = std::max(lmax, sh.l);
+    h->sh.push_back(sh);
+  }
+  h->nbf = off;
+  h->natom = natom;
+  h->lmax = lmax;
+  build_sph(h, MG_MAX_L + 1);
+  if (setup_pairs(h)) return MG_ERR_MEMORY;
+  return 0;
+}
+
+int mg_nbf(mg_handle* H) { return H ? H->h.nbf : -1; }
+int mg_natom(mg_handle* H) { return H ? H->h.natom : -1; }
+
+int mg_eri_quartets_size(mg_handle* H, const int32_t* q4, int64_t nq, int64_t* offsets) {
+  if (!H || (!q4 && nq) || !offsets) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  const int ns = h->sh.size();
+  int64_t o = 0;
+  for (int64_t t = 0; t < nq; ++t) {
+    offsets[t] = o;
+    const int s[4] = {q4[4 * t], q4[4 * t + 1], q4[4 * t + 2], q4[4 * t + 3]};
+    int64_t n = 1;
+    for (int x = 0; x < 4; ++x) {
+      if (s[x] < 0 || s[x] >= ns) { h->err = "shell index out of range"; return MG_ERR_ARG; }
+      n *= (int64_t)h->sh[s[x]].nc * h->sh[s[x]].ncomp;
+    }
+    o += n;
+  }
+  offsets[nq] = o;
+  return 0;
+}
+
+int mg_eri_quartets(mg_handle* H, const int32_t* q4, int64_t nq, const int64_t* offsets, double* d_out, void* stream) {
+  if (!H || (!q4 && nq) || !offsets || (!d_out && nq)) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  cudaSetDevice(h->device);
+  std::vector<EriItem> items;
+  std::vector<EriClass> classes;
+  int rc = build_eri_items(h, q4, nq, offsets, items, classes);
+  if (rc) return rc;
+  return run_eri_items(h, items, classes, d_out, (cudaStream_t)stream);
+}
+
+int mg_schwarz(mg_handle* H, double* tmax) {
+  if (!H || !tmax) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  cudaSetDevice(h->device);
+  const int ns = h->sh.size();
+  if (h->tmax.empty()) {
+    std::vector<int32_t> q;
+    for (int i = 0; i < ns; ++i)
+      for (int j = 0; j <= i; ++j) { q.push_back(i); q.push_back(j); q.push_back(i); q.push_back(j); }
+    const int64_t nq = q.size() / 4;
+    std::vector<int64_t> off(nq + 1);
+    mg_eri_quartets_size(H, q.data(), nq, off.data());
+    double* d_out = nullptr;
+    if (cudaMalloc(&d_out, sizeof(double) * std::max<int64_t>(off[nq], 1)) != cudaSuccess) {
+      h->err = "cudaMalloc Schwarz";
+      return MG_ERR_MEMORY;
+    }
+    int rc = mg_eri_quartets(H, q.data(), nq, off.data(), d_out, nullptr);
+    std::vector<double> blk(off[nq]);
+    if (!rc) rc = cudaMemcpy(blk.data(), d_out, sizeof(double) * off[nq], cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : MG_ERR_CUDA;
+    cudaFree(d_out);
+    if (rc) return rc;
+    h->tmax.assign((size_t)ns * ns, 0.0);
+    for (int64_t t = 0; t < nq; ++t) {
+      const int i = q[4 * t], j = q[4 * t + 1];
+      const ShellH &A = h->sh[i], &B = h->sh[j];
+      const int nij = A.nc * B.nc, nijkl = nij * nij, nsa = A.ncomp, nsb = B.ncomp;
+      double mx = 0;
+      for (int sb = 0; sb < nsb; ++sb)
+        for (int sa = 0; sa < nsa; ++sa)
+          for (int kb = 0; kb < B.nc; ++kb)
+            for (int ka = 0; ka < A.nc; ++ka) {
+              const int ij = ka + A.nc * kb;
+              const int64_t ijkl = ij + (int64_t)nij * ij;
+              const int64_t sab = sa + nsa * sb;
+              const double v = blk[off[t] + ijkl + nijkl * (sab + (int64_t)nsa * nsb * sab)];
+              mx = std::max(mx, std::fabs(v));
+            }
+      h->tmax[(size_t)i * ns + j] = h->tmax[(size_t)j * ns + i] = std::sqrt(mx);
+    }
+  }
+  std::copy(h->tmax.begin(), h->tmax.end(), tmax);
+  return 0;
+}
+
+}  // extern "C"

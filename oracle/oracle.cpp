@@ -362,7 +362,9 @@ void rys2d(int nr, int imax, int jmax, double zeta, double eta, const double* P,
 }
 
 // (AB|CD) contracted, spherical, reference layout [ijkl][a][b][c][d]
-void eri_quartet(const Basis& bs, int iS, int jS, int kS, int lS, double* out) {
+// absmode: use |contraction coefficients| and |[e0|f0]| -- the cancellation-free
+// magnitude S of each integral, used to scale the FP64 parity bar.
+void eri_quartet(const Basis& bs, int iS, int jS, int kS, int lS, double* out, bool absmode = false) {
   const Shell &a = bs.sh[iS], &b = bs.sh[jS], &c = bs.sh[kS], &d = bs.sh[lS];
   int la = a.l, lb = b.l, lc = c.l, ld = d.l;
   int nijkl = a.nc * b.nc * c.nc * d.nc;
@@ -413,15 +415,17 @@ void eri_quartet(const Basis& bs, int iS, int jS, int kS, int lS, double* out) {
           const Cart &E = elist[ie], &F = flist[jf];
           double s = 0;
           for (int r = 0; r < nr; ++r) s += G.at(0, r, E.x, F.x) * G.at(1, r, E.y, F.y) * G.at(2, r, E.z, F.z);
-          ef[ie + (size_t)ne * jf] = s * Fact;
+          ef[ie + (size_t)ne * jf] = absmode ? std::fabs(s * Fact) : s * Fact;
         }
       for (int l4 = 0; l4 < d.nc; ++l4)
         for (int k3 = 0; k3 < c.nc; ++k3) {
           double ccd = c.c[ic + c.np * k3] * d.c[id + d.np * l4];
+          if (absmode) ccd = std::fabs(ccd);
           if (ccd == 0.0) continue;
           for (int j2 = 0; j2 < b.nc; ++j2)
             for (int i1 = 0; i1 < a.nc; ++i1) {
               double cf = a.c[ia + a.np * i1] * b.c[ib + b.np * j2] * ccd;
+              if (absmode) cf = std::fabs(cf);
               if (cf == 0.0) continue;
               int ijkl = i1 + a.nc * (j2 + b.nc * (k3 + c.nc * l4));
               double* ac = &acc[(size_t)ijkl * ne * nf];
@@ -438,13 +442,13 @@ void eri_quartet(const Basis& bs, int iS, int jS, int kS, int lS, double* out) {
     for (int jf = 0; jf < nf; ++jf)
       for (int sab = 0; sab < na * nb; ++sab) {
         double s = 0;
-        for (int ie = 0; ie < ne; ++ie) s += Hab[ie + (size_t)ne * sab] * ac[ie + (size_t)ne * jf];
+        for (int ie = 0; ie < ne; ++ie) s += (absmode ? std::fabs(Hab[ie + (size_t)ne * sab]) : Hab[ie + (size_t)ne * sab]) * ac[ie + (size_t)ne * jf];
         tmpab[sab + (size_t)na * nb * jf] = s;
       }
     for (int scd = 0; scd < nc * nd; ++scd)
       for (int sab = 0; sab < na * nb; ++sab) {
         double s = 0;
-        for (int jf = 0; jf < nf; ++jf) s += Hcd[jf + (size_t)nf * scd] * tmpab[sab + (size_t)na * nb * jf];
+        for (int jf = 0; jf < nf; ++jf) s += (absmode ? std::fabs(Hcd[jf + (size_t)nf * scd]) : Hcd[jf + (size_t)nf * scd]) * tmpab[sab + (size_t)na * nb * jf];
         out[ijkl + (size_t)nijkl * (sab + (size_t)na * nb * scd)] = s;
       }
   }
@@ -984,6 +988,11 @@ int or_nbf(void* h) { return ((Handle*)h)->bs.nbf; }
 
 int or_eri_quartet(void* h, int i, int j, int k, int l, double* out) {
   eri_quartet(((Handle*)h)->bs, i, j, k, l, out);
+  return 0;
+}
+// cancellation-free magnitude of every integral of the block (same layout)
+int or_eri_quartet_abs(void* h, int i, int j, int k, int l, double* out) {
+  eri_quartet(((Handle*)h)->bs, i, j, k, l, out, true);
   return 0;
 }
 

@@ -39,6 +39,7 @@ def lib():
         L.or_basis_free.argtypes = [vp]
         L.or_nbf.argtypes = [vp]
         L.or_eri_quartet.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, d]
+        L.or_eri_quartet_abs.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, d]
         L.or_schwarz.argtypes = [vp, d]
         L.or_eri_full.argtypes = [vp, C.c_double, d]
         L.or_rs_count.restype = C.c_int64
@@ -104,6 +105,14 @@ class Oracle:
         lib().or_eri_quartet(self.h, i, j, k, l, _p(out))
         return out
 
+    def eri_quartet_abs(self, i, j, k, l):
+        """Cancellation-free magnitude S of each integral (|coefficients|,
+        |primitive [e0|f0]|, |HRR|): the scale of FP64 rounding error."""
+        shp = self.quartet_shape(i, j, k, l)
+        out = np.empty(int(np.prod(shp)))
+        lib().or_eri_quartet_abs(self.h, i, j, k, l, _p(out))
+        return out
+
     def schwarz(self):
         t = np.empty(self.nshell * self.nshell)
         lib().or_schwarz(self.h, _p(t))
@@ -161,6 +170,17 @@ class Oracle:
         g = np.empty(3 * self.mol.natom)
         lib().or_grad(self.h, _p(Dc), cutint, _p(g))
         return g.reshape(-1, 3)
+
+
+# FP64 parity bar of one integral: 1e-11 absolute plus a rounding term scaled
+# by the integral's cancellation-free magnitude S (random-sign general
+# contractions over exponents spanning 4 decades cancel by up to ~1e7).
+ERI_ABS_TOL = 1e-11
+ERI_REL_S = 1e-13
+
+
+def eri_tolerance(S):
+    return ERI_ABS_TOL + ERI_REL_S * S
 
 
 def energy_from_full(eri, D):
