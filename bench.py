@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""Benchmark of the two-electron hot path on B200.
+
+One step = the Coulomb/exchange build from Cholesky vectors for the
+1500-basis-function cluster (120 atoms, rank-200 density, ThrCom 1e-6) plus
+the two-electron nuclear gradient of the 460-basis-function cluster (20
+atoms 4s3p2d, rank-40 density, Schwarz 1e-12).  The J/K leg runs in the
+mixed-precision path; the same step in the plain FP64 GPU path is timed
+beside it, with the energy difference between the two.  Inputs are seeded
+synthetic molecules (no data files).  Set-up (integrals, Cholesky
+decomposition) is outside the timed region.
+
+Prints one JSON line (rank 0).  --impl reference times the CPU restatement
+of the reference path (oracle port) on a bounded sample instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+JK_CFG = "c3"
+GRAD_CFG = "c4"
+THRCOM = 1e-6
+CUTINT = 1e-12
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (200 ms period)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.lines = []
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.p = None
+
+    def _read(self):
+        for ln in self.p.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------- FP64 peak
+FP64_PEAK_SRC = r"""
+extern "C" __global__ void dfma_peak(double* out, int iters) {
+  double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9;
+  double a4 = a0 + 4e-9, a5 = a0 + 5e-9, a6 = a0 + 6e-9, a7 = a0 + 7e-9;
+  const double b = 0.999999, c = 1e-7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      a0 = fma(a0, b, c); a1 = fma(a1, b, c); a2 = fma(a2, b, c); a3 = fma(a3, b, c);
+      a4 = fma(a4, b, c); a5 = fma(a5, b, c); a6 = fma(a6, b, c); a7 = fma(a7, b, c);
+    }
+  }
+  out[blockIdx.x * blockDim.x + threadIdx.x] = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+}
+"""
+
+
+def measure_fp64_peak(torch):
+    """DFMA throughput (TFLOP/s, FMA = 2 flops) of a register-only kernel on all SMs."""
+    from torch.utils.cpp_extension import load_inline  # noqa: F401  (not used: compile via nvcc below)
+    import ctypes
+    import tempfile
+    d = tempfile.mkdtemp()
+    src = os.path.join(d, "k.cu")
+    so = os.path.join(d, "k.so")
+    with open(src, "w") as f:
+        f.write(FP64_PEAK_SRC + r"""
+#include <cuda_runtime.h>
+extern "C" float run_peak(int blocks, int threads, int iters) {
+  double* out; cudaMalloc(&out, sizeof(double) * blocks * threads);
+  dfma_peak<<<blocks, threads>>>(out, 16);
+  cudaEvent_t e0, e1; cudaEventCreate(&e0); cudaEventCreate(&e1);
+  cudaEventRecord(e0); dfma_peak<<<blocks, threads>>>(out, iters); cudaEventRecord(e1);
+  cudaEventSynchronize(e1); float ms; cudaEventElapsedTime(&ms, e0, e1); cudaFree(out); return ms;
+}
+""")
+    r = subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-Xcompiler", "-fPIC", "-shared",
+                        "-o", so, src], capture_output=True, text=True)
+    if r.returncode != 0:
+        return None
+    lib = ctypes.CDLL(so)
+    lib.run_peak.restype = ctypes.c_float
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    blocks, threads, iters = sms * 8, 256, 4000
+    ms = lib.run_peak(blocks, threads, iters)
+    flops = 2.0 * 8 * 16 * iters * blocks * threads
+    return flops / (ms * 1e-3) / 1e12
+
+
+# --------------------------------------------------------------- workload
+def setup(torch, device):
+    from openmolcas_b200 import basis as B
+    from openmolcas_b200.molgpu import MolGpu
+    t0 = time.time()
+    m3 = B.config_molecule(JK_CFG)
+    g3 = MolGpu(m3, device)
+    info = g3.cho_drv(thrcom=THRCOM)
+    t_cho = time.time() - t0
+    C3 = torch.from_numpy(B.density_factor(m3.nbf, B.CONFIGS[JK_CFG]["rank"], B.CONFIGS[JK_CFG]["seed"]))
+    m4 = B.config_molecule(GRAD_CFG)
+    g4 = MolGpu(m4, device)
+    C4 = B.density_factor(m4.nbf, B.CONFIGS[GRAD_CFG]["rank"], B.CONFIGS[GRAD_CFG]["seed"])
+    D4 = torch.from_numpy(C4 @ C4.T)
+    return dict(m3=m3, g3=g3, C3=C3, m4=m4, g4=g4, D4=D4, cho=info, t_cho=t_cho)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="molgpu", choices=["molgpu", "reference"])
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        return run_reference(args)
+    return run_gpu(args, rank, world)
+
+
+def run_gpu(args, rank, world):
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from openmolcas_b200.molgpu import MolGpu, lib as mglib
+    S = setup(torch, local)
+    g3, g4, C3, D4 = S["g3"], S["g4"], S["C3"], S["D4"]
+    dev = f"cuda:{local}"
+    C3d = C3.to(dev)
+    D4d = D4.to(dev)
+    st = torch.cuda.current_stream()
+    prec_mixed = MolGpu.PREC_MIXED
+    try:
+        g3.cho_jk(C3d, precision=prec_mixed)
+    except Exception:
+        prec_mixed = MolGpu.PREC_FP64  # mixed path unavailable: report FP64 and say so
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step(prec, ev=None):
+        if ev is not None:
+            ev[0].record(st)
+        J, K = g3.cho_jk(C3d, precision=prec)
+        if ev is not None:
+            ev[1].record(st)
+        gr = g4.drvg1(D4d, cutint=CUTINT)
+        if ev is not None:
+            ev[2].record(st)
+        return J, K, gr
+
+    def timed(prec, K, W):
+        for _ in range(W):
+            step(prec)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+        n0 = mglib().mg_kernel_launches()
+        out = None
+        for k in range(K):
+            flush.zero_()  # L2 flush between steps, outside the events
+            out = step(prec, evs[k])
+        torch.cuda.synchronize()
+        launches = mglib().mg_kernel_launches() - n0
+        if dist:
+            dist.barrier()
+        jk = [e[0].elapsed_time(e[1]) for e in evs]
+        gr = [e[1].elapsed_time(e[2]) for e in evs]
+        return np.array(jk), np.array(gr), launches, out
+
+    # mixed path (headline)
+    clk = ClockSampler(local)
+    clk.start()
+    jk_m, gr_m, launches, out_m = timed(prec_mixed, args.steps, args.warmup)
+    clocks = clk.stop()
+    # plain FP64 path, same step
+    jk_d, gr_d, _, out_d = timed(MolGpu.PREC_FP64, max(2, min(args.steps, 3)), 1)
+    step_m = (jk_m + gr_m) / 1e3
+    step_d = (jk_d.mean() + gr_d.mean()) / 1e3
+    ms = float(step_m.mean() * 1e3)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    # energies of both paths
+    J, K, grad = out_m
+    Jd, Kd, gradd = out_d
+    D3 = C3d @ C3d.t()
+    E_m = float(0.5 * (D3 * J).sum() - 0.25 * (D3 * K).sum())
+    E_d = float(0.5 * (D3 * Jd).sum() - 0.25 * (D3 * Kd).sum())
+    # e2e through the public API with host buffers (pinned), copies inside
+    C3h = C3.clone().pin_memory()
+    D4h = D4.clone().pin_memory()
+    torch.cuda.synchronize()
+    e2e_times = []
+    for k in range(max(2, args.steps)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        Cd = C3h.to(dev, non_blocking=True)
+        Dd = D4h.to(dev, non_blocking=True)
+        Jx, Kx = g3.cho_jk(Cd, precision=prec_mixed)
+        gx = g4.drvg1(Dd, cutint=CUTINT)
+        Jh, Kh, gh = Jx.cpu(), Kx.cpu(), gx.cpu()
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e = float(np.mean(e2e_times[1:] if len(e2e_times) > 2 else e2e_times))
+    h2d = C3h.numel() * 8 + D4h.numel() * 8
+    d2h = 2 * g3.nbf * g3.nbf * 8 + g4.natom * 3 * 8
+    # rooflines of the two legs
+    peaks, src = _peaks()
+    fp64_peak = measure_fp64_peak(torch)
+    n, r, M = g3.nbf, C3.shape[1], S["cho"]["M"]
+    jk_flops = 4.0 * n * n * r * M  # half-transform + K contraction (ideal, exact FP32 products)
+    jk_s = float(jk_m.mean()) / 1e3
+    gr_s = float(gr_m.mean()) / 1e3
+    gflops = grad_flops(g4)
+    legs = {
+        "jk": {"bound": "tensor", "achieved": jk_flops / jk_s / 1e12, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+               "frac": jk_flops / jk_s / 1e12 / peaks["bf16_tflops"], "peak_source": f"{src} bf16 burst",
+               "algorithmic_flops": jk_flops, "seconds": jk_s},
+        "grad": {"bound": "fp64", "achieved": gflops / gr_s / 1e12 if gflops else None, "peak": fp64_peak,
+                 "unit": "TFLOP/s", "frac": (gflops / gr_s / 1e12 / fp64_peak) if (gflops and fp64_peak) else None,
+                 "peak_source": "DFMA microbenchmark measured in this run", "algorithmic_flops": gflops,
+                 "seconds": gr_s},
+    }
+    dom = "jk" if jk_s >= gr_s else "grad"
+    roof = dict(legs[dom])
+    roof["kernel"] = dom
+    roof["traffic"] = None
+    cpu = cpu_baseline(S)
+    res = {
+        "metric": "J/K+grad seconds per step (J/K mixed @1500 bf + 2e gradient @460 bf)",
+        "value": ms / 1e3 * 1.0,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 (gradient, Cholesky); fp32 vectors x split-bf16 (J/K)" if prec_mixed else "f64",
+        "data": "synthetic (seeded molecules, random contractions and densities)",
+        "config": {"workload": f"J/K: {JK_CFG} 120 atoms {g3.nbf} bf, M={M} Cholesky vectors (ThrCom {THRCOM}), "
+                               f"rank {r} density; gradient: {GRAD_CFG} 20 atoms {g4.nbf} bf, rank 40 density, "
+                               f"Schwarz {CUTINT}", "l2": "flushed (256 MB write) between timed steps",
+                   "parallelism": f"replicas x{world}", "jk_precision": "mixed" if prec_mixed else "fp64"},
+        "legs_s": {"jk_mixed": jk_s, "grad": gr_s, "jk_fp64": float(jk_d.mean()) / 1e3},
+        "fp64_path_s": step_d,
+        "speedup_vs_fp64_path": step_d / (ms / 1e3),
+        "energy": {"E_mixed": E_m, "E_fp64": E_d, "dE": E_m - E_d},
+        "cholesky": {"M": M, "npass": S["cho"]["npass"], "setup_s": S["t_cho"]},
+        "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches // max(1, args.steps)),
+        "roofline": roof,
+        "roofline_legs": legs,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def grad_flops(g):
+    try:
+        from openmolcas_b200.molgpu import lib as mglib
+        import ctypes
+        f = mglib().mg_drvg1_flops
+        f.restype = ctypes.c_double
+        f.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        return float(f(g.h, CUTINT))
+    except Exception:
+        return None
+
+
+def cpu_baseline(S=None, budget_s=20.0, threads=None):
+    """Oracle (CPU restatement) on a bounded sample of the same workload,
+    extrapolated to one full step.  J/K: the oracle's J/K over a subset of
+    vectors of the same shape (cost is value-independent), scaled by M;
+    gradient: every k-th unique quartet, scaled by k."""
+    from oracle import oracle as O
+    from openmolcas_b200 import basis as B
+    if threads:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    m3 = S["m3"] if S else B.config_molecule(JK_CFG)
+    m4 = S["m4"] if S else B.config_molecule(GRAD_CFG)
+    M = S["cho"]["M"] if S else 7 * m3.nbf // 2  # typical vectors per function at ThrCom 1e-6
+    o3 = O.Oracle(m3)
+    nrs = m3.nbf * (m3.nbf + 1) // 2
+    rng = np.random.default_rng(0)
+    r = B.CONFIGS[JK_CFG]["rank"]
+    Cm = B.density_factor(m3.nbf, r, B.CONFIGS[JK_CFG]["seed"])
+    nv = 2
+    Ls = rng.standard_normal((nrs, nv)) * 1e-3
+    t0 = time.time()
+    o3.cho_jk(Ls, Cm)
+    t_jk_sample = time.time() - t0
+    t_jk = t_jk_sample * M / nv
+    o4 = O.Oracle(m4)
+    C4 = B.density_factor(m4.nbf, B.CONFIGS[GRAD_CFG]["rank"], B.CONFIGS[GRAD_CFG]["seed"])
+    D4 = C4 @ C4.T
+    o4.schwarz()
+    stride = 4000
+    t0 = time.time()
+    _, nq = O.grad_sampled(o4, D4, CUTINT, stride)
+    t_gr_sample = time.time() - t0
+    t_gr = t_gr_sample * stride
+    return {"value": t_jk + t_gr, "unit": "s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"J/K: {nv} of {M} vectors (scaled x{M / nv:.0f}, {t_jk_sample:.1f}s); gradient: every "
+                      f"{stride}th of {nq} unique quartets (scaled x{stride}, {t_gr_sample:.1f}s)",
+            "legs_s": {"jk": t_jk, "grad": t_gr}}
+
+
+def run_reference(args):
+    import multiprocessing
+    cores = multiprocessing.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    vals = []
+    cb = None
+    for k in range(args.warmup + args.steps):
+        cb = cpu_baseline(None, threads=cores)
+        if k >= args.warmup:
+            vals.append(cb["value"])
+    v = float(np.mean(vals))
+    res = {
+        "metric": "J/K+grad seconds per step (J/K mixed @1500 bf + 2e gradient @460 bf)",
+        "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded molecules)", "impl": "reference",
+        "config": {"workload": f"J/K {JK_CFG} + gradient {GRAD_CFG} (CPU restatement of the reference path)"},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": cb["cores"], "kind": "port", "sample": cb["sample"]},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(res), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

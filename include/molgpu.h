@@ -67,6 +67,67 @@ int mg_eri_quartets_size(mg_handle* h, const int32_t* quartets, int64_t nq, int6
 int mg_eri_quartets(mg_handle* h, const int32_t* quartets, int64_t nq, const int64_t* offsets, double* d_out,
                     void* stream);
 
+/* ---------------------------------------------------------------------
+ * Cholesky decomposition of the ERI matrix (replaces Cho_Drv / Cho_Drv_Inner
+ * with the default algorithm 4, cholesky_util/cho_drv.F90:14,
+ * cho_drv_inner.F90:14, cho_decom_a4.F90:12).  Vectors stay on the device
+ * inside the handle, FP64, in reduced-set layout: AO pairs a>=b grouped by
+ * shell pair (i>=j in iTri order); inside a pair a fastest (i>j) or iTri
+ * (i==j) (cholesky_util/plf_cho_diag.F90:60-72).
+ */
+typedef struct mg_cho_cfg {
+  double thrcom; /* decomposition threshold ThrCom (cholesky.F90:128, 1e-4) */
+  double span;   /* Span (cho_inp.F90:151, 1e-2)                            */
+  int minqual;   /* MinQual (50)                                             */
+  int maxqual;   /* MaxQual (100)                                            */
+  int maxvec;    /* capacity of the vector store (0 = 8 x nbf)               */
+} mg_cho_cfg;
+
+int mg_cho_default(mg_cho_cfg* cfg);
+/* Returns 0 ok, MG_ERR_DECOMP (104) on a decomposition failure (Cho_Quit 104),
+ * MG_ERR_MEMORY when the vectors do not fit.  Synchronous. */
+int mg_cho_drv(mg_handle* h, const mg_cho_cfg* cfg, void* stream);
+int mg_cho_info(mg_handle* h, int64_t* nrs, int* nvec, int* npass);
+/* pivot (rs index) and pass of every vector, in vector order */
+int mg_cho_pivots(mg_handle* h, int32_t* piv, int32_t* pass_of);
+/* AO indices and shell pair of every rs entry (host arrays of length nrs) */
+int mg_cho_rs_list(mg_handle* h, int32_t* a, int32_t* b, int32_t* sp);
+/* copy vectors [first, first+count) to d_out (nrs x count, column-major) */
+int mg_cho_copy_vectors(mg_handle* h, int first, int count, double* d_out, void* stream);
+/* exact diagonal (ab|ab) over the rs list (CHO_GETDIAG, cho_getdiag.F90:12) */
+int mg_cho_diag(mg_handle* h, double* d_diag, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Coulomb and exchange matrices from the Cholesky vectors of the handle
+ * (replaces CHO_LK_SCF, fock_util/cho_lk_scf.F90:14, for one density):
+ *   D = C C^T, C (nbf x r, column-major, device);
+ *   J_ab = sum_cd (ab|cd) D_cd,  K_ab = sum_cd (ac|bd) D_cd
+ * with (ab|cd) ~ sum_J L_ab,J L_cd,J.  J, K: nbf x nbf device, overwritten
+ * (the reference accumulates into FLT/KLT; callers add).
+ * precision: MG_PREC_FP64 (FP64 vectors, FP64 products) or MG_PREC_MIXED
+ * (FP32 vectors, 3-term split-BF16 tensor-core products, FP32 accumulation).
+ */
+#define MG_PREC_FP64 0
+#define MG_PREC_MIXED 1
+int mg_cho_jk(mg_handle* h, const double* d_C, int r, double* d_J, double* d_K, int precision, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Two-electron nuclear gradient (replaces Drvg1, alaska/drvg1.F90:15, with
+ * the 1/2 of alaska.F90:236 applied): d_grad[3*natom] = dE/dR of
+ * E = 1/2 tr(DJ) - 1/4 tr(DK) at fixed density, D the full nbf x nbf
+ * symmetric density on the device (row-major = column-major).  Unique shell
+ * quartets with TMax(ij) TMax(kl) < cutint are skipped (Shell_MxSchwz
+ * screening).  Asynchronous on `stream`.
+ */
+int mg_drvg1(mg_handle* h, const double* d_D, double cutint, double* d_grad, void* stream);
+/* Algorithmic FP64 flop count of one mg_drvg1 call (roofline accounting;
+ * no reference counterpart).  Negative on error. */
+double mg_drvg1_flops(mg_handle* h, double cutint);
+
+/* Number of kernels of this library launched so far in this process (library
+ * calls such as cuBLAS are not counted).  No reference counterpart. */
+long long mg_kernel_launches(void);
+
 #ifdef __cplusplus
 }
 #endif

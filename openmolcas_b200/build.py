@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmolgpu.so")
-SOURCES = ["basis_host.cu", "eri.cu", "capi.cu"]
+SOURCES = ["basis_host.cu", "eri.cu", "cholesky.cu", "grad.cu", "jk.cu", "capi.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -36,7 +36,7 @@ def build(force=False, verbose=False):
     if not force and not needs_build():
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB + ".tmp"] + sources()
+    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB + ".tmp"] + sources() + ["-lcublas"]
     r = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)

@@ -192,17 +192,60 @@ std::vector<double> hrr_matrix(const Handle* h, int la, int lb, const double* A,
   return H;
 }
 
+// Primitive-pair prescreening (the role of Screen, integral_util/
+// screen.F90:109-148): a primitive pair p of shell pair AB is dropped when
+//   s_p * S / sqrt(zeta_p + zeta_min) * 1e3 < kPrimThr,
+// s_p = kappa_p * max_ij |C_i(a) C_j(b)| * (1 + |AB| + zeta_p^-1/2)^(la+lb),
+// S = max over all primitive pairs of s_q.  s_p s_q / sqrt(zeta+eta) bounds
+// |[ab|cd]| of the primitive quartet (F_m <= 1, polynomial factors bounded
+// generously), so every dropped contribution is below 1e-21.
+static const double kPrimThr = 1e-18;
+
 int setup_pairs(Handle* h) {
   const int ns = h->sh.size();
   const double twop54 = std::sqrt(2.0) * std::pow(M_PI, 1.25);
   h->pairs.clear();
-  std::vector<double> zeta, kappa, px, py, pz, al, be, coef, hrr;
+  // pass 1: bounds
+  struct PP { double s, z; };
+  std::vector<std::vector<PP>> est(ns * (ns + 1) / 2);
+  double Smax = 0, zmin = 1e300;
   for (int i = 0; i < ns; ++i)
     for (int j = 0; j <= i; ++j) {
       const ShellH &a = h->sh[i], &b = h->sh[j];
+      double AB2 = 0;
+      for (int x = 0; x < 3; ++x) AB2 += (a.A[x] - b.A[x]) * (a.A[x] - b.A[x]);
+      auto& v = est[pair_id(i, j)];
+      for (int jb = 0; jb < b.np; ++jb)
+        for (int ia = 0; ia < a.np; ++ia) {
+          const double x = a.e[ia], y = b.e[jb], z = x + y;
+          const double k = std::max(twop54 * std::exp(-x * y * AB2 / z) / z, 1e-99);
+          double cm = 0;
+          for (int kb = 0; kb < b.nc; ++kb)
+            for (int ka = 0; ka < a.nc; ++ka) cm = std::max(cm, std::fabs(a.c[ia + a.np * ka] * b.c[jb + b.np * kb]));
+          const double ang = std::pow(1.0 + std::sqrt(AB2) + 1.0 / std::sqrt(z), a.l + b.l);
+          v.push_back({k * cm * ang, z});
+          Smax = std::max(Smax, k * cm * ang);
+          zmin = std::min(zmin, z);
+        }
+    }
+  std::vector<double> zeta, kappa, px, py, pz, al, be, coef, hrr;
+  long long kept = 0, total = 0;
+  for (int i = 0; i < ns; ++i)
+    for (int j = 0; j <= i; ++j) {
+      const ShellH &a = h->sh[i], &b = h->sh[j];
+      const auto& v = est[pair_id(i, j)];
+      std::vector<int> keep;
+      int best = 0;
+      for (int p = 0; p < (int)v.size(); ++p) {
+        if (v[p].s > v[best].s) best = p;
+        if (v[p].s * Smax / std::sqrt(v[p].z + zmin) * 1e3 >= kPrimThr) keep.push_back(p);
+      }
+      if (keep.empty()) keep.push_back(best);
+      total += v.size();
+      kept += keep.size();
       DPair d{};
       d.i = i; d.j = j; d.la = a.l; d.lb = b.l; d.na = a.np; d.nb = b.np; d.nci = a.nc; d.ncj = b.nc;
-      d.np = a.np * b.np;
+      d.np = keep.size();
       d.prim_off = zeta.size();
       d.coef_off = coef.size();
       d.nsa = ncomp(a.l); d.nsb = ncomp(b.l);
@@ -211,20 +254,22 @@ int setup_pairs(Handle* h) {
       d.atom_a = a.atom; d.atom_b = b.atom; d.ao_a = a.off; d.ao_b = b.off;
       double AB2 = 0;
       for (int x = 0; x < 3; ++x) AB2 += (a.A[x] - b.A[x]) * (a.A[x] - b.A[x]);
-      for (int jb = 0; jb < b.np; ++jb)
-        for (int ia = 0; ia < a.np; ++ia) {
-          const double x = a.e[ia], y = b.e[jb], z = x + y, zi = 1.0 / z;
-          double k = twop54 * std::exp(-x * y * AB2 * zi) * zi;
-          if (k < 1e-99) k = 1e-99;
-          zeta.push_back(z); kappa.push_back(k); al.push_back(x); be.push_back(y);
-          px.push_back((x * a.A[0] + y * b.A[0]) * zi);
-          py.push_back((x * a.A[1] + y * b.A[1]) * zi);
-          pz.push_back((x * a.A[2] + y * b.A[2]) * zi);
-        }
+      for (int p : keep) {
+        const int ia = p % a.np, jb = p / a.np;
+        const double x = a.e[ia], y = b.e[jb], z = x + y, zi = 1.0 / z;
+        double k = twop54 * std::exp(-x * y * AB2 * zi) * zi;
+        if (k < 1e-99) k = 1e-99;
+        zeta.push_back(z); kappa.push_back(k); al.push_back(x); be.push_back(y);
+        px.push_back((x * a.A[0] + y * b.A[0]) * zi);
+        py.push_back((x * a.A[1] + y * b.A[1]) * zi);
+        pz.push_back((x * a.A[2] + y * b.A[2]) * zi);
+      }
       for (int kb = 0; kb < b.nc; ++kb)
         for (int ka = 0; ka < a.nc; ++ka)
-          for (int jb = 0; jb < b.np; ++jb)
-            for (int ia = 0; ia < a.np; ++ia) coef.push_back(a.c[ia + a.np * ka] * b.c[jb + b.np * kb]);
+          for (int p : keep) {
+            const int ia = p % a.np, jb = p / a.np;
+            coef.push_back(a.c[ia + a.np * ka] * b.c[jb + b.np * kb]);
+          }
       int ne, emin;
       std::vector<double> H = hrr_matrix(h, a.l, b.l, a.A, b.A, ne, emin);
       d.ne = ne; d.emin = emin;
@@ -232,6 +277,8 @@ int setup_pairs(Handle* h) {
       hrr.insert(hrr.end(), H.begin(), H.end());
       h->pairs.push_back(d);
     }
+  h->prim_kept = kept;
+  h->prim_total = total;
   h->tot_np = zeta.size();
   std::vector<double> prim;
   for (auto* v : {&zeta, &kappa, &px, &py, &pz, &al, &be}) prim.insert(prim.end(), v->begin(), v->end());

@@ -15,23 +15,18 @@ struct mg_handle {
 };
 
 namespace mg {
-size_t eri_smem_plan(int nab, int ncd, int max_accd, int max_nef, int max_tmp, int& NP);
-int eri_launch_class(Handle* h, const EriItem* d_items, int nitems, int nab, int ncd, int NP, size_t smem, double* out,
-                     cudaStream_t st);
+std::atomic<long long> g_launches{0};
 
 // Accumulator budget (doubles) of one work item: nc * nef <= this.
 static const int kAccBudget = 12288;
 
-struct EriClass {
-  int nab, ncd, begin, count, NP;
-  size_t smem;
-};
 
-// Split quartets into work items grouped by (la+lb, lc+ld) class.
+// Split quartets into work items grouped by (la+lb, lc+ld) class; a work
+// item covers a range of the ket contracted-pair index kl.
 int build_eri_items(Handle* h, const int32_t* q4, int64_t nq, const int64_t* offsets, std::vector<EriItem>& items,
                     std::vector<EriClass>& classes) {
-  std::map<int, std::vector<EriItem>> byc;
-  std::map<int, int> mx_acc, mx_nef, mx_tmp;
+  std::vector<std::vector<EriItem>> byc(64);
+  std::vector<ClassStats> st(64);
   const int ns = h->sh.size();
   for (int64_t t = 0; t < nq; ++t) {
     const int i = q4[4 * t], j = q4[4 * t + 1], k = q4[4 * t + 2], l = q4[4 * t + 3];
@@ -39,41 +34,60 @@ int build_eri_items(Handle* h, const int32_t* q4, int64_t nq, const int64_t* off
       h->err = "mg_eri_quartets: shell indices out of range or non-canonical pair (need i>=j, k>=l)";
       return MG_ERR_ARG;
     }
-    const DPair& P = h->pairs[pair_id(i, j)];
-    const DPair& Q = h->pairs[pair_id(k, l)];
+    const int p = pair_id(i, j), q = pair_id(k, l);
+    const DPair& P = h->pairs[p];
+    const DPair& Q = h->pairs[q];
     const int nab = P.la + P.lb, ncd = Q.la + Q.lb;
     const int nef = P.ne * Q.ne;
-    const int nijkl = P.nci * P.ncj * Q.nci * Q.ncj;
-    const int chunk = std::max(1, kAccBudget / nef);
+    const int nij = P.nci * P.ncj, nkl = Q.nci * Q.ncj;
+    if (nij * nef > kAccBudget) {
+      h->err = "mg_eri_quartets: bra contraction block too large";
+      return MG_ERR_ARG;
+    }
+    const int chunk = std::max(1, kAccBudget / (nij * nef));
     const int key = nab * 8 + ncd;
-    for (int c0 = 0; c0 < nijkl; c0 += chunk) {
+    ClassStats& cs = st[key];
+    for (int c0 = 0; c0 < nkl; c0 += chunk) {
       EriItem it;
-      it.p = pair_id(i, j);
-      it.q = pair_id(k, l);
+      it.p = p;
+      it.q = q;
       it.c0 = c0;
-      it.c1 = std::min(nijkl, c0 + chunk);
+      it.c1 = std::min(nkl, c0 + chunk);
       it.out_off = offsets[t];
       byc[key].push_back(it);
-      const int nc = it.c1 - it.c0;
-      mx_acc[key] = std::max(mx_acc[key], nc * nef);
-      mx_nef[key] = std::max(mx_nef[key], nef);
-      mx_tmp[key] = std::max(mx_tmp[key], nc * P.nsa * P.nsb * Q.ne);
+      const int nklc = it.c1 - it.c0;
+      cs.max_acc = std::max(cs.max_acc, nij * nklc * nef);
+      cs.max_nef = std::max(cs.max_nef, nef);
+      cs.max_tmp = std::max(cs.max_tmp, nij * nklc * P.nsa * P.nsb * Q.ne);
+      cs.max_nij = std::max(cs.max_nij, nij);
+      cs.max_npab = std::max(cs.max_npab, P.np);
+      cs.max_npcd = std::max(cs.max_npcd, Q.np);
+      cs.max_cab = std::max(cs.max_cab, nij * P.np);
+      cs.max_ccd = std::max(cs.max_ccd, nklc * Q.np);
     }
   }
   items.clear();
   classes.clear();
-  for (auto& kv : byc) {
+  for (int key = 0; key < 64; ++key) {
+    auto& v = byc[key];
+    if (v.empty()) continue;
     EriClass c;
-    c.nab = kv.first / 8;
-    c.ncd = kv.first % 8;
+    c.nab = key / 8;
+    c.ncd = key % 8;
     c.begin = items.size();
-    c.count = kv.second.size();
-    c.smem = eri_smem_plan(c.nab, c.ncd, mx_acc[kv.first], mx_nef[kv.first], mx_tmp[kv.first], c.NP);
-    if (c.NP < 1) {
+    c.count = v.size();
+    c.plan = eri_plan(c.nab, c.ncd, st[key]);
+    if (c.plan.PAB < 1) {
       h->err = "mg_eri_quartets: class does not fit in shared memory";
       return MG_ERR_ARG;
     }
-    items.insert(items.end(), kv.second.begin(), kv.second.end());
+    // heaviest quartets first so the groups of one CTA carry similar work
+    std::stable_sort(v.begin(), v.end(), [&](const EriItem& a, const EriItem& b) {
+      const long long wa = (long long)h->pairs[a.p].np * h->pairs[a.q].np * (a.c1 - a.c0);
+      const long long wb = (long long)h->pairs[b.p].np * h->pairs[b.q].np * (b.c1 - b.c0);
+      return wa > wb;
+    });
+    items.insert(items.end(), v.begin(), v.end());
     classes.push_back(c);
   }
   return 0;
@@ -86,10 +100,9 @@ int run_eri_items(Handle* h, const std::vector<EriItem>& items, const std::vecto
   if (!d_items) { h->err = "workspace allocation failed"; return MG_ERR_MEMORY; }
   cudaMemcpyAsync(d_items, items.data(), sizeof(EriItem) * items.size(), cudaMemcpyHostToDevice, st);
   for (const EriClass& c : classes) {
-    // grid.x limit is 2^31-1: split very long classes anyway for safety
-    for (int b = 0; b < c.count; b += (1 << 30)) {
-      int n = std::min(c.count - b, 1 << 30);
-      if (eri_launch_class(h, d_items + c.begin + b, n, c.nab, c.ncd, c.NP, c.smem, d_out, st)) {
+    for (int b = 0; b < c.count; b += (1 << 28)) {
+      int n = std::min(c.count - b, 1 << 28);
+      if (eri_launch_class(h, d_items + c.begin + b, n, c.nab, c.ncd, c.plan, d_out, st)) {
         h->err = std::string("ERI kernel launch failed: ") + cudaGetErrorString(cudaGetLastError());
         return MG_ERR_CUDA;
       }
@@ -120,6 +133,10 @@ int mg_create(const char* rys_table_path, int device, mg_handle** out) {
 }
 
 static void free_basis(Handle* h) {
+  cho_free(h->cho);
+  h->cho = nullptr;
+  grad_free(h->grad);
+  h->grad = nullptr;
   cudaFree(h->d_pairs); cudaFree(h->d_prim); cudaFree(h->d_coef); cudaFree(h->d_hrr); cudaFree(h->d_tmax);
   h->d_pairs = nullptr; h->d_prim = nullptr; h->d_coef = nullptr; h->d_hrr = nullptr; h->d_tmax = nullptr;
   h->tmax.clear();
@@ -250,6 +267,112 @@ int mg_schwarz(mg_handle* H, double* tmax) {
   }
   std::copy(h->tmax.begin(), h->tmax.end(), tmax);
   return 0;
+}
+
+int mg_cho_default(mg_cho_cfg* cfg) {
+  if (!cfg) return MG_ERR_ARG;
+  cfg->thrcom = 1e-4;
+  cfg->span = 1e-2;
+  cfg->minqual = 50;
+  cfg->maxqual = 100;
+  cfg->maxvec = 0;
+  return 0;
+}
+
+int mg_cho_drv(mg_handle* H, const mg_cho_cfg* cfg, void* stream) {
+  if (!H || !cfg || cfg->thrcom <= 0 || cfg->maxqual < 1) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  if (h->pairs.empty()) { h->err = "mg_cho_drv: no basis"; return MG_ERR_ARG; }
+  cudaSetDevice(h->device);
+  cho_free(h->cho);
+  h->cho = nullptr;
+  ChoCfgH c;
+  c.thrcom = cfg->thrcom;
+  c.span = cfg->span;
+  c.minqual = cfg->minqual;
+  c.maxqual = std::min(cfg->maxqual, 100000);
+  c.maxvec = cfg->maxvec > 0 ? cfg->maxvec : h->nbf * (h->nbf + 1) / 2;
+  ChoState* st = nullptr;
+  int rc = cho_decompose(h, c, st, (cudaStream_t)stream, h->err);
+  h->cho = st;
+  return rc;
+}
+
+int mg_cho_info(mg_handle* H, int64_t* nrs, int* nvec, int* npass) {
+  if (!H || !H->h.cho) return MG_ERR_ARG;
+  if (nrs) *nrs = cho_nrs(H->h.cho);
+  if (nvec) *nvec = cho_nvec(H->h.cho);
+  if (npass) *npass = cho_npass(H->h.cho);
+  return 0;
+}
+
+int mg_cho_pivots(mg_handle* H, int32_t* piv, int32_t* pass_of) {
+  if (!H || !H->h.cho) return MG_ERR_ARG;
+  cho_pivots(H->h.cho, piv, pass_of);
+  return 0;
+}
+
+int mg_cho_rs_list(mg_handle* H, int32_t* a, int32_t* b, int32_t* sp) {
+  if (!H || !H->h.cho) return MG_ERR_ARG;
+  cho_rs_list(H->h.cho, a, b, sp);
+  return 0;
+}
+
+int mg_cho_copy_vectors(mg_handle* H, int first, int count, double* d_out, void* stream) {
+  if (!H || !H->h.cho || (!d_out && count)) return MG_ERR_ARG;
+  cudaSetDevice(H->h.device);
+  return cho_copy_vectors(H->h.cho, first, count, d_out, (cudaStream_t)stream);
+}
+
+int mg_cho_diag(mg_handle* H, double* d_diag, void* stream) {
+  if (!H || !H->h.cho || !d_diag) return MG_ERR_ARG;
+  cudaSetDevice(H->h.device);
+  cudaMemcpyAsync(d_diag, cho_diag0(H->h.cho), sizeof(double) * cho_nrs(H->h.cho), cudaMemcpyDeviceToDevice,
+                  (cudaStream_t)stream);
+  return 0;
+}
+
+int mg_drvg1(mg_handle* H, const double* d_D, double cutint, double* d_grad, void* stream) {
+  if (!H || !d_D || !d_grad) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  if (h->pairs.empty()) { h->err = "mg_drvg1: no basis"; return MG_ERR_ARG; }
+  cudaSetDevice(h->device);
+  if (h->tmax.empty()) {
+    std::vector<double> t((size_t)h->sh.size() * h->sh.size());
+    int rc = mg_schwarz(H, t.data());
+    if (rc) return rc;
+  }
+  if (!h->grad) h->grad = new GradPlan;
+  if (h->grad->cutint != cutint) {
+    int rc = grad_build(h, cutint, *h->grad);
+    if (rc) return rc;
+  }
+  return grad_run(h, *h->grad, d_D, d_grad, (cudaStream_t)stream);
+}
+
+int mg_cho_jk(mg_handle* H, const double* d_C, int r, double* d_J, double* d_K, int precision, void* stream) {
+  if (!H || !d_C || !d_J || !d_K || r < 1) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  if (!h->cho) { h->err = "mg_cho_jk: no Cholesky vectors (call mg_cho_drv)"; return MG_ERR_ARG; }
+  cudaSetDevice(h->device);
+  if (precision == MG_PREC_FP64) return jk_fp64(h, d_C, r, d_J, d_K, (cudaStream_t)stream, 32);
+  if (precision == MG_PREC_MIXED) return jk_mixed(h, d_C, r, d_J, d_K, (cudaStream_t)stream, 64);
+  h->err = "mg_cho_jk: unsupported precision";
+  return MG_ERR_ARG;
+}
+
+long long mg_kernel_launches(void) { return g_launches.load(); }
+
+double mg_drvg1_flops(mg_handle* H, double cutint) {
+  if (!H) return -1;
+  Handle* h = &H->h;
+  if (h->tmax.empty()) {
+    std::vector<double> t((size_t)h->sh.size() * h->sh.size());
+    if (mg_schwarz(H, t.data())) return -1;
+  }
+  if (!h->grad) h->grad = new GradPlan;
+  if (h->grad->cutint != cutint && grad_build(h, cutint, *h->grad)) return -1;
+  return grad_plan_flops(h, *h->grad);
 }
 
 }  // extern "C"

@@ -69,133 +69,171 @@ __device__ __forceinline__ void rys_rw(const RysArgs& ra, double T, double* x, d
   }
 }
 
+// Threads of one quartet group synchronise on their own named barrier
+// (id 1 + group); a group of 32 is one warp.
+__device__ __forceinline__ void group_sync(int g, int tpq) {
+  if (tpq == 32) {
+    __syncwarp();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(tpq) : "memory");
+  }
+}
+
 template <int NAB, int NCD>
-__global__ void __launch_bounds__(256) eri_kernel(const EriItem* __restrict__ items, const DPair* __restrict__ pairs,
-                                                  const double* __restrict__ prim, int tot_np,
-                                                  const double* __restrict__ coef, const double* __restrict__ hrr,
-                                                  RysArgs ra, double* __restrict__ out, int NP) {
+__global__ void __launch_bounds__(256) eri_kernel(const EriItem* __restrict__ items, int nitems,
+                                                  const DPair* __restrict__ pairs, const double* __restrict__ prim,
+                                                  int tot_np, const double* __restrict__ coef,
+                                                  const double* __restrict__ hrr, RysArgs ra, double* __restrict__ out,
+                                                  int PAB, int PCD, int tpq, int gsm) {
   constexpr int NR = (NAB + NCD) / 2 + 1;
   constexpr int NI = NAB + 1, NJ = NCD + 1;
   constexpr int G1 = NR * NI * NJ;  // one direction
   constexpr int NCF = 10;
-  extern __shared__ double sm[];
-  const EriItem it = items[blockIdx.x];
+  extern __shared__ double smem_all[];
+  const int g = threadIdx.x / tpq;
+  const int item = blockIdx.x * (blockDim.x / tpq) + g;
+  if (item >= nitems) return;  // whole group leaves; no other group waits on it
+  double* sm = smem_all + (size_t)g * gsm;
+  const EriItem it = items[item];
   const DPair& P = pairs[it.p];
   const DPair& Q = pairs[it.q];
   const int npab = P.np, npcd = Q.np;
   const int nij = P.nci * P.ncj;
   const int ne = P.ne, nf = Q.ne, nef = ne * nf;
-  const int nc = it.c1 - it.c0;
+  const int nklc = it.c1 - it.c0;  // ket contracted-pair range [c0, c1)
+  const int nacc = nij * nklc * nef;
   const int eoff = P.emin * (P.emin + 1) * (P.emin + 2) / 6;
   const int foff = Q.emin * (Q.emin + 1) * (Q.emin + 2) / 6;
-  double* acc = sm;                       // nc * nef
-  double* cf = acc + nc * nef;            // NP * NR * NCF
-  double* G = cf + NP * NR * NCF;         // NP * 3 * G1
-  double* E = G + NP * 3 * G1;            // NP * nef (also HRR temp)
-  const int tid = threadIdx.x, nth = blockDim.x;
-  for (int o = tid; o < nc * nef; o += nth) acc[o] = 0.0;
+  const int NT = PAB * PCD;
+  // shared layout: acc | Cab | Ccd | { X | cf | G | E }  (HRR temp reuses {})
+  double* acc = sm;
+  double* Cab = acc + nacc;
+  double* Ccd = Cab + nij * npab;
+  double* X = Ccd + nklc * npcd;
+  double* cf = X + nij * PCD * nef;
+  double* G = cf + NT * NR * NCF;
+  double* E = G + NT * 3 * G1;
+  const int tid = threadIdx.x - g * tpq, nth = tpq;
+  for (int o = tid; o < nacc; o += nth) acc[o] = 0.0;
+  for (int o = tid; o < nij * npab; o += nth) Cab[o] = coef[P.coef_off + o];
+  for (int o = tid; o < nklc * npcd; o += nth) Ccd[o] = coef[Q.coef_off + (size_t)it.c0 * npcd + o];
   const double Ap0 = P.Ap[0], Ap1 = P.Ap[1], Ap2 = P.Ap[2];
   const double Cp0 = Q.Ap[0], Cp1 = Q.Ap[1], Cp2 = Q.Ap[2];
-  const long long ntot = (long long)npab * npcd;
-  for (long long base = 0; base < ntot; base += NP) {
-    const int nt = (int)min((long long)NP, ntot - base);
-    __syncthreads();
-    // ---- 1a: roots and recursion coefficients
-    for (int t = tid; t < nt; t += nth) {
-      const long long tg = base + t;
-      const int pcd = (int)(tg / npab), pab = (int)(tg - (long long)pcd * npab);
-      const int ia = P.prim_off + pab, ic = Q.prim_off + pcd;
-      const double zeta = prim[ia], eta = prim[ic];
-      const double kab = prim[tot_np + ia], kcd = prim[tot_np + ic];
-      const double px = prim[2 * tot_np + ia], py = prim[3 * tot_np + ia], pz = prim[4 * tot_np + ia];
-      const double qx = prim[2 * tot_np + ic], qy = prim[3 * tot_np + ic], qz = prim[4 * tot_np + ic];
-      const double ze = zeta + eta, zei = 1.0 / ze, rho = zeta * eta * zei;
-      const double dx = px - qx, dy = py - qy, dz = pz - qz;
-      const double T = rho * (dx * dx + dy * dy + dz * dz);
-      const double fact = kab * kcd * sqrt(zei);
-      double x[NR], w[NR];
-      rys_rw<NR>(ra, T, x, w);
-      const double zi = 1.0 / zeta, ei = 1.0 / eta;
+  for (int pcd0 = 0; pcd0 < npcd; pcd0 += PCD) {
+    const int npc = min(PCD, npcd - pcd0);
+    group_sync(g, tpq);
+    for (int o = tid; o < nij * PCD * nef; o += nth) X[o] = 0.0;
+    for (int pab0 = 0; pab0 < npab; pab0 += PAB) {
+      const int npa = min(PAB, npab - pab0);
+      const int nt = npa * npc;
+      group_sync(g, tpq);
+      // ---- 1a: roots and recursion coefficients (t = pa + npa * pc)
+      for (int t = tid; t < nt; t += nth) {
+        const int pc = t / npa, pa = t - pc * npa;
+        const int ia = P.prim_off + pab0 + pa, ic = Q.prim_off + pcd0 + pc;
+        const double zeta = prim[ia], eta = prim[ic];
+        const double kab = prim[tot_np + ia], kcd = prim[tot_np + ic];
+        const double px = prim[2 * tot_np + ia], py = prim[3 * tot_np + ia], pz = prim[4 * tot_np + ia];
+        const double qx = prim[2 * tot_np + ic], qy = prim[3 * tot_np + ic], qz = prim[4 * tot_np + ic];
+        const double ze = zeta + eta, zei = 1.0 / ze, rho = zeta * eta * zei;
+        const double dx = px - qx, dy = py - qy, dz = pz - qz;
+        const double T = rho * (dx * dx + dy * dy + dz * dz);
+        const double fact = kab * kcd * sqrt(zei);
+        double x[NR], w[NR];
+        rys_rw<NR>(ra, T, x, w);
+        const double zi = 1.0 / zeta, ei = 1.0 / eta;
 #pragma unroll
-      for (int r = 0; r < NR; ++r) {
-        const double U2 = x[r] * zei;
-        double* c = cf + (t * NR + r) * NCF;
-        c[0] = 0.5 * U2;
-        c[1] = 0.5 * (1.0 - U2 * eta) * zi;
-        c[2] = 0.5 * (1.0 - U2 * zeta) * ei;
-        c[3] = px - Ap0 - eta * U2 * dx;
-        c[4] = py - Ap1 - eta * U2 * dy;
-        c[5] = pz - Ap2 - eta * U2 * dz;
-        c[6] = qx - Cp0 + zeta * U2 * dx;
-        c[7] = qy - Cp1 + zeta * U2 * dy;
-        c[8] = qz - Cp2 + zeta * U2 * dz;
-        c[9] = w[r] * fact;
-      }
-    }
-    __syncthreads();
-    // ---- 1b: 2D recursion per (quartet, root, direction)
-    for (int job = tid; job < nt * NR * 3; job += nth) {
-      const int d = job % 3, tr = job / 3, r = tr % NR, t = tr / NR;
-      const double* c = cf + (t * NR + r) * NCF;
-      const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
-      double I[NI][NJ];
-      I[0][0] = d == 2 ? c[9] : 1.0;
-      if (NI > 1) I[1][0] = C00 * I[0][0];
-#pragma unroll
-      for (int i = 1; i < NI - 1; ++i) I[i + 1][0] = C00 * I[i][0] + i * B10 * I[i - 1][0];
-#pragma unroll
-      for (int j = 0; j < NJ - 1; ++j) {
-#pragma unroll
-        for (int i = 0; i < NI; ++i) {
-          double v = D00 * I[i][j];
-          if (j > 0) v += j * B01 * I[i][j - 1];
-          if (i > 0) v += i * B00 * I[i - 1][j];
-          I[i][j + 1] = v;
+        for (int r = 0; r < NR; ++r) {
+          const double U2 = x[r] * zei;
+          double* c = cf + (t * NR + r) * NCF;
+          c[0] = 0.5 * U2;
+          c[1] = 0.5 * (1.0 - U2 * eta) * zi;
+          c[2] = 0.5 * (1.0 - U2 * zeta) * ei;
+          c[3] = px - Ap0 - eta * U2 * dx;
+          c[4] = py - Ap1 - eta * U2 * dy;
+          c[5] = pz - Ap2 - eta * U2 * dz;
+          c[6] = qx - Cp0 + zeta * U2 * dx;
+          c[7] = qy - Cp1 + zeta * U2 * dy;
+          c[8] = qz - Cp2 + zeta * U2 * dz;
+          c[9] = w[r] * fact;
         }
       }
-      double* g = G + (t * 3 + d) * G1 + r * NI * NJ;
+      group_sync(g, tpq);
+      // ---- 1b: 2D recursion per (quartet, root, direction)
+      if (NI * NJ > 1) {
+        for (int job = tid; job < nt * NR * 3; job += nth) {
+          const int d = job % 3, tr = job / 3, r = tr % NR, t = tr / NR;
+          const double* c = cf + (t * NR + r) * NCF;
+          const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
+          double I[NI][NJ];
+          I[0][0] = d == 2 ? c[9] : 1.0;
+          if (NI > 1) I[1][0] = C00 * I[0][0];
 #pragma unroll
-      for (int i = 0; i < NI; ++i)
+          for (int i = 1; i < NI - 1; ++i) I[i + 1][0] = C00 * I[i][0] + i * B10 * I[i - 1][0];
 #pragma unroll
-        for (int j = 0; j < NJ; ++j) g[i * NJ + j] = I[i][j];
-    }
-    __syncthreads();
-    // ---- 2a: [e0|f0] per primitive quartet
-    for (int job = tid; job < nt * nef; job += nth) {
-      const int ef = job % nef, t = job / nef;
-      const int ie = ef % ne, jf = ef / ne;
-      const unsigned char* ce = c_cart[eoff + ie];
-      const unsigned char* cfp = c_cart[foff + jf];
-      const double* gx = G + (t * 3 + 0) * G1 + ce[0] * NJ + cfp[0];
-      const double* gy = G + (t * 3 + 1) * G1 + ce[1] * NJ + cfp[1];
-      const double* gz = G + (t * 3 + 2) * G1 + ce[2] * NJ + cfp[2];
-      double s = 0.0;
+          for (int j = 0; j < NJ - 1; ++j) {
 #pragma unroll
-      for (int r = 0; r < NR; ++r) s = fma(gx[r * NI * NJ] * gy[r * NI * NJ], gz[r * NI * NJ], s);
-      E[t * nef + ef] = s;
-    }
-    __syncthreads();
-    // ---- 2b: contraction
-    for (int o = tid; o < nc * nef; o += nth) {
-      const int ijkl = it.c0 + o / nef, ef = o - (o / nef) * nef;
-      const int kl = ijkl / nij, ij = ijkl - kl * nij;
-      const double* ca = coef + P.coef_off + (size_t)ij * npab;
-      const double* cc = coef + Q.coef_off + (size_t)kl * npcd;
-      int pcd = (int)(base / npab), pab = (int)(base - (long long)pcd * npab);
-      double s = 0.0;
-      for (int t = 0; t < nt; ++t) {
-        s = fma(__ldg(ca + pab) * __ldg(cc + pcd), E[t * nef + ef], s);
-        if (++pab == npab) { pab = 0; ++pcd; }
+            for (int i = 0; i < NI; ++i) {
+              double v = D00 * I[i][j];
+              if (j > 0) v += j * B01 * I[i][j - 1];
+              if (i > 0) v += i * B00 * I[i - 1][j];
+              I[i][j + 1] = v;
+            }
+          }
+          double* gg = G + (t * 3 + d) * G1 + r * NI * NJ;
+#pragma unroll
+          for (int i = 0; i < NI; ++i)
+#pragma unroll
+            for (int j = 0; j < NJ; ++j) gg[i * NJ + j] = I[i][j];
+        }
+        group_sync(g, tpq);
+        // ---- 2a: [e0|f0] per primitive quartet
+        for (int job = tid; job < nt * nef; job += nth) {
+          const int ef = job % nef, t = job / nef;
+          const int ie = ef % ne, jf = ef / ne;
+          const unsigned char* ce = c_cart[eoff + ie];
+          const unsigned char* cfp = c_cart[foff + jf];
+          const double* gx = G + (t * 3 + 0) * G1 + ce[0] * NJ + cfp[0];
+          const double* gy = G + (t * 3 + 1) * G1 + ce[1] * NJ + cfp[1];
+          const double* gz = G + (t * 3 + 2) * G1 + ce[2] * NJ + cfp[2];
+          double s = 0.0;
+#pragma unroll
+          for (int r = 0; r < NR; ++r) s = fma(gx[r * NI * NJ] * gy[r * NI * NJ], gz[r * NI * NJ], s);
+          E[t * nef + ef] = s;
+        }
+      } else {
+        // (ss|ss): [00|00] = w * prefactor, no recursion
+        for (int t = tid; t < nt; t += nth) E[t] = cf[t * NR * NCF + 9];
       }
+      group_sync(g, tpq);
+      // ---- 2b1: bra half-transform  X[ij][pc][ef] += sum_pa Cab[ij][pa] E[pa,pc][ef]
+      for (int o = tid; o < nij * npc * nef; o += nth) {
+        const int ef = o % nef, r1 = o / nef, pc = r1 % npc, ij = r1 / npc;
+        const double* ca = Cab + ij * npab + pab0;
+        const double* e = E + (size_t)pc * npa * nef + ef;
+        double s = 0.0;
+        for (int pa = 0; pa < npa; ++pa) s = fma(ca[pa], e[pa * nef], s);
+        X[ef + nef * (pc + PCD * ij)] += s;
+      }
+    }
+    group_sync(g, tpq);
+    // ---- 2b2: ket half-transform  acc[ij][kl][ef] += sum_pc Ccd[kl][pc] X[ij][pc][ef]
+    for (int o = tid; o < nacc; o += nth) {
+      const int ef = o % nef, r1 = o / nef, ij = r1 % nij, klc = r1 / nij;
+      const double* cc = Ccd + klc * npcd + pcd0;
+      const double* xx = X + ef + nef * PCD * ij;
+      double s = 0.0;
+      for (int pc = 0; pc < npc; ++pc) s = fma(cc[pc], xx[nef * pc], s);
       acc[o] += s;
     }
   }
-  __syncthreads();
+  group_sync(g, tpq);
   // ---- 3: HRR + spherical, bra then ket
+  const int nc = nij * nklc;
   const int nsab = P.nsa * P.nsb, nscd = Q.nsa * Q.nsb;
   const double* Hab = hrr + P.hrr_off;
   const double* Hcd = hrr + Q.hrr_off;
-  double* tmp = E;  // nc * nsab * nf
+  double* tmp = X;  // nc * nsab * nf
   for (int o = tid; o < nc * nsab * nf; o += nth) {
     const int jf = o % nf, r1 = o / nf, sab = r1 % nsab, cl = r1 / nsab;
     const double* a = acc + cl * nef + jf * ne;
@@ -204,21 +242,22 @@ __global__ void __launch_bounds__(256) eri_kernel(const EriItem* __restrict__ it
     for (int ie = 0; ie < ne; ++ie) s = fma(__ldg(hc + ie), a[ie], s);
     tmp[o] = s;
   }
-  __syncthreads();
+  group_sync(g, tpq);
   const long long nijkl = (long long)nij * Q.nci * Q.ncj;
+  const long long cbase = (long long)nij * it.c0;
   for (int o = tid; o < nc * nsab * nscd; o += nth) {
     const int cl = o % nc, r1 = o / nc, sab = r1 % nsab, scd = r1 / nsab;
     const double* tp = tmp + ((size_t)cl * nsab + sab) * nf;
     const double* hc = Hcd + (size_t)scd * nf;
     double s = 0.0;
     for (int jf = 0; jf < nf; ++jf) s = fma(__ldg(hc + jf), tp[jf], s);
-    out[it.out_off + (it.c0 + cl) + nijkl * (sab + (long long)nsab * scd)] = s;
+    out[it.out_off + cbase + cl + nijkl * (sab + (long long)nsab * scd)] = s;
   }
 }
 
 // ---------------------------------------------------------------- launch
-using KernelFn = void (*)(const EriItem*, const DPair*, const double*, int, const double*, const double*, RysArgs,
-                          double*, int);
+using KernelFn = void (*)(const EriItem*, int, const DPair*, const double*, int, const double*, const double*,
+                          RysArgs, double*, int, int, int, int);
 
 template <int NAB, int NCD>
 static KernelFn get_kernel() {
@@ -257,24 +296,48 @@ static KernelFn pick(int nab, int ncd) {
   return nullptr;
 }
 
-// shared-memory plan for one class: NP primitive quartets per chunk and the
-// dynamic shared-memory bytes (acc | cf | G | max(E, HRR temp)).
-size_t eri_smem_plan(int nab, int ncd, int max_accd, int max_nef, int max_tmp, int& NP) {
+// Launch plan of one class.  tpq threads work on one quartet (a group);
+// 256/tpq groups share a CTA.  Primitive quartets are processed in tiles of
+// PAB bra x PCD ket primitive pairs.  Per-group shared memory (doubles):
+//   acc (nij*nklc*nef) | Cab (nij*npab) | Ccd (nklc*npcd) |
+//   max( X (nij*PCD*nef) + NT*(NR*10 + 3*G1 + nef),  HRR temp )
+
+
+ClassPlan eri_plan(int nab, int ncd, const ClassStats& cs) {
   const int NR = (nab + ncd) / 2 + 1;
   const int G1 = NR * (nab + 1) * (ncd + 1);
-  const size_t budget = 224 * 1024 / 8;  // doubles
-  size_t total = 0;
-  int np = 256;
-  for (; np >= 1; --np) {
-    total = (size_t)max_accd + (size_t)np * (NR * 10 + 3 * G1) + std::max((size_t)np * max_nef, (size_t)max_tmp);
-    if (total <= budget) break;
+  const size_t budget = 224 * 1024 / 8;  // doubles per CTA
+  ClassPlan pl{0, 0, 0, 0, 0};
+  auto need = [&](int pab, int pcd) {
+    const size_t nt = (size_t)pab * pcd;
+    const size_t tile = (size_t)cs.max_nij * pcd * cs.max_nef + nt * (NR * 10 + 3 * G1 + cs.max_nef);
+    return (size_t)cs.max_acc + cs.max_cab + cs.max_ccd + std::max(tile, (size_t)cs.max_tmp);
+  };
+  int pab = std::max(1, std::min(cs.max_npab, 64));
+  int pcd = std::max(1, std::min(cs.max_npcd, std::max(1, 256 / pab)));
+  const int width = std::max({cs.max_acc, pab * pcd * cs.max_nef / 2, pab * pcd * NR * 3});
+  int tpq = width <= 48 ? 32 : width <= 160 ? 64 : width <= 640 ? 128 : 256;
+  for (; tpq <= 256; tpq *= 2) {
+    const int groups = 256 / tpq;
+    const size_t gbudget = budget / groups;
+    int a = pab, c = pcd;
+    while (need(a, c) > gbudget && (a > 1 || c > 1)) {
+      if (c > 1) c = (c + 1) / 2;
+      else a = (a + 1) / 2;
+    }
+    if (need(a, c) <= gbudget) {
+      pl.tpq = tpq;
+      pl.PAB = a;
+      pl.PCD = c;
+      pl.gsm = (int)((need(a, c) + 1) & ~(size_t)1);
+      pl.smem = 8 * (size_t)pl.gsm * groups;
+      return pl;
+    }
   }
-  if (np < 1) { NP = 0; return 0; }
-  NP = np;
-  return 8 * total;
+  return pl;  // PAB == 0: does not fit
 }
 
-int eri_launch_class(Handle* h, const EriItem* d_items, int nitems, int nab, int ncd, int NP, size_t smem, double* out,
+int eri_launch_class(Handle* h, const EriItem* d_items, int nitems, int nab, int ncd, const ClassPlan& pl, double* out,
                      cudaStream_t st) {
   init_cart_table();
   KernelFn k = pick(nab, ncd);
@@ -282,7 +345,11 @@ int eri_launch_class(Handle* h, const EriItem* d_items, int nitems, int nab, int
   RysArgs ra;
   for (int i = 0; i < MG_MAX_RYS; ++i) ra.m[i] = h->rys_meta[i];
   ra.tab = h->d_rys;
-  k<<<nitems, 256, smem, st>>>(d_items, h->d_pairs, h->d_prim, h->tot_np, h->d_coef, h->d_hrr, ra, out, NP);
+  const int groups = 256 / pl.tpq;
+  const int nblk = (nitems + groups - 1) / groups;
+  k<<<nblk, 256, pl.smem, st>>>(d_items, nitems, h->d_pairs, h->d_prim, h->tot_np, h->d_coef, h->d_hrr, ra, out, pl.PAB,
+                                pl.PCD, pl.tpq, pl.gsm);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   return cudaGetLastError() == cudaSuccess ? 0 : 3;
 }
 

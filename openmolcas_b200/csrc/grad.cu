@@ -1,0 +1,540 @@
+// Two-electron nuclear gradient (FP64) -- the adjoint of the ERI kernel.
+//
+// Restates the reference path Drvg1 -> Eval_g1_ijkl -> TwoEl_g -> Rysg1
+// (alaska/drvg1.F90:15, alaska_util/eval_g1_ijkl.F90:15, twoel_g.F90:15,
+// rys_util/rysg1.F90:91-288):
+//   * 2-PDM of a closed-shell determinant, PGet1 (integral_util/pget1.F90:
+//     66-106): G_ijkl = D_ij D_kl - 1/4 (D_ik D_jl + D_il D_jk), built per
+//     shell quartet from D in shared memory, back-transformed spherical ->
+//     Cartesian (SphCr1/SphCr2, twoel_g.F90:328-340);
+//   * de-contraction to each primitive quartet (Tcrtnc, twoel_g.F90:390);
+//   * Rys roots for l_tot + 1 (nRys = (sum l + 3)/2, rysg1.F90:91), 2D
+//     recursion, 2D-level HRR (HRR2Da/HRR2Db), derivative 2D integrals
+//     2a I(a+1) - a I(a-1) (Rys2Dg), contraction with the 2-PDM (Assg1);
+//   * translational invariance gives the fourth centre (Distg1), the
+//     gradient is scaled by 1/2 (alaska.F90:236) and by the permutational
+//     degeneracy of the unique quartet.
+// Nothing is stored: integrals are recomputed primitive quartet by primitive
+// quartet and contracted on the fly (the "hand-written adjoint").
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "mg_internal.h"
+
+namespace mg {
+
+struct RysArgsG {
+  RysMeta m[MG_MAX_RYS];
+  const double* tab;
+};
+
+
+// Cartesian -> spherical matrices (column m, row Cartesian) for l = 0..3,
+// C3 Cartesian order; offsets c_sph_off[l].
+__constant__ double c_sph[1 + 9 + 30 + 70];
+__constant__ int c_sph_off[4];
+__constant__ unsigned char c_cartg[120][3];
+
+static void init_grad_tables(const Handle* h) {
+  static bool done = false;
+  if (done) return;
+  std::vector<double> s;
+  int off[4];
+  for (int l = 0; l <= 3; ++l) {
+    off[l] = s.size();
+    s.insert(s.end(), h->sph[l].begin(), h->sph[l].end());
+  }
+  cudaMemcpyToSymbol(c_sph, s.data(), sizeof(double) * s.size());
+  cudaMemcpyToSymbol(c_sph_off, off, sizeof(off));
+  unsigned char t[120][3];
+  int k = 0;
+  for (int l = 0; l <= 7; ++l)
+    for (int lx = l; lx >= 0; --lx)
+      for (int ly = l - lx; ly >= 0; --ly) {
+        t[k][0] = lx; t[k][1] = ly; t[k][2] = l - lx - ly;
+        ++k;
+      }
+  cudaMemcpyToSymbol(c_cartg, t, sizeof(t));
+  done = true;
+}
+
+__device__ __forceinline__ void gsync(int g, int tpq) {
+  if (tpq == 32) __syncwarp();
+  else asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(tpq) : "memory");
+}
+
+__device__ __forceinline__ int d_ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__device__ __forceinline__ int d_ncomp(int l) { return l >= 2 ? 2 * l + 1 : d_ncart(l); }
+__device__ __forceinline__ int d_ccum(int l) { return l * (l + 1) * (l + 2) / 6; }
+
+// one Rys root/weight of order N at T (table or asymptotic)
+template <int N>
+__device__ __forceinline__ void rys_one(const RysArgsG& ra, double T, int r, double& x, double& w) {
+  const RysMeta& m = ra.m[N - 1];
+  if (T >= m.tmax) {
+    const double ai = 1.0 / T;
+    x = m.hx[r] * ai;
+    w = m.hw[r] * sqrt(ai);
+  } else {
+    int k = (int)(T * m.invh);
+    k = k < m.K ? k : m.K - 1;
+    const double s = 2.0 * (T - k * m.h) * m.invh - 1.0;
+    const double* c = ra.tab + m.off + (size_t)k * (2 * N * 8);
+    const double* cx = c + r * 8;
+    const double* cw = c + (N + r) * 8;
+    double ax = __ldg(cx + 7), aw = __ldg(cw + 7);
+#pragma unroll
+    for (int j = 6; j >= 0; --j) {
+      ax = fma(ax, s, __ldg(cx + j));
+      aw = fma(aw, s, __ldg(cw + j));
+    }
+    x = ax;
+    w = aw;
+  }
+}
+
+template <int NAB1, int NCD1>
+__global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ items, int nitems,
+                                                   const DPair* __restrict__ pairs, const double* __restrict__ prim,
+                                                   int tot_np, const double* __restrict__ coef,
+                                                   const double* __restrict__ Dm, int nbf, RysArgsG ra,
+                                                   double* __restrict__ grad, int tpq, int gsm, int rw) {
+  constexpr int NR = (NAB1 + NCD1 + 1) / 2;
+  constexpr int NI = NAB1 + 1, NJ = NCD1 + 1;
+  extern __shared__ double smem_all[];
+  const int g = threadIdx.x / tpq;
+  const int item = blockIdx.x * (blockDim.x / tpq) + g;
+  if (item >= nitems) return;
+  const int tid = threadIdx.x - g * tpq;
+  double* sm = smem_all + (size_t)g * gsm;
+  const GradItem it = items[item];
+  const DPair& P = pairs[it.p];
+  const DPair& Q = pairs[it.q];
+  const int la = P.la, lb = P.lb, lc = Q.la, ld = Q.lb;
+  const int nca = d_ncart(la), ncb = d_ncart(lb), ncc = d_ncart(lc), ncd = d_ncart(ld);
+  const int nsa = d_ncomp(la), nsb = d_ncomp(lb), nsc = d_ncomp(lc), nsd = d_ncomp(ld);
+  const int ncart4 = nca * ncb * ncc * ncd;
+  const int nc = it.c1 - it.c0;
+  const int nij = P.nci * P.ncj;
+  const int n1d = (la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
+  const int scr = NI * (lb + 2) * NJ + (la + 2) * (lb + 2) * NJ * (ld + 1);
+  // shared layout (doubles):  Gam | union{ stage-0 temp | Gp, cf, CO, G2, F, S }
+  // Gp is only materialised with more than one contracted quartet (else the
+  // single coefficient is folded into the sum).  F and S hold rw roots.
+  double* Gam = sm;                               // nc * ncart4
+  double* Tmp = Gam + nc * ncart4;                // stage-0 temp (nc * ncart4)
+  double* Gp = Tmp;                               // ncart4 (nc > 1)
+  double* cf = Tmp + (nc > 1 ? ncart4 : 0);       // NR * 10 + 4
+  double* CO = cf + NR * 10 + 4;                  // nc
+  double* G2 = CO + nc;                           // 3 * NR * NI * NJ  (unused slot kept for layout)
+  double* F = G2 + 3 * NR;                        // rw * 3 * 4 * n1d
+  double* S = F + rw * 12 * n1d;                  // 3 * rw * scr
+  // ---- stage 0: contracted 2-PDM (PGet1), spherical, then -> Cartesian
+  {
+    const int nsp4 = nsa * nsb * nsc * nsd;
+    for (int o = tid; o < nc * nsp4; o += tpq) {
+      const int il = o % nc, r1 = o / nc;
+      const int sa = r1 % nsa, r2 = r1 / nsa, sb = r2 % nsb, r3 = r2 / nsb, sc = r3 % nsc, sd = r3 / nsc;
+      const int ijkl = it.c0 + il;
+      const int kl = ijkl / nij, ij = ijkl - kl * nij;
+      const int ki = ij % P.nci, kj = ij / P.nci, kk = kl % Q.nci, kq = kl / Q.nci;
+      const int pa = P.ao_a + sa * P.nci + ki, pb = P.ao_b + sb * P.ncj + kj;
+      const int pc = Q.ao_a + sc * Q.nci + kk, pd = Q.ao_b + sd * Q.ncj + kq;
+      const double v = Dm[(size_t)pa * nbf + pb] * Dm[(size_t)pc * nbf + pd] -
+                       0.25 * (Dm[(size_t)pa * nbf + pc] * Dm[(size_t)pb * nbf + pd] +
+                               Dm[(size_t)pa * nbf + pd] * Dm[(size_t)pb * nbf + pc]);
+      Tmp[o] = v;
+    }
+    gsync(g, tpq);
+    // four one-index transforms: d, c, b, a (layout il + nc*(a + A*(b + B*(c + C*d))))
+    const double* Sd = c_sph + c_sph_off[ld];
+    const double* Sc = c_sph + c_sph_off[lc];
+    const double* Sb = c_sph + c_sph_off[lb];
+    const double* Sa = c_sph + c_sph_off[la];
+    // d: [il][sa][sb][sc][sd] -> [il][sa][sb][sc][cd]
+    {
+      const int inner = nc * nsa * nsb * nsc;
+      for (int o = tid; o < inner * ncd; o += tpq) {
+        const int in = o % inner, cd = o / inner;
+        double s = 0;
+        for (int m = 0; m < nsd; ++m) s = fma(Sd[cd + ncd * m], Tmp[in + inner * m], s);
+        Gam[o] = s;
+      }
+      gsync(g, tpq);
+    }
+    // c: [il][sa][sb][sc][cd] -> [il][sa][sb][cc][cd]
+    {
+      const int inner = nc * nsa * nsb;
+      for (int o = tid; o < inner * ncc * ncd; o += tpq) {
+        const int in = o % inner, r1 = o / inner, cc = r1 % ncc, cd = r1 / ncc;
+        double s = 0;
+        for (int m = 0; m < nsc; ++m) s = fma(Sc[cc + ncc * m], Gam[in + inner * (m + nsc * cd)], s);
+        Tmp[o] = s;
+      }
+      gsync(g, tpq);
+    }
+    // b
+    {
+      const int inner = nc * nsa;
+      const int outer = ncc * ncd;
+      for (int o = tid; o < inner * ncb * outer; o += tpq) {
+        const int in = o % inner, r1 = o / inner, cb = r1 % ncb, ou = r1 / ncb;
+        double s = 0;
+        for (int m = 0; m < nsb; ++m) s = fma(Sb[cb + ncb * m], Tmp[in + inner * (m + nsb * ou)], s);
+        Gam[o] = s;
+      }
+      gsync(g, tpq);
+    }
+    // a
+    {
+      const int outer = ncb * ncc * ncd;
+      for (int o = tid; o < nc * nca * outer; o += tpq) {
+        const int il = o % nc, r1 = o / nc, ca = r1 % nca, ou = r1 / nca;
+        double s = 0;
+        for (int m = 0; m < nsa; ++m) s = fma(Sa[ca + nca * m], Gam[il + nc * (m + nsa * ou)], s);
+        Tmp[o] = s;
+      }
+      gsync(g, tpq);
+      for (int o = tid; o < nc * ncart4; o += tpq) Gam[o] = Tmp[o];
+      gsync(g, tpq);
+    }
+  }
+  double acc[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+  const double A0 = P.A[0], A1 = P.A[1], A2 = P.A[2];
+  const double C0 = Q.A[0], C1 = Q.A[1], C2 = Q.A[2];
+  const double ABx[3] = {P.A[0] - P.B[0], P.A[1] - P.B[1], P.A[2] - P.B[2]};
+  const double CDx[3] = {Q.A[0] - Q.B[0], Q.A[1] - Q.B[1], Q.A[2] - Q.B[2]};
+  const int npab = P.np, npcd = Q.np;
+  const long long ntot = (long long)npab * npcd;
+  const int ca0 = d_ccum(la), cb0 = d_ccum(lb), cc0 = d_ccum(lc), cd0 = d_ccum(ld);
+  for (long long tq = 0; tq < ntot; ++tq) {
+    const int pcd = (int)(tq / npab), pab = (int)(tq - (long long)pcd * npab);
+    const int ia = P.prim_off + pab, ic = Q.prim_off + pcd;
+    // ---- (1) roots (thread r), contraction coefficients (threads < nc)
+    if (tid < NR) {
+      const int r = tid;
+      const double zeta = prim[ia], eta = prim[ic];
+      const double px = prim[2 * tot_np + ia], py = prim[3 * tot_np + ia], pz = prim[4 * tot_np + ia];
+      const double qx = prim[2 * tot_np + ic], qy = prim[3 * tot_np + ic], qz = prim[4 * tot_np + ic];
+      const double ze = zeta + eta, zei = 1.0 / ze, rho = zeta * eta * zei;
+      const double dx = px - qx, dy = py - qy, dz = pz - qz;
+      const double T = rho * (dx * dx + dy * dy + dz * dz);
+      const double fact = prim[tot_np + ia] * prim[tot_np + ic] * sqrt(zei);
+      double x, w;
+      rys_one<NR>(ra, T, r, x, w);
+      const double U2 = x * zei;
+      double* c = cf + r * 10;
+      c[0] = 0.5 * U2;
+      c[1] = 0.5 * (1.0 - U2 * eta) / zeta;
+      c[2] = 0.5 * (1.0 - U2 * zeta) / eta;
+      c[3] = px - A0 - eta * U2 * dx;
+      c[4] = py - A1 - eta * U2 * dy;
+      c[5] = pz - A2 - eta * U2 * dz;
+      c[6] = qx - C0 + zeta * U2 * dx;
+      c[7] = qy - C1 + zeta * U2 * dy;
+      c[8] = qz - C2 + zeta * U2 * dz;
+      c[9] = w * fact;
+      if (r == 0) {
+        cf[NR * 10 + 0] = 2.0 * prim[5 * tot_np + ia];  // 2 alpha
+        cf[NR * 10 + 1] = 2.0 * prim[6 * tot_np + ia];  // 2 beta
+        cf[NR * 10 + 2] = 2.0 * prim[5 * tot_np + ic];  // 2 gamma
+      }
+    }
+    for (int il = tid; il < nc; il += tpq) {
+      const int ijkl = it.c0 + il;
+      const int kl = ijkl / nij, ij = ijkl - kl * nij;
+      CO[il] = coef[P.coef_off + (size_t)ij * npab + pab] * coef[Q.coef_off + (size_t)kl * npcd + pcd];
+    }
+    gsync(g, tpq);
+    // ---- (3) primitive-level 2-PDM (Tcrtnc); single contraction: folded in below
+    if (nc > 1) {
+      for (int o = tid; o < ncart4; o += tpq) {
+        double s = 0.0;
+        for (int il = 0; il < nc; ++il) s = fma(CO[il], Gam[il + nc * o], s);
+        Gp[o] = s;
+      }
+    }
+    const double co0 = CO[0];
+    for (int r0 = 0; r0 < NR; r0 += rw) {
+      const int nrw = min(rw, NR - r0);
+      // ---- (2) 2D recursion, 2D-level HRR and derivative factors per (root, direction)
+      if (tid < 3 * nrw) {
+        const int d = tid % 3, rl = tid / 3, r = r0 + rl;
+        const double* c = cf + r * 10;
+        const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
+        double I[NI][NJ];
+        I[0][0] = d == 2 ? c[9] : 1.0;
+        if (NI > 1) I[1][0] = C00 * I[0][0];
+#pragma unroll
+        for (int i = 1; i < NI - 1; ++i) I[i + 1][0] = C00 * I[i][0] + i * B10 * I[i - 1][0];
+#pragma unroll
+        for (int j = 0; j < NJ - 1; ++j) {
+#pragma unroll
+          for (int i = 0; i < NI; ++i) {
+            double v = D00 * I[i][j];
+            if (j > 0) v += j * B01 * I[i][j - 1];
+            if (i > 0) v += i * B00 * I[i - 1][j];
+            I[i][j + 1] = v;
+          }
+        }
+        double* T = S + (size_t)tid * scr;            // T[a][b][f]
+        double* U = T + NI * (lb + 2) * NJ;          // U[a][b][c][d]
+        const int LB2 = lb + 2;
+#pragma unroll
+        for (int a = 0; a < NI; ++a)
+#pragma unroll
+          for (int f = 0; f < NJ; ++f) T[(a * LB2) * NJ + f] = I[a][f];
+        const double ab = ABx[d], cdv = CDx[d];
+        for (int b = 1; b < LB2; ++b)
+          for (int a = 0; a + b <= NAB1; ++a)
+            for (int f = 0; f < NJ; ++f)
+              T[(a * LB2 + b) * NJ + f] = T[((a + 1) * LB2 + b - 1) * NJ + f] + ab * T[(a * LB2 + b - 1) * NJ + f];
+        const int LD1 = ld + 1;
+        for (int a = 0; a < la + 2; ++a)
+          for (int b = 0; b < LB2; ++b) {
+            if (a + b > NAB1) continue;
+            double* u = U + ((a * LB2 + b) * NJ) * LD1;
+            for (int cc = 0; cc < NJ; ++cc) u[cc * LD1] = T[(a * LB2 + b) * NJ + cc];
+            for (int dd = 1; dd < LD1; ++dd)
+              for (int cc = 0; cc + dd <= NCD1; ++cc)
+                u[cc * LD1 + dd] = u[(cc + 1) * LD1 + dd - 1] + cdv * u[cc * LD1 + dd - 1];
+          }
+        const double ta = cf[NR * 10 + 0], tb = cf[NR * 10 + 1], tg = cf[NR * 10 + 2];
+        double* Fo = F + (size_t)(rl * 3 + d) * 4 * n1d;
+        for (int dd = 0; dd <= ld; ++dd)
+          for (int cc = 0; cc <= lc; ++cc)
+            for (int b = 0; b <= lb; ++b)
+              for (int a = 0; a <= la; ++a) {
+                const int o = a + (la + 1) * (b + (lb + 1) * (cc + (lc + 1) * dd));
+                const double* u0 = U + (((a * LB2 + b) * NJ) + cc) * LD1 + dd;
+                Fo[o] = u0[0];
+                Fo[n1d + o] = ta * u0[LB2 * NJ * LD1] - (a ? a * u0[-LB2 * NJ * LD1] : 0.0);
+                Fo[2 * n1d + o] = tb * u0[NJ * LD1] - (b ? b * u0[-NJ * LD1] : 0.0);
+                Fo[3 * n1d + o] = tg * u0[LD1] - (cc ? cc * u0[-LD1] : 0.0);
+              }
+      }
+      gsync(g, tpq);
+      // ---- (4) Assg1: sum over Cartesian components and the roots of this wave
+      for (int o = tid; o < ncart4; o += tpq) {
+        const double gm = nc > 1 ? Gp[o] : co0 * Gam[o];
+        if (gm == 0.0) continue;
+        const int ca = o % nca, r1 = o / nca, cb = r1 % ncb, r2 = r1 / ncb, cc = r2 % ncc, cd = r2 / ncc;
+        const unsigned char* ea = c_cartg[ca0 + ca];
+        const unsigned char* eb = c_cartg[cb0 + cb];
+        const unsigned char* ec = c_cartg[cc0 + cc];
+        const unsigned char* ed = c_cartg[cd0 + cd];
+        int idx[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) idx[d] = ea[d] + (la + 1) * (eb[d] + (lb + 1) * (ec[d] + (lc + 1) * ed[d]));
+        for (int rl = 0; rl < nrw; ++rl) {
+          const double* Fx = F + (size_t)(rl * 3 + 0) * 4 * n1d + idx[0];
+          const double* Fy = F + (size_t)(rl * 3 + 1) * 4 * n1d + idx[1];
+          const double* Fz = F + (size_t)(rl * 3 + 2) * 4 * n1d + idx[2];
+          const double X = Fx[0], Y = Fy[0], Z = Fz[0];
+          const double gyz = gm * Y * Z, gxz = gm * X * Z, gxy = gm * X * Y;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            acc[3 * k + 0] = fma(gyz, Fx[(k + 1) * n1d], acc[3 * k + 0]);
+            acc[3 * k + 1] = fma(gxz, Fy[(k + 1) * n1d], acc[3 * k + 1]);
+            acc[3 * k + 2] = fma(gxy, Fz[(k + 1) * n1d], acc[3 * k + 2]);
+          }
+        }
+      }
+      gsync(g, tpq);
+    }
+  }
+  // ---- reduce over the group, distribute to atoms (Distg1)
+  double* red = S;  // tpq/32 * 9 doubles (S holds at least 72)
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    double v = acc[k];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if ((tid & 31) == 0) red[(tid >> 5) * 9 + k] = v;
+  }
+  gsync(g, tpq);
+  if (tid < 9) {
+    double v = 0.0;
+    for (int w = 0; w < tpq / 32; ++w) v += red[w * 9 + tid];
+    v *= it.scale;
+    const int X = tid / 3, d = tid % 3;
+    const int atom = X == 0 ? P.atom_a : X == 1 ? P.atom_b : Q.atom_a;
+    atomicAdd(&grad[3 * atom + d], v);
+    atomicAdd(&grad[3 * Q.atom_b + d], -v);  // translational invariance
+  }
+}
+
+// ------------------------------------------------------------------ launch
+using GradFn = void (*)(const GradItem*, int, const DPair*, const double*, int, const double*, const double*, int,
+                        RysArgsG, double*, int, int, int);
+
+template <int A, int B>
+static GradFn gk() {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(grad_kernel<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    attr = true;
+  }
+  return grad_kernel<A, B>;
+}
+template <int A>
+static GradFn gk_b(int b) {
+  switch (b) {
+    case 1: return gk<A, 1>();
+    case 2: return gk<A, 2>();
+    case 3: return gk<A, 3>();
+    case 4: return gk<A, 4>();
+    case 5: return gk<A, 5>();
+    case 6: return gk<A, 6>();
+    case 7: return gk<A, 7>();
+  }
+  return nullptr;
+}
+static GradFn pick_grad(int a, int b) {
+  switch (a) {
+    case 1: return gk_b<1>(b);
+    case 2: return gk_b<2>(b);
+    case 3: return gk_b<3>(b);
+    case 4: return gk_b<4>(b);
+    case 5: return gk_b<5>(b);
+    case 6: return gk_b<6>(b);
+    case 7: return gk_b<7>(b);
+  }
+  return nullptr;
+}
+
+
+// per-group shared memory (doubles) of one item with rw roots per wave
+static size_t grad_group_smem(const DPair& P, const DPair& Q, int nc, int rw) {
+  const int la = P.la, lb = P.lb, lc = Q.la, ld = Q.lb;
+  const int NI = la + lb + 2, NJ = lc + ld + 2;
+  const int NR = (la + lb + lc + ld + 3) / 2;
+  const size_t ncart4 = (size_t)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+  const size_t n1d = (size_t)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
+  const size_t scr = (size_t)NI * (lb + 2) * NJ + (size_t)(la + 2) * (lb + 2) * NJ * (ld + 1);
+  const size_t mainsz = (nc > 1 ? ncart4 : 0) + NR * 10 + 4 + nc + 3 * NR + rw * 12 * n1d +
+                        std::max<size_t>(3 * rw * scr, 8 * 9);
+  return nc * ncart4 + std::max(nc * ncart4, mainsz);
+}
+
+static int grad_roots(const DPair& P, const DPair& Q) { return (P.la + P.lb + Q.la + Q.lb + 3) / 2; }
+
+int grad_build(Handle* h, double cutint, GradPlan& plan) {
+  const int ns = h->sh.size();
+  const size_t budget = 224 * 1024 / 8;
+  std::vector<std::vector<GradItem>> byc(64);
+  std::vector<size_t> mx(64, 0);
+  std::vector<int> rwmin(64, 99);
+  for (int i = 0; i < ns; ++i)
+    for (int j = 0; j <= i; ++j) {
+      const int p = pair_id(i, j);
+      const double tij = h->tmax[(size_t)i * ns + j];
+      for (int k = 0; k <= i; ++k)
+        for (int l = 0; l <= (k == i ? j : k); ++l) {
+          if (tij * h->tmax[(size_t)k * ns + l] < cutint) continue;
+          const int q = pair_id(k, l);
+          const DPair &P = h->pairs[p], &Q = h->pairs[q];
+          // all four on one atom: the gradient contribution vanishes
+          if (P.atom_a == P.atom_b && P.atom_a == Q.atom_a && P.atom_a == Q.atom_b) continue;
+          const int deg = (i == j ? 1 : 2) * (k == l ? 1 : 2) * (p == q ? 1 : 2);
+          const int nijkl = P.nci * P.ncj * Q.nci * Q.ncj;
+          const int NR = grad_roots(P, Q);
+          int nc = nijkl, rw = NR;
+          while (nc > 1 && grad_group_smem(P, Q, nc, 1) > budget) nc = (nc + 1) / 2;
+          while (rw > 1 && grad_group_smem(P, Q, nc, rw) > budget) --rw;
+          if (grad_group_smem(P, Q, nc, rw) > budget) { h->err = "gradient quartet does not fit in shared memory"; return MG_ERR_ARG; }
+          const int key = (P.la + P.lb + 1) * 8 + (Q.la + Q.lb + 1);
+          for (int c0 = 0; c0 < nijkl; c0 += nc) {
+            GradItem it{p, q, c0, std::min(nijkl, c0 + nc), 0.5 * deg};
+            byc[key].push_back(it);
+            mx[key] = std::max(mx[key], grad_group_smem(P, Q, it.c1 - it.c0, rw));
+            rwmin[key] = std::min(rwmin[key], rw);
+          }
+        }
+    }
+  plan.items.clear();
+  plan.classes.clear();
+  for (int key = 0; key < 64; ++key) {
+    if (byc[key].empty()) continue;
+    auto& v = byc[key];
+    std::stable_sort(v.begin(), v.end(), [&](const GradItem& a, const GradItem& b) {
+      return (long long)h->pairs[a.p].np * h->pairs[a.q].np > (long long)h->pairs[b.p].np * h->pairs[b.q].np;
+    });
+    GradClass c;
+    c.nab1 = key / 8;
+    c.ncd1 = key % 8;
+    c.begin = plan.items.size();
+    c.count = v.size();
+    c.tpq = 64;
+    c.gsm = (int)((mx[key] + 1) & ~(size_t)1);
+    c.groups = (int)std::max<size_t>(1, std::min<size_t>(4, budget / c.gsm));
+    c.rw = rwmin[key];
+    plan.items.insert(plan.items.end(), v.begin(), v.end());
+    plan.classes.push_back(c);
+  }
+  cudaFree(plan.d_items);
+  plan.d_items = nullptr;
+  if (!plan.items.empty()) {
+    if (cudaMalloc(&plan.d_items, sizeof(GradItem) * plan.items.size()) != cudaSuccess) return MG_ERR_MEMORY;
+    cudaMemcpy(plan.d_items, plan.items.data(), sizeof(GradItem) * plan.items.size(), cudaMemcpyHostToDevice);
+  }
+  plan.cutint = cutint;
+  return 0;
+}
+
+int grad_run(Handle* h, const GradPlan& plan, const double* d_D, double* d_grad, cudaStream_t st) {
+  init_grad_tables(h);
+  RysArgsG ra;
+  for (int i = 0; i < MG_MAX_RYS; ++i) ra.m[i] = h->rys_meta[i];
+  ra.tab = h->d_rys;
+  cudaMemsetAsync(d_grad, 0, sizeof(double) * 3 * h->natom, st);
+  for (const GradClass& c : plan.classes) {
+    GradFn k = pick_grad(c.nab1, c.ncd1);
+    if (!k) { h->err = "gradient class out of range"; return MG_ERR_ARG; }
+    const int nblk = (c.count + c.groups - 1) / c.groups;
+    k<<<nblk, c.tpq * c.groups, sizeof(double) * (size_t)c.gsm * c.groups, st>>>(
+        plan.d_items + c.begin, c.count, h->d_pairs, h->d_prim, h->tot_np, h->d_coef, d_D, h->nbf, ra, d_grad, c.tpq,
+        c.gsm, c.rw);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (cudaGetLastError() != cudaSuccess) { h->err = "gradient kernel launch failed"; return MG_ERR_CUDA; }
+  }
+  return 0;
+}
+
+void grad_free(GradPlan* p) {
+  if (!p) return;
+  cudaFree(p->d_items);
+  delete p;
+}
+
+// Algorithmic FP64 flop count of a gradient plan (FMA = 2): per primitive
+// quartet the Rys roots (2 x 7 FMA per root and weight + 30), per root and
+// direction the 2D recursion (4 NI NJ), 2D-level HRR (2 (lb+1) NI NJ +
+// 2 (la+2)(lb+2) NJ ld) and derivative factors (8 n1d), the primitive 2-PDM
+// (2 nc ncart4 when nc > 1) and Assg1 (24 flops per Cartesian quartet and
+// root); per work item the 2-PDM and its spherical->Cartesian transform.
+double grad_plan_flops(const Handle* h, const GradPlan& plan) {
+  double f = 0;
+  for (const GradItem& it : plan.items) {
+    const DPair &P = h->pairs[it.p], &Q = h->pairs[it.q];
+    const int la = P.la, lb = P.lb, lc = Q.la, ld = Q.lb;
+    const int NI = la + lb + 2, NJ = lc + ld + 2, NR = (la + lb + lc + ld + 3) / 2;
+    const double ncart4 = (double)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+    const double nsp4 = (double)ncomp(la) * ncomp(lb) * ncomp(lc) * ncomp(ld);
+    const double n1d = (double)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
+    const int nc = it.c1 - it.c0;
+    const double per_prim = NR * 28.0 + 30.0 +
+                            3.0 * NR * (4.0 * NI * NJ + 2.0 * (lb + 1) * NI * NJ + 2.0 * (la + 2) * (lb + 2) * NJ * ld +
+                                        8.0 * n1d) +
+                            (nc > 1 ? 2.0 * nc * ncart4 : 0.0) + 24.0 * ncart4 * NR;
+    const double per_item = nc * nsp4 * 8.0 + 2.0 * nc * ncart4 * 4.0 * std::max(ncomp(la), ncomp(ld));
+    f += per_prim * (double)P.np * Q.np + per_item;
+  }
+  return f;
+}
+
+}  // namespace mg

@@ -1,0 +1,283 @@
+// Coulomb / exchange matrices from Cholesky vectors (the CHO_LK_SCF build,
+// fock_util/cho_lk_scf.F90:14) on the GPU.
+//
+//   D = C C^T (C: nbf x r, the Cholesky/orbital factor of the density, as
+//   ChoSCF_Drv passes it, scf/choscf_drv.F90:115-116)
+//   J_ab = sum_J L_ab,J V_J,  V_J = sum_cd L_cd,J D_cd     (cho_lk_scf.F90:442-449)
+//   K_ab = sum_J sum_k X_J[a,k] X_J[b,k],  X_J = L_J C      (cho_lk_scf.F90:507-830)
+//
+// Mixed path: vectors stored FP32; per block of vectors the rs-packed L_J
+// are unpacked straight into split BF16 pairs (hi + lo, hi = bf16(x),
+// lo = bf16(x - hi)); both GEMMs run as 3 BF16 tensor-core products
+// (hi*hi + hi*lo + lo*hi) with FP32 accumulation; each block's partial K is
+// FP32 over nb*r terms and is added to the FP64 result, so accumulation error
+// does not grow with the number of vectors.  J uses FP32 loads with FP64
+// accumulation.
+//
+// FP64 path ("plain FP64 GPU path"): vectors in FP64, per block of vectors
+// the rs-packed L_J are unpacked to dense symmetric nbf x nbf matrices, the
+// half-transform is one strided-batched DGEMM and K accumulates by DSYRK.
+// LK screening is not applied (dense tensor work is cheaper on the GPU than
+// the screening bookkeeping); the result equals the unscreened reference.
+#include <cublas_v2.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "mg_internal.h"
+
+namespace mg {
+
+// dw[t] = w_t D[a_t, b_t], w = 2 for a != b (both triangles), 1 on the diagonal
+__global__ void k_pack_density(const int* __restrict__ rs_a, const int* __restrict__ rs_b, int64_t nrs,
+                               const double* __restrict__ D, int n, double* __restrict__ dw) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nrs) return;
+  const int a = rs_a[t], b = rs_b[t];
+  dw[t] = (a == b ? 1.0 : 2.0) * D[(size_t)a * n + b];
+}
+
+// J[a,b] = J[b,a] = jrs[t]
+__global__ void k_unpack_sym(const int* __restrict__ rs_a, const int* __restrict__ rs_b, int64_t nrs,
+                             const double* __restrict__ v, int n, double* __restrict__ M) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nrs) return;
+  const int a = rs_a[t], b = rs_b[t];
+  M[(size_t)a * n + b] = v[t];
+  M[(size_t)b * n + a] = v[t];
+}
+
+// Lsq[J][a][b] = Lsq[J][b][a] = L[t + nrs*J] for a block of nb vectors
+__global__ void k_unpack_block(const int* __restrict__ rs_a, const int* __restrict__ rs_b, int64_t nrs,
+                               const double* __restrict__ L, int nb, int n, double* __restrict__ Lsq) {
+  int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (o >= nrs * nb) return;
+  const int64_t t = o % nrs;
+  const int64_t J = o / nrs;
+  const int a = rs_a[t], b = rs_b[t];
+  const double v = L[t + nrs * J];
+  double* M = Lsq + (size_t)J * n * n;
+  M[(size_t)a * n + b] = v;
+  M[(size_t)b * n + a] = v;
+}
+
+__global__ void k_symmetrize_lower(double* __restrict__ K, int n) {
+  int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (o >= (int64_t)n * n) return;
+  const int i = (int)(o % n), j = (int)(o / n);
+  if (i > j) K[(size_t)i * n + j] = K[(size_t)j * n + i];  // column-major lower -> full
+}
+
+static inline unsigned nb256(int64_t n) { return (unsigned)((n + 255) / 256); }
+
+struct JkWork {
+  int* d_rs_a = nullptr;
+  int* d_rs_b = nullptr;
+  int64_t nrs = 0;
+};
+
+int jk_fp64(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block) {
+  ChoState* c = h->cho;
+  const int64_t nrs = cho_nrs(c);
+  const int M = cho_nvec(c);
+  const int n = h->nbf;
+  cublasHandle_t cb = cho_cublas(c);
+  cublasSetStream(cb, st);
+  const int* d_ra = cho_rs_a_dev(c);
+  const int* d_rb = cho_rs_b_dev(c);
+  // scratch: dw (nrs), V (block), jrs (nrs), D (n*n), Lsq (block*n*n), X (n * block * r)
+  const size_t need = sizeof(double) * ((size_t)nrs * 2 + block + (size_t)n * n + (size_t)block * n * n +
+                                        (size_t)n * block * r);
+  double* ws = (double*)ws_get(h, need, st);
+  if (!ws) { h->err = "jk workspace allocation failed"; return MG_ERR_MEMORY; }
+  double* dw = ws;
+  double* jrs = dw + nrs;
+  double* V = jrs + nrs;
+  double* D = V + block;
+  double* Lsq = D + (size_t)n * n;
+  double* X = Lsq + (size_t)block * n * n;
+  const double one = 1.0, zero = 0.0;
+  // D = C C^T  (C column-major n x r); D symmetric so layout-agnostic
+  cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, r, &one, d_C, n, d_C, n, &zero, D, n);
+  k_pack_density<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, D, n, dw);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  cudaMemsetAsync(jrs, 0, sizeof(double) * nrs, st);
+  cudaMemsetAsync(d_K, 0, sizeof(double) * n * n, st);
+  for (int J0 = 0; J0 < M; J0 += block) {
+    const int nb = std::min(block, M - J0);
+    // vectors J0.. may straddle storage blocks: gather into a contiguous view
+    const double* Lb = cho_vec_ptr(c, J0, nb, st, h);
+    if (!Lb) { h->err = "vector block gather failed"; return MG_ERR_MEMORY; }
+    // Coulomb: V = L_b^T dw ; jrs += L_b V
+    cublasDgemv(cb, CUBLAS_OP_T, (int)nrs, nb, &one, Lb, (int)nrs, dw, 1, &zero, V, 1);
+    cublasDgemv(cb, CUBLAS_OP_N, (int)nrs, nb, &one, Lb, (int)nrs, V, 1, &one, jrs, 1);
+    // Exchange: X_J = Lsq_J C (n x r each), K += X X^T
+    k_unpack_block<<<nb256(nrs * nb), 256, 0, st>>>(d_ra, d_rb, nrs, Lb, nb, n, Lsq);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    cublasDgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_N, n, r, n, &one, Lsq, n, (long long)n * n, d_C, n, 0, &zero,
+                              X, n, (long long)n * r, nb);
+    cublasDsyrk(cb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, nb * r, &one, X, n, &one, d_K, n);
+  }
+  k_unpack_sym<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, jrs, n, d_J);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_symmetrize_lower<<<nb256((int64_t)n * n), 256, 0, st>>>(d_K, n);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError() == cudaSuccess ? 0 : MG_ERR_CUDA;
+}
+
+// ------------------------------------------------------------ mixed path
+// split x -> (hi, lo) BF16
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn(x);
+  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+// Lhi/Llo[J][a][b] (= [J][b][a]) from the FP32 rs vectors of a block
+__global__ void k_unpack_block_split(const int* __restrict__ rs_a, const int* __restrict__ rs_b, int64_t nrs,
+                                     const float* __restrict__ L, int nb, int n, __nv_bfloat16* __restrict__ Lhi,
+                                     __nv_bfloat16* __restrict__ Llo) {
+  int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (o >= nrs * nb) return;
+  const int64_t t = o % nrs;
+  const int64_t J = o / nrs;
+  const int a = rs_a[t], b = rs_b[t];
+  __nv_bfloat16 hi, lo;
+  split_bf16(L[t + nrs * J], hi, lo);
+  const size_t base = (size_t)J * n * n;
+  Lhi[base + (size_t)a * n + b] = hi;
+  Llo[base + (size_t)a * n + b] = lo;
+  Lhi[base + (size_t)b * n + a] = hi;
+  Llo[base + (size_t)b * n + a] = lo;
+}
+
+__global__ void k_split_f64(const double* __restrict__ x, int64_t n, __nv_bfloat16* __restrict__ hi,
+                            __nv_bfloat16* __restrict__ lo) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  __nv_bfloat16 h, l;
+  split_bf16((float)x[t], h, l);
+  hi[t] = h;
+  lo[t] = l;
+}
+
+__global__ void k_split_f32(const float* __restrict__ x, int64_t n, __nv_bfloat16* __restrict__ hi,
+                            __nv_bfloat16* __restrict__ lo) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  __nv_bfloat16 h, l;
+  split_bf16(x[t], h, l);
+  hi[t] = h;
+  lo[t] = l;
+}
+
+// V[J] = sum_t L[t,J] dw[t]   (FP32 loads, FP64 accumulation); one CTA per vector
+__global__ void k_jvec(const float* __restrict__ L, int64_t nrs, const double* __restrict__ dw, double* __restrict__ V) {
+  const int J = blockIdx.x;
+  const float* l = L + nrs * J;
+  double s = 0.0;
+  for (int64_t t = threadIdx.x; t < nrs; t += blockDim.x) s = fma((double)l[t], dw[t], s);
+  __shared__ double red[32];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if (threadIdx.x == 0) V[J] = s;
+  }
+}
+
+// jrs[t] += sum_J L[t,J] V[J]
+__global__ void k_jacc(const float* __restrict__ L, int64_t nrs, int nb, const double* __restrict__ V,
+                       double* __restrict__ jrs) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nrs) return;
+  double s = 0.0;
+  for (int J = 0; J < nb; ++J) s = fma((double)L[t + nrs * J], V[J], s);
+  jrs[t] += s;
+}
+
+__global__ void k_add_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, int64_t n) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < n) b[t] += (double)a[t];
+}
+
+int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block) {
+  ChoState* c = h->cho;
+  const int64_t nrs = cho_nrs(c);
+  const int M = cho_nvec(c);
+  const int n = h->nbf;
+  if (!cho_vec_ptr32(c, 0, 1)) {
+    int rc = cho_make_fp32(c, st);
+    if (rc) { h->err = "FP32 vector copy failed"; return rc; }
+  }
+  cublasHandle_t cb = cho_cublas(c);
+  cublasSetStream(cb, st);
+  const int* d_ra = cho_rs_a_dev(c);
+  const int* d_rb = cho_rs_b_dev(c);
+  // scratch (bytes): dw, jrs (f64 nrs), V (f64 block), D (f64 n*n), Chi/Clo (bf16 n*r),
+  // Lhi/Llo (bf16 block*n*n), X (f32 n*block*r), Xhi/Xlo (bf16 n*block*r), Kb (f32 n*n)
+  const size_t nn = (size_t)n * n, nbr = (size_t)n * block * r;
+  size_t need = 8 * ((size_t)2 * nrs + block + nn) + 2 * (2 * (size_t)n * r) + 2 * (2 * (size_t)block * nn) +
+                4 * nbr + 2 * (2 * nbr) + 4 * nn + 1024;
+  char* ws = (char*)ws_get(h, need, st);
+  if (!ws) { h->err = "jk workspace allocation failed"; return MG_ERR_MEMORY; }
+  auto take = [&](size_t bytes) { char* p = ws; ws += (bytes + 255) & ~(size_t)255; return (void*)p; };
+  double* dw = (double*)take(8 * nrs);
+  double* jrs = (double*)take(8 * nrs);
+  double* V = (double*)take(8 * block);
+  double* D = (double*)take(8 * nn);
+  __nv_bfloat16* Chi = (__nv_bfloat16*)take(2 * (size_t)n * r);
+  __nv_bfloat16* Clo = (__nv_bfloat16*)take(2 * (size_t)n * r);
+  __nv_bfloat16* Lhi = (__nv_bfloat16*)take(2 * (size_t)block * nn);
+  __nv_bfloat16* Llo = (__nv_bfloat16*)take(2 * (size_t)block * nn);
+  float* X = (float*)take(4 * nbr);
+  __nv_bfloat16* Xhi = (__nv_bfloat16*)take(2 * nbr);
+  __nv_bfloat16* Xlo = (__nv_bfloat16*)take(2 * nbr);
+  float* Kb = (float*)take(4 * nn);
+  const double one = 1.0, zero = 0.0;
+  const float onef = 1.0f, zerof = 0.0f;
+  cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, r, &one, d_C, n, d_C, n, &zero, D, n);
+  k_pack_density<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, D, n, dw);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_split_f64<<<nb256((int64_t)n * r), 256, 0, st>>>(d_C, (int64_t)n * r, Chi, Clo);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  cudaMemsetAsync(jrs, 0, 8 * nrs, st);
+  cudaMemsetAsync(d_K, 0, 8 * nn, st);
+  for (int J0 = 0; J0 < M; J0 += block) {
+    const int nb = std::min(block, M - J0);
+    const float* Lb = cho_vec_ptr32(c, J0, nb);
+    if (!Lb) { h->err = "vector block straddles storage blocks"; return MG_ERR_ARG; }
+    // Coulomb
+    k_jvec<<<nb, 256, 0, st>>>(Lb, nrs, dw, V);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    k_jacc<<<nb256(nrs), 256, 0, st>>>(Lb, nrs, nb, V, jrs);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    // Exchange: X_J = L_J C  (3 split products, FP32 accumulation)
+    k_unpack_block_split<<<nb256(nrs * nb), 256, 0, st>>>(d_ra, d_rb, nrs, Lb, nb, n, Lhi, Llo);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    const __nv_bfloat16* As[3] = {Lhi, Lhi, Llo};
+    const __nv_bfloat16* Bs[3] = {Chi, Clo, Chi};
+    for (int q = 0; q < 3; ++q)
+      cublasGemmStridedBatchedEx(cb, CUBLAS_OP_N, CUBLAS_OP_N, n, r, n, &onef, As[q], CUDA_R_16BF, n, (long long)nn,
+                                 Bs[q], CUDA_R_16BF, n, 0, q == 0 ? &zerof : &onef, X, CUDA_R_32F, n,
+                                 (long long)n * r, nb, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
+    // K_b = X X^T over this block (3 split products), then K += K_b in FP64
+    k_split_f32<<<nb256((int64_t)n * nb * r), 256, 0, st>>>(X, (int64_t)n * nb * r, Xhi, Xlo);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    const __nv_bfloat16* Ps[3] = {Xhi, Xhi, Xlo};
+    const __nv_bfloat16* Qs[3] = {Xhi, Xlo, Xhi};
+    for (int q = 0; q < 3; ++q)
+      cublasGemmEx(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, nb * r, &onef, Ps[q], CUDA_R_16BF, n, Qs[q], CUDA_R_16BF, n,
+                   q == 0 ? &zerof : &onef, Kb, CUDA_R_32F, n, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
+    k_add_f32_to_f64<<<nb256((int64_t)nn), 256, 0, st>>>(Kb, d_K, (int64_t)nn);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+  k_unpack_sym<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, jrs, n, d_J);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError() == cudaSuccess ? 0 : MG_ERR_CUDA;
+}
+
+}  // namespace mg

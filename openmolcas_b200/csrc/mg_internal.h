@@ -2,14 +2,20 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <string>
 #include <vector>
+
+#include "../../include/molgpu.h"
 
 #define MG_MAX_RYS 9
 #define MG_MAX_L 3
 
 namespace mg {
+
+// number of kernels of this library launched so far (all handles)
+extern std::atomic<long long> g_launches;
 
 // Per-order metadata of the Rys root/weight table (constant memory).
 struct RysMeta {
@@ -46,6 +52,19 @@ struct EriItem {
   long long out_off;
 };
 
+// Launch plan of one ERI class (eri.cu) and per-class statistics.
+struct ClassPlan {
+  int tpq, PAB, PCD, gsm;
+  size_t smem;
+};
+struct ClassStats {
+  int max_acc = 0, max_nef = 0, max_tmp = 0, max_nij = 0, max_npab = 0, max_npcd = 0, max_cab = 0, max_ccd = 0;
+};
+struct EriClass {
+  int nab, ncd, begin, count;
+  ClassPlan plan;
+};
+
 struct ShellH {
   double A[3];
   int l, np, nc, atom, off, ncomp;
@@ -68,6 +87,7 @@ struct Handle {
   DPair* d_pairs = nullptr;
   double* d_prim = nullptr;   // SoA: [7][tot_np]: zeta, kappa, Px, Py, Pz, alpha, beta
   int tot_np = 0;
+  long long prim_kept = 0, prim_total = 0;  // primitive pairs after prescreening
   double* d_coef = nullptr;
   double* d_hrr = nullptr;
   double* d_rys = nullptr;
@@ -77,7 +97,53 @@ struct Handle {
   double* d_tmax = nullptr;
   Workspace ws;
   std::string err;
+  struct ChoState* cho = nullptr;  // Cholesky vectors of the current basis
+  struct GradPlan* grad = nullptr; // gradient work list (per Schwarz threshold)
 };
+
+struct GradItem {
+  int p, q;      // bra / ket canonical pairs
+  int c0, c1;    // contracted ijkl range
+  double scale;  // 1/2 * degeneracy
+};
+struct GradClass {
+  int nab1, ncd1, begin, count, tpq, gsm, groups, rw;
+};
+struct GradPlan {
+  std::vector<GradItem> items;
+  std::vector<GradClass> classes;
+  GradItem* d_items = nullptr;
+  double cutint = -1;
+};
+int grad_build(Handle* h, double cutint, GradPlan& plan);
+int grad_run(Handle* h, const GradPlan& plan, const double* d_D, double* d_grad, cudaStream_t st);
+void grad_free(GradPlan* p);
+double grad_plan_flops(const Handle* h, const GradPlan& plan);
+
+struct ChoState;
+struct ChoCfgH {
+  double thrcom, span;
+  int minqual, maxqual, maxvec;
+};
+int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st, std::string& err);
+int cho_make_fp32(ChoState* c, cudaStream_t st);
+void cho_free(ChoState* c);
+int64_t cho_nrs(const ChoState* c);
+int cho_nvec(const ChoState* c);
+int cho_npass(const ChoState* c);
+void cho_pivots(const ChoState* c, int32_t* piv, int32_t* pass_of);
+void cho_rs_list(const ChoState* c, int32_t* a, int32_t* b, int32_t* sp);
+int cho_copy_vectors(const ChoState* c, int first, int count, double* d_out, cudaStream_t st);
+const double* cho_diag0(const ChoState* c);
+typedef struct cublasContext* cublasHandle_t;
+cublasHandle_t cho_cublas(ChoState* c);
+const int* cho_rs_a_dev(const ChoState* c);
+const int* cho_rs_b_dev(const ChoState* c);
+const double* cho_vec_ptr(const ChoState* c, int J0, int nb, cudaStream_t st, Handle* h);
+const float* cho_vec_ptr32(const ChoState* c, int J0, int nb);
+int cho_vec_block();
+int jk_fp64(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block);
+int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block);
 
 inline int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 inline int ncart_cum(int l) { return l <= 0 ? 0 : l * (l + 1) * (l + 2) / 6; }
@@ -91,7 +157,14 @@ std::vector<double> hrr_matrix(const Handle* h, int la, int lb, const double* A,
 int setup_pairs(Handle* h);
 void* ws_get(Handle* h, size_t bytes, cudaStream_t st);
 
-// device launchers (eri.cu)
+// ERI work lists (capi.cu) and launchers (eri.cu)
+ClassPlan eri_plan(int nab, int ncd, const ClassStats& cs);
+int eri_launch_class(Handle* h, const EriItem* d_items, int nitems, int nab, int ncd, const ClassPlan& pl, double* out,
+                     cudaStream_t st);
+int build_eri_items(Handle* h, const int32_t* q4, int64_t nq, const int64_t* offsets, std::vector<EriItem>& items,
+                    std::vector<EriClass>& classes);
+int run_eri_items(Handle* h, const std::vector<EriItem>& items, const std::vector<EriClass>& classes, double* d_out,
+                  cudaStream_t st);
 int eri_run(Handle* h, const EriItem* d_items, const std::vector<int>& class_begin, const std::vector<int>& class_nab,
             const std::vector<int>& class_ncd, const std::vector<int>& class_np, const std::vector<size_t>& class_smem,
             double* out, cudaStream_t st);

@@ -47,6 +47,15 @@ def lib():
     L.mg_schwarz.argtypes = [vp, d]
     L.mg_eri_quartets_size.argtypes = [vp, i32, C.c_int64, i64]
     L.mg_eri_quartets.argtypes = [vp, i32, C.c_int64, i64, C.c_void_p, C.c_void_p]
+    L.mg_cho_default.argtypes = [C.c_void_p]
+    L.mg_cho_drv.argtypes = [vp, C.c_void_p, C.c_void_p]
+    L.mg_cho_info.argtypes = [vp, i64, i, i]
+    L.mg_cho_pivots.argtypes = [vp, i32, i32]
+    L.mg_cho_rs_list.argtypes = [vp, i32, i32, i32]
+    L.mg_cho_copy_vectors.argtypes = [vp, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    L.mg_cho_diag.argtypes = [vp, C.c_void_p, C.c_void_p]
+    L.mg_drvg1.argtypes = [vp, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
+    L.mg_cho_jk.argtypes = [vp, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     _lib = L
     return L
 
@@ -57,6 +66,12 @@ def _p(a, t=C.c_double):
 
 def _stream(device):
     return C.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+class ChoCfg(C.Structure):
+    """mg_cho_cfg: Cholesky thresholds (defaults of cho_inp.F90 / cholesky.F90)."""
+    _fields_ = [("thrcom", C.c_double), ("span", C.c_double), ("minqual", C.c_int), ("maxqual", C.c_int),
+                ("maxvec", C.c_int)]
 
 
 class MolGpu:
@@ -126,6 +141,87 @@ class MolGpu:
         t = np.empty(self.nshell * self.nshell)
         self._check(self.L.mg_schwarz(self.h, _p(t)), "mg_schwarz")
         return t.reshape(self.nshell, self.nshell)
+
+
+    # -------------------------------------------------------- Cholesky
+    def cho_drv(self, thrcom: float = 1e-4, span: float = 1e-2, minqual: int = 50, maxqual: int = 100,
+                maxvec: int = 0):
+        """Cho_Drv (algorithm 4): decompose the ERI matrix; vectors stay on the GPU."""
+        cfg = ChoCfg()
+        self.L.mg_cho_default(C.byref(cfg))
+        cfg.thrcom, cfg.span, cfg.minqual, cfg.maxqual, cfg.maxvec = thrcom, span, minqual, maxqual, maxvec
+        self._check(self.L.mg_cho_drv(self.h, C.byref(cfg), _stream(self.device)), "mg_cho_drv")
+        return self.cho_info()
+
+    def cho_info(self):
+        nrs = C.c_int64()
+        nvec = C.c_int()
+        npass = C.c_int()
+        self._check(self.L.mg_cho_info(self.h, C.byref(nrs), C.byref(nvec), C.byref(npass)), "mg_cho_info")
+        return dict(nrs=nrs.value, M=nvec.value, npass=npass.value)
+
+    def cho_pivots(self):
+        M = self.cho_info()["M"]
+        piv = np.empty(M, np.int32)
+        pas = np.empty(M, np.int32)
+        self._check(self.L.mg_cho_pivots(self.h, _p(piv, C.c_int32), _p(pas, C.c_int32)), "mg_cho_pivots")
+        return piv, pas
+
+    def cho_rs_list(self):
+        n = self.cho_info()["nrs"]
+        a, b, sp = (np.empty(n, np.int32) for _ in range(3))
+        self._check(self.L.mg_cho_rs_list(self.h, _p(a, C.c_int32), _p(b, C.c_int32), _p(sp, C.c_int32)),
+                    "mg_cho_rs_list")
+        return a, b, sp
+
+    def cho_vectors(self, first: int = 0, count: int | None = None) -> torch.Tensor:
+        """Vectors [first, first+count) as a (count, nrs) FP64 device tensor."""
+        info = self.cho_info()
+        if count is None:
+            count = info["M"] - first
+        out = torch.empty((count, info["nrs"]), dtype=torch.float64, device=f"cuda:{self.device}")
+        self._check(self.L.mg_cho_copy_vectors(self.h, first, count, C.c_void_p(out.data_ptr()),
+                                               _stream(self.device)), "mg_cho_copy_vectors")
+        return out
+
+    def cho_diag(self) -> torch.Tensor:
+        out = torch.empty(self.cho_info()["nrs"], dtype=torch.float64, device=f"cuda:{self.device}")
+        self._check(self.L.mg_cho_diag(self.h, C.c_void_p(out.data_ptr()), _stream(self.device)), "mg_cho_diag")
+        return out
+
+
+    # ------------------------------------------------------------- J/K
+    PREC_FP64 = 0
+    PREC_MIXED = 1
+
+    def cho_jk(self, Cfac: torch.Tensor, precision: int = 0, J: torch.Tensor | None = None,
+               K: torch.Tensor | None = None):
+        """CHO_LK_SCF for one density D = C C^T: returns (J, K), nbf x nbf device tensors."""
+        dev = f"cuda:{self.device}"
+        # column-major n x r == row-major r x n
+        Cc = Cfac.to(device=dev, dtype=torch.float64).t().contiguous()
+        n, r = self.nbf, Cfac.shape[1]
+        if Cfac.shape[0] != n:
+            raise MolGpuError(f"C must have {n} rows")
+        if J is None:
+            J = torch.empty((n, n), dtype=torch.float64, device=dev)
+        if K is None:
+            K = torch.empty((n, n), dtype=torch.float64, device=dev)
+        self._check(self.L.mg_cho_jk(self.h, C.c_void_p(Cc.data_ptr()), r, C.c_void_p(J.data_ptr()),
+                                     C.c_void_p(K.data_ptr()), precision, _stream(self.device)), "mg_cho_jk")
+        return J, K
+
+    # -------------------------------------------------------- gradient
+    def drvg1(self, D: torch.Tensor, cutint: float = 1e-12, out: torch.Tensor | None = None) -> torch.Tensor:
+        """Drvg1: two-electron gradient dE/dR (natom x 3) of E = 1/2 tr(DJ) - 1/4 tr(DK)."""
+        D = D.to(device=f"cuda:{self.device}", dtype=torch.float64).contiguous()
+        if D.shape != (self.nbf, self.nbf):
+            raise MolGpuError(f"density must be {self.nbf}x{self.nbf}")
+        if out is None:
+            out = torch.empty((self.natom, 3), dtype=torch.float64, device=f"cuda:{self.device}")
+        self._check(self.L.mg_drvg1(self.h, C.c_void_p(D.data_ptr()), cutint, C.c_void_p(out.data_ptr()),
+                                    _stream(self.device)), "mg_drvg1")
+        return out
 
 
 def unique_quartets(nshell: int, tmax: np.ndarray | None = None, cutint: float = 0.0) -> np.ndarray:

@@ -1125,7 +1125,13 @@ int or_cho_jk(void* h, const double* L, int M, const double* C, int r, double* J
 // dE/dR of E = 1/2 tr(DJ) - 1/4 tr(DK) with exact ERIs (Drvg1 path),
 // D full nbf x nbf symmetric; grad[3*natom].  Quartets screened by
 // tmax(ij) tmax(kl) < cutint.
+int or_grad_sampled(void* h, const double* D, double cutint, int stride, double* grad, int64_t* nquartets);
 int or_grad(void* h, const double* D, double cutint, double* grad) {
+  return or_grad_sampled(h, D, cutint, 1, grad, nullptr);
+}
+// every stride-th unique quartet only (timing samples of the CPU baseline);
+// *nquartets receives the total number of unique quartets after screening
+int or_grad_sampled(void* h, const double* D, double cutint, int stride, double* grad, int64_t* nquartets) {
   Basis& bs = ((Handle*)h)->bs;
   if (bs.tmax.empty()) compute_tmax(bs);
   int ns = bs.sh.size();
@@ -1138,6 +1144,12 @@ int or_grad(void* h, const double* D, double cutint, double* grad) {
           int deg = (i == j ? 1 : 2) * (k == l ? 1 : 2) * ((i == k && j == l) ? 1 : 2);
           qs.push_back({i, j, k, l, deg});
         }
+  if (nquartets) *nquartets = qs.size();
+  if (stride > 1) {
+    std::vector<std::array<int, 5>> sub;
+    for (size_t t = 0; t < qs.size(); t += stride) sub.push_back(qs[t]);
+    qs.swap(sub);
+  }
   int na = bs.natom;
   std::fill(grad, grad + 3 * na, 0.0);
 #pragma omp parallel

@@ -49,6 +49,8 @@ def lib():
         L.or_cholesky.argtypes = [vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, i, i, i, d, i]
         L.or_cho_jk.argtypes = [vp, d, C.c_int, d, C.c_int, d, d]
         L.or_grad.argtypes = [vp, d, C.c_double, d]
+        L.or_grad_sampled.argtypes = [vp, d, C.c_double, C.c_int, d, C.POINTER(C.c_int64)]
+        L.or_num_threads.restype = C.c_int
         rc = L.or_load_rys(TABLE.encode())
         if rc != 0:
             raise RuntimeError(f"oracle: cannot load Rys table ({rc})")
@@ -181,6 +183,19 @@ ERI_REL_S = 1e-13
 
 def eri_tolerance(S):
     return ERI_ABS_TOL + ERI_REL_S * S
+
+
+def grad_sampled(orc, D, cutint, stride):
+    """Oracle gradient over every stride-th unique quartet; returns (grad, nquartets)."""
+    Dc = np.ascontiguousarray(D, dtype=np.float64)
+    g = np.empty(3 * orc.mol.natom)
+    nq = C.c_int64(0)
+    lib().or_grad_sampled(orc.h, _p(Dc), cutint, stride, _p(g), C.byref(nq))
+    return g.reshape(-1, 3), nq.value
+
+
+def num_threads():
+    return lib().or_num_threads()
 
 
 def energy_from_full(eri, D):
