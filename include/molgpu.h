@@ -67,6 +67,25 @@ int mg_eri_quartets_size(mg_handle* h, const int32_t* quartets, int64_t nq, int6
 int mg_eri_quartets(mg_handle* h, const int32_t* quartets, int64_t nq, const int64_t* offsets, double* d_out,
                     void* stream);
 
+/* Allocation-free variant of mg_eri_quartets.  No counterpart in the
+ * reference.  For callers that cannot let the library allocate device memory
+ * during a call: programs that reserve all device memory in their own pool
+ * up front, frameworks whose caching allocator already holds it, or code that
+ * must not get the device-wide synchronisation of cudaFree between its
+ * stream-ordered work.  Same arguments and output as mg_eri_quartets; the
+ * work list is staged in a fixed 1.5 MiB device array inside the library
+ * (held by every GPU that loads the library until exit), so no cudaMalloc or
+ * cudaFree is called.  At most 65536 work items per call (one per quartet,
+ * more for quartets with large contracted blocks); larger lists are rejected
+ * with MG_ERR_ARG.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and should come before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (different
+ * streams, or different threads) race on it; calls on one stream are
+ * ordered.  Nothing in the array needs to start at zero: each call overwrites
+ * the entries it uses and every output element is written. */
+int mg_eri_quartets_noalloc(mg_handle* h, const int32_t* quartets, int64_t nq, const int64_t* offsets,
+                            double* d_out, void* stream);
+
 /* ---------------------------------------------------------------------
  * Cholesky decomposition of the ERI matrix (replaces Cho_Drv / Cho_Drv_Inner
  * with the default algorithm 4, cholesky_util/cho_drv.F90:14,

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmolgpu.so")
-SOURCES = ["basis_host.cu", "eri.cu", "cholesky.cu", "grad.cu", "jk.cu", "capi.cu"]
+SOURCES = ["basis_host.cu", "eri.cu", "cholesky.cu", "grad.cu", "jk.cu", "capi.cu", "eri_noalloc.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
