@@ -80,7 +80,7 @@ __device__ __forceinline__ void group_sync(int g, int tpq) {
 }
 
 template <int NAB, int NCD>
-__global__ void __launch_bounds__(256) eri_kernel(const EriItem* __restrict__ items, int nitems,
+__global__ void __launch_bounds__(256, 3) eri_kernel(const EriItem* __restrict__ items, int nitems,
                                                   const DPair* __restrict__ pairs, const double* __restrict__ prim,
                                                   int tot_np, const double* __restrict__ coef,
                                                   const double* __restrict__ hrr, RysArgs ra, double* __restrict__ out,
@@ -165,26 +165,18 @@ __global__ void __launch_bounds__(256) eri_kernel(const EriItem* __restrict__ it
           const int d = job % 3, tr = job / 3, r = tr % NR, t = tr / NR;
           const double* c = cf + (t * NR + r) * NCF;
           const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
-          double I[NI][NJ];
-          I[0][0] = d == 2 ? c[9] : 1.0;
-          if (NI > 1) I[1][0] = C00 * I[0][0];
-#pragma unroll
-          for (int i = 1; i < NI - 1; ++i) I[i + 1][0] = C00 * I[i][0] + i * B10 * I[i - 1][0];
-#pragma unroll
-          for (int j = 0; j < NJ - 1; ++j) {
-#pragma unroll
-            for (int i = 0; i < NI; ++i) {
-              double v = D00 * I[i][j];
-              if (j > 0) v += j * B01 * I[i][j - 1];
-              if (i > 0) v += i * B00 * I[i - 1][j];
-              I[i][j + 1] = v;
-            }
-          }
+          // recursion written straight to shared memory (keeps registers low)
           double* gg = G + (t * 3 + d) * G1 + r * NI * NJ;
-#pragma unroll
-          for (int i = 0; i < NI; ++i)
-#pragma unroll
-            for (int j = 0; j < NJ; ++j) gg[i * NJ + j] = I[i][j];
+          gg[0] = d == 2 ? c[9] : 1.0;
+          if (NI > 1) gg[NJ] = C00 * gg[0];
+          for (int i = 1; i < NI - 1; ++i) gg[(i + 1) * NJ] = C00 * gg[i * NJ] + i * B10 * gg[(i - 1) * NJ];
+          for (int j = 0; j < NJ - 1; ++j)
+            for (int i = 0; i < NI; ++i) {
+              double v = D00 * gg[i * NJ + j];
+              if (j > 0) v += j * B01 * gg[i * NJ + j - 1];
+              if (i > 0) v += i * B00 * gg[(i - 1) * NJ + j];
+              gg[i * NJ + j + 1] = v;
+            }
         }
         group_sync(g, tpq);
         // ---- 2a: [e0|f0] per primitive quartet
@@ -306,32 +298,36 @@ static KernelFn pick(int nab, int ncd) {
 ClassPlan eri_plan(int nab, int ncd, const ClassStats& cs) {
   const int NR = (nab + ncd) / 2 + 1;
   const int G1 = NR * (nab + 1) * (ncd + 1);
-  const size_t budget = 224 * 1024 / 8;  // doubles per CTA
   ClassPlan pl{0, 0, 0, 0, 0};
   auto need = [&](int pab, int pcd) {
     const size_t nt = (size_t)pab * pcd;
     const size_t tile = (size_t)cs.max_nij * pcd * cs.max_nef + nt * (NR * 10 + 3 * G1 + cs.max_nef);
     return (size_t)cs.max_acc + cs.max_cab + cs.max_ccd + std::max(tile, (size_t)cs.max_tmp);
   };
-  int pab = std::max(1, std::min(cs.max_npab, 64));
-  int pcd = std::max(1, std::min(cs.max_npcd, std::max(1, 256 / pab)));
-  const int width = std::max({cs.max_acc, pab * pcd * cs.max_nef / 2, pab * pcd * NR * 3});
-  int tpq = width <= 48 ? 32 : width <= 160 ? 64 : width <= 640 ? 128 : 256;
-  for (; tpq <= 256; tpq *= 2) {
-    const int groups = 256 / tpq;
-    const size_t gbudget = budget / groups;
-    int a = pab, c = pcd;
-    while (need(a, c) > gbudget && (a > 1 || c > 1)) {
-      if (c > 1) c = (c + 1) / 2;
-      else a = (a + 1) / 2;
-    }
-    if (need(a, c) <= gbudget) {
-      pl.tpq = tpq;
-      pl.PAB = a;
-      pl.PCD = c;
-      pl.gsm = (int)((need(a, c) + 1) & ~(size_t)1);
-      pl.smem = 8 * (size_t)pl.gsm * groups;
-      return pl;
+  // Shared-memory budget per CTA: 72 KB first (3 CTAs per SM), larger only
+  // when the class needs it.
+  const size_t budgets[3] = {72 * 1024 / 8, 112 * 1024 / 8, 224 * 1024 / 8};
+  for (size_t budget : budgets) {
+    int pab = std::max(1, std::min(cs.max_npab, 64));
+    int pcd = std::max(1, std::min(cs.max_npcd, std::max(1, 256 / pab)));
+    const int width = std::max({cs.max_acc, pab * pcd * cs.max_nef / 2, pab * pcd * NR * 3});
+    int tpq = width <= 48 ? 32 : width <= 160 ? 64 : width <= 640 ? 128 : 256;
+    for (; tpq <= 256; tpq *= 2) {
+      const int groups = 256 / tpq;
+      const size_t gbudget = budget / groups;
+      int a = pab, c = pcd;
+      while (need(a, c) > gbudget && (a > 1 || c > 1)) {
+        if (c > 1) c = (c + 1) / 2;
+        else a = (a + 1) / 2;
+      }
+      if (need(a, c) <= gbudget) {
+        pl.tpq = tpq;
+        pl.PAB = a;
+        pl.PCD = c;
+        pl.gsm = (int)((need(a, c) + 1) & ~(size_t)1);
+        pl.smem = 8 * (size_t)pl.gsm * groups;
+        return pl;
+      }
     }
   }
   return pl;  // PAB == 0: does not fit

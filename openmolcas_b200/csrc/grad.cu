@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
                                                    const DPair* __restrict__ pairs, const double* __restrict__ prim,
                                                    int tot_np, const double* __restrict__ coef,
                                                    const double* __restrict__ Dm, int nbf, RysArgsG ra,
-                                                   double* __restrict__ grad, int tpq, int gsm, int rw) {
+                                                   double* __restrict__ grad, int tpq, int gsm, int PAB, int PCD) {
   constexpr int NR = (NAB1 + NCD1 + 1) / 2;
   constexpr int NI = NAB1 + 1, NJ = NCD1 + 1;
   extern __shared__ double smem_all[];
@@ -117,45 +117,49 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
   const int nca = d_ncart(la), ncb = d_ncart(lb), ncc = d_ncart(lc), ncd = d_ncart(ld);
   const int nsa = d_ncomp(la), nsb = d_ncomp(lb), nsc = d_ncomp(lc), nsd = d_ncomp(ld);
   const int ncart4 = nca * ncb * ncc * ncd;
-  const int nc = it.c1 - it.c0;
   const int nij = P.nci * P.ncj;
+  const int nklc = it.c1 - it.c0;  // ket contracted pairs [c0, c1)
+  const int nc = nij * nklc;
+  const bool multi = nc > 1;
+  const int npab = P.np, npcd = Q.np;
   const int n1d = (la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
   const int scr = NI * (lb + 2) * NJ + (la + 2) * (lb + 2) * NJ * (ld + 1);
-  // shared layout (doubles):  Gam | union{ stage-0 temp | Gp, cf, CO, G2, F, S }
-  // Gp is only materialised with more than one contracted quartet (else the
-  // single coefficient is folded into the sum).  F and S hold rw roots.
-  double* Gam = sm;                               // nc * ncart4
-  double* Tmp = Gam + nc * ncart4;                // stage-0 temp (nc * ncart4)
-  double* Gp = Tmp;                               // ncart4 (nc > 1)
-  double* cf = Tmp + (nc > 1 ? ncart4 : 0);       // NR * 10 + 4
-  double* CO = cf + NR * 10 + 4;                  // nc
-  double* G2 = CO + nc;                           // 3 * NR * NI * NJ  (unused slot kept for layout)
-  double* F = G2 + 3 * NR;                        // rw * 3 * 4 * n1d
-  double* S = F + rw * 12 * n1d;                  // 3 * rw * scr
+  const int NT = PAB * PCD;
+  const int CFT = NR * 10 + 4;  // per-quartet coefficient record
+  // shared layout: Gam | Cab | Ccd | Y | union{ stage-0 temp | tile: cf, Gp, F, S }
+  double* Gam = sm;                            // nc * ncart4, index il + nc * abcd
+  double* Cab = Gam + nc * ncart4;             // nij * npab
+  double* Ccd = Cab + nij * npab;              // nklc * npcd
+  double* Y = Ccd + nklc * npcd;               // nij * PCD * ncart4 (multi only)
+  double* U0 = Y + (multi ? nij * PCD * ncart4 : 0);
+  double* Tmp = U0;                            // stage-0 temp (nc * ncart4)
+  double* cf = U0;                             // NT * CFT
+  double* Gp = cf + NT * CFT;                  // NT * ncart4 (multi only)
+  double* F = Gp + (multi ? NT * ncart4 : 0);  // NT * NR * 12 * n1d
+  double* S = F + NT * NR * 12 * n1d;          // NT * 3 * NR * scr
+  for (int o = tid; o < nij * npab; o += tpq) Cab[o] = coef[P.coef_off + o];
+  for (int o = tid; o < nklc * npcd; o += tpq) Ccd[o] = coef[Q.coef_off + (size_t)it.c0 * npcd + o];
   // ---- stage 0: contracted 2-PDM (PGet1), spherical, then -> Cartesian
   {
     const int nsp4 = nsa * nsb * nsc * nsd;
     for (int o = tid; o < nc * nsp4; o += tpq) {
       const int il = o % nc, r1 = o / nc;
       const int sa = r1 % nsa, r2 = r1 / nsa, sb = r2 % nsb, r3 = r2 / nsb, sc = r3 % nsc, sd = r3 / nsc;
-      const int ijkl = it.c0 + il;
+      const int ijkl = nij * it.c0 + il;
       const int kl = ijkl / nij, ij = ijkl - kl * nij;
       const int ki = ij % P.nci, kj = ij / P.nci, kk = kl % Q.nci, kq = kl / Q.nci;
       const int pa = P.ao_a + sa * P.nci + ki, pb = P.ao_b + sb * P.ncj + kj;
       const int pc = Q.ao_a + sc * Q.nci + kk, pd = Q.ao_b + sd * Q.ncj + kq;
-      const double v = Dm[(size_t)pa * nbf + pb] * Dm[(size_t)pc * nbf + pd] -
-                       0.25 * (Dm[(size_t)pa * nbf + pc] * Dm[(size_t)pb * nbf + pd] +
-                               Dm[(size_t)pa * nbf + pd] * Dm[(size_t)pb * nbf + pc]);
-      Tmp[o] = v;
+      Tmp[o] = Dm[(size_t)pa * nbf + pb] * Dm[(size_t)pc * nbf + pd] -
+               0.25 * (Dm[(size_t)pa * nbf + pc] * Dm[(size_t)pb * nbf + pd] +
+                       Dm[(size_t)pa * nbf + pd] * Dm[(size_t)pb * nbf + pc]);
     }
     gsync(g, tpq);
-    // four one-index transforms: d, c, b, a (layout il + nc*(a + A*(b + B*(c + C*d))))
     const double* Sd = c_sph + c_sph_off[ld];
     const double* Sc = c_sph + c_sph_off[lc];
     const double* Sb = c_sph + c_sph_off[lb];
     const double* Sa = c_sph + c_sph_off[la];
-    // d: [il][sa][sb][sc][sd] -> [il][sa][sb][sc][cd]
-    {
+    {  // d: [il][sa][sb][sc][sd] -> [il][sa][sb][sc][cd]   (Tmp -> Gam)
       const int inner = nc * nsa * nsb * nsc;
       for (int o = tid; o < inner * ncd; o += tpq) {
         const int in = o % inner, cd = o / inner;
@@ -165,8 +169,7 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
       }
       gsync(g, tpq);
     }
-    // c: [il][sa][sb][sc][cd] -> [il][sa][sb][cc][cd]
-    {
+    {  // c  (Gam -> Tmp)
       const int inner = nc * nsa * nsb;
       for (int o = tid; o < inner * ncc * ncd; o += tpq) {
         const int in = o % inner, r1 = o / inner, cc = r1 % ncc, cd = r1 / ncc;
@@ -176,8 +179,7 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
       }
       gsync(g, tpq);
     }
-    // b
-    {
+    {  // b  (Tmp -> Gam)
       const int inner = nc * nsa;
       const int outer = ncc * ncd;
       for (int o = tid; o < inner * ncb * outer; o += tpq) {
@@ -188,8 +190,7 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
       }
       gsync(g, tpq);
     }
-    // a
-    {
+    {  // a  (Gam -> Tmp -> Gam)
       const int outer = ncb * ncc * ncd;
       for (int o = tid; o < nc * nca * outer; o += tpq) {
         const int il = o % nc, r1 = o / nc, ca = r1 % nca, ou = r1 / nca;
@@ -209,92 +210,93 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
   const double C0 = Q.A[0], C1 = Q.A[1], C2 = Q.A[2];
   const double ABx[3] = {P.A[0] - P.B[0], P.A[1] - P.B[1], P.A[2] - P.B[2]};
   const double CDx[3] = {Q.A[0] - Q.B[0], Q.A[1] - Q.B[1], Q.A[2] - Q.B[2]};
-  const int npab = P.np, npcd = Q.np;
-  const long long ntot = (long long)npab * npcd;
   const int ca0 = d_ccum(la), cb0 = d_ccum(lb), cc0 = d_ccum(lc), cd0 = d_ccum(ld);
-  for (long long tq = 0; tq < ntot; ++tq) {
-    const int pcd = (int)(tq / npab), pab = (int)(tq - (long long)pcd * npab);
-    const int ia = P.prim_off + pab, ic = Q.prim_off + pcd;
-    // ---- (1) roots (thread r), contraction coefficients (threads < nc)
-    if (tid < NR) {
-      const int r = tid;
-      const double zeta = prim[ia], eta = prim[ic];
-      const double px = prim[2 * tot_np + ia], py = prim[3 * tot_np + ia], pz = prim[4 * tot_np + ia];
-      const double qx = prim[2 * tot_np + ic], qy = prim[3 * tot_np + ic], qz = prim[4 * tot_np + ic];
-      const double ze = zeta + eta, zei = 1.0 / ze, rho = zeta * eta * zei;
-      const double dx = px - qx, dy = py - qy, dz = pz - qz;
-      const double T = rho * (dx * dx + dy * dy + dz * dz);
-      const double fact = prim[tot_np + ia] * prim[tot_np + ic] * sqrt(zei);
-      double x, w;
-      rys_one<NR>(ra, T, r, x, w);
-      const double U2 = x * zei;
-      double* c = cf + r * 10;
-      c[0] = 0.5 * U2;
-      c[1] = 0.5 * (1.0 - U2 * eta) / zeta;
-      c[2] = 0.5 * (1.0 - U2 * zeta) / eta;
-      c[3] = px - A0 - eta * U2 * dx;
-      c[4] = py - A1 - eta * U2 * dy;
-      c[5] = pz - A2 - eta * U2 * dz;
-      c[6] = qx - C0 + zeta * U2 * dx;
-      c[7] = qy - C1 + zeta * U2 * dy;
-      c[8] = qz - C2 + zeta * U2 * dz;
-      c[9] = w * fact;
-      if (r == 0) {
-        cf[NR * 10 + 0] = 2.0 * prim[5 * tot_np + ia];  // 2 alpha
-        cf[NR * 10 + 1] = 2.0 * prim[6 * tot_np + ia];  // 2 beta
-        cf[NR * 10 + 2] = 2.0 * prim[5 * tot_np + ic];  // 2 gamma
-      }
-    }
-    for (int il = tid; il < nc; il += tpq) {
-      const int ijkl = it.c0 + il;
-      const int kl = ijkl / nij, ij = ijkl - kl * nij;
-      CO[il] = coef[P.coef_off + (size_t)ij * npab + pab] * coef[Q.coef_off + (size_t)kl * npcd + pcd];
-    }
+  const int LB2 = lb + 2, LD1 = ld + 1;
+  for (int pcd0 = 0; pcd0 < npcd; pcd0 += PCD) {
+    const int npc = min(PCD, npcd - pcd0);
     gsync(g, tpq);
-    // ---- (3) primitive-level 2-PDM (Tcrtnc); single contraction: folded in below
-    if (nc > 1) {
-      for (int o = tid; o < ncart4; o += tpq) {
+    // ---- ket half-transform of the 2-PDM: Y[ij][pc][abcd] = sum_kl Ccd[kl][pc] Gam[ij,kl][abcd]
+    if (multi) {
+      for (int o = tid; o < nij * npc * ncart4; o += tpq) {
+        const int ij = o % nij, r1 = o / nij, pc = r1 % npc, abcd = r1 / npc;
         double s = 0.0;
-        for (int il = 0; il < nc; ++il) s = fma(CO[il], Gam[il + nc * o], s);
-        Gp[o] = s;
+        for (int klc = 0; klc < nklc; ++klc) s = fma(Ccd[klc * npcd + pcd0 + pc], Gam[ij + nij * klc + nc * abcd], s);
+        Y[ij + nij * (pc + PCD * abcd)] = s;
       }
     }
-    const double co0 = CO[0];
-    for (int r0 = 0; r0 < NR; r0 += rw) {
-      const int nrw = min(rw, NR - r0);
-      // ---- (2) 2D recursion, 2D-level HRR and derivative factors per (root, direction)
-      if (tid < 3 * nrw) {
-        const int d = tid % 3, rl = tid / 3, r = r0 + rl;
-        const double* c = cf + r * 10;
-        const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
-        double I[NI][NJ];
-        I[0][0] = d == 2 ? c[9] : 1.0;
-        if (NI > 1) I[1][0] = C00 * I[0][0];
-#pragma unroll
-        for (int i = 1; i < NI - 1; ++i) I[i + 1][0] = C00 * I[i][0] + i * B10 * I[i - 1][0];
-#pragma unroll
-        for (int j = 0; j < NJ - 1; ++j) {
-#pragma unroll
-          for (int i = 0; i < NI; ++i) {
-            double v = D00 * I[i][j];
-            if (j > 0) v += j * B01 * I[i][j - 1];
-            if (i > 0) v += i * B00 * I[i - 1][j];
-            I[i][j + 1] = v;
-          }
+    for (int pab0 = 0; pab0 < npab; pab0 += PAB) {
+      const int npa = min(PAB, npab - pab0);
+      const int nt = npa * npc;
+      gsync(g, tpq);
+      // ---- (1) roots: one (quartet, root) per thread
+      for (int job = tid; job < nt * NR; job += tpq) {
+        const int r = job % NR, t = job / NR;
+        const int pc = t / npa, pa = t - pc * npa;
+        const int ia = P.prim_off + pab0 + pa, ic = Q.prim_off + pcd0 + pc;
+        const double zeta = prim[ia], eta = prim[ic];
+        const double px = prim[2 * tot_np + ia], py = prim[3 * tot_np + ia], pz = prim[4 * tot_np + ia];
+        const double qx = prim[2 * tot_np + ic], qy = prim[3 * tot_np + ic], qz = prim[4 * tot_np + ic];
+        const double ze = zeta + eta, zei = 1.0 / ze, rho = zeta * eta * zei;
+        const double dx = px - qx, dy = py - qy, dz = pz - qz;
+        const double T = rho * (dx * dx + dy * dy + dz * dz);
+        const double fact = prim[tot_np + ia] * prim[tot_np + ic] * sqrt(zei);
+        double x, w;
+        rys_one<NR>(ra, T, r, x, w);
+        const double U2 = x * zei;
+        double* c = cf + t * CFT + r * 10;
+        c[0] = 0.5 * U2;
+        c[1] = 0.5 * (1.0 - U2 * eta) / zeta;
+        c[2] = 0.5 * (1.0 - U2 * zeta) / eta;
+        c[3] = px - A0 - eta * U2 * dx;
+        c[4] = py - A1 - eta * U2 * dy;
+        c[5] = pz - A2 - eta * U2 * dz;
+        c[6] = qx - C0 + zeta * U2 * dx;
+        c[7] = qy - C1 + zeta * U2 * dy;
+        c[8] = qz - C2 + zeta * U2 * dz;
+        c[9] = w * fact;
+        if (r == 0) {
+          double* e = cf + t * CFT + NR * 10;
+          e[0] = 2.0 * prim[5 * tot_np + ia];         // 2 alpha
+          e[1] = 2.0 * prim[6 * tot_np + ia];         // 2 beta
+          e[2] = 2.0 * prim[5 * tot_np + ic];         // 2 gamma
+          e[3] = Cab[pab0 + pa] * Ccd[pcd0 + pc];     // single-contraction coefficient
         }
-        double* T = S + (size_t)tid * scr;            // T[a][b][f]
-        double* U = T + NI * (lb + 2) * NJ;          // U[a][b][c][d]
-        const int LB2 = lb + 2;
-#pragma unroll
-        for (int a = 0; a < NI; ++a)
-#pragma unroll
-          for (int f = 0; f < NJ; ++f) T[(a * LB2) * NJ + f] = I[a][f];
+      }
+      // ---- (3) primitive 2-PDM (Tcrtnc) by the bra half-transform
+      if (multi) {
+        for (int o = tid; o < nt * ncart4; o += tpq) {
+          const int abcd = o % ncart4, t = o / ncart4;
+          const int pc = t / npa, pa = t - pc * npa;
+          const double* y = Y + nij * (pc + PCD * abcd);
+          double s = 0.0;
+          for (int ij = 0; ij < nij; ++ij) s = fma(Cab[ij * npab + pab0 + pa], y[ij], s);
+          Gp[t * ncart4 + abcd] = s;
+        }
+      }
+      gsync(g, tpq);
+      // ---- (2) 2D recursion, 2D-level HRR and derivative factors per (quartet, root, direction)
+      for (int job = tid; job < nt * NR * 3; job += tpq) {
+        const int d = job % 3, tr = job / 3, r = tr % NR, t = tr / NR;
+        const double* c = cf + t * CFT + r * 10;
+        const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
+        double* T = S + (size_t)job * scr;   // T[a][b][f]
+        double* U = T + NI * LB2 * NJ;       // U[a][b][c][d]
+        // 2D recursion written into the b = 0 plane of T
+        T[0] = d == 2 ? c[9] : 1.0;
+        if (NI > 1) T[LB2 * NJ] = C00 * T[0];
+        for (int i = 1; i < NI - 1; ++i) T[((i + 1) * LB2) * NJ] = C00 * T[(i * LB2) * NJ] + i * B10 * T[((i - 1) * LB2) * NJ];
+        for (int j = 0; j < NJ - 1; ++j)
+          for (int i = 0; i < NI; ++i) {
+            double v = D00 * T[(i * LB2) * NJ + j];
+            if (j > 0) v += j * B01 * T[(i * LB2) * NJ + j - 1];
+            if (i > 0) v += i * B00 * T[((i - 1) * LB2) * NJ + j];
+            T[(i * LB2) * NJ + j + 1] = v;
+          }
         const double ab = ABx[d], cdv = CDx[d];
         for (int b = 1; b < LB2; ++b)
           for (int a = 0; a + b <= NAB1; ++a)
             for (int f = 0; f < NJ; ++f)
               T[(a * LB2 + b) * NJ + f] = T[((a + 1) * LB2 + b - 1) * NJ + f] + ab * T[(a * LB2 + b - 1) * NJ + f];
-        const int LD1 = ld + 1;
         for (int a = 0; a < la + 2; ++a)
           for (int b = 0; b < LB2; ++b) {
             if (a + b > NAB1) continue;
@@ -304,8 +306,9 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
               for (int cc = 0; cc + dd <= NCD1; ++cc)
                 u[cc * LD1 + dd] = u[(cc + 1) * LD1 + dd - 1] + cdv * u[cc * LD1 + dd - 1];
           }
-        const double ta = cf[NR * 10 + 0], tb = cf[NR * 10 + 1], tg = cf[NR * 10 + 2];
-        double* Fo = F + (size_t)(rl * 3 + d) * 4 * n1d;
+        const double* e = cf + t * CFT + NR * 10;
+        const double ta = e[0], tb = e[1], tg = e[2];
+        double* Fo = F + ((size_t)(t * NR + r) * 3 + d) * 4 * n1d;
         for (int dd = 0; dd <= ld; ++dd)
           for (int cc = 0; cc <= lc; ++cc)
             for (int b = 0; b <= lb; ++b)
@@ -319,11 +322,12 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
               }
       }
       gsync(g, tpq);
-      // ---- (4) Assg1: sum over Cartesian components and the roots of this wave
-      for (int o = tid; o < ncart4; o += tpq) {
-        const double gm = nc > 1 ? Gp[o] : co0 * Gam[o];
+      // ---- (4) Assg1: sum over Cartesian components and roots
+      for (int o = tid; o < nt * ncart4; o += tpq) {
+        const int abcd = o % ncart4, t = o / ncart4;
+        const double gm = multi ? Gp[t * ncart4 + abcd] : cf[t * CFT + NR * 10 + 3] * Gam[abcd];
         if (gm == 0.0) continue;
-        const int ca = o % nca, r1 = o / nca, cb = r1 % ncb, r2 = r1 / ncb, cc = r2 % ncc, cd = r2 / ncc;
+        const int ca = abcd % nca, r1 = abcd / nca, cb = r1 % ncb, r2 = r1 / ncb, cc = r2 % ncc, cd = r2 / ncc;
         const unsigned char* ea = c_cartg[ca0 + ca];
         const unsigned char* eb = c_cartg[cb0 + cb];
         const unsigned char* ec = c_cartg[cc0 + cc];
@@ -331,12 +335,14 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
         int idx[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) idx[d] = ea[d] + (la + 1) * (eb[d] + (lb + 1) * (ec[d] + (lc + 1) * ed[d]));
-        for (int rl = 0; rl < nrw; ++rl) {
-          const double* Fx = F + (size_t)(rl * 3 + 0) * 4 * n1d + idx[0];
-          const double* Fy = F + (size_t)(rl * 3 + 1) * 4 * n1d + idx[1];
-          const double* Fz = F + (size_t)(rl * 3 + 2) * 4 * n1d + idx[2];
-          const double X = Fx[0], Y = Fy[0], Z = Fz[0];
-          const double gyz = gm * Y * Z, gxz = gm * X * Z, gxy = gm * X * Y;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          const double* Fb = F + (size_t)(t * NR + r) * 3 * 4 * n1d;
+          const double* Fx = Fb + idx[0];
+          const double* Fy = Fb + 4 * n1d + idx[1];
+          const double* Fz = Fb + 8 * n1d + idx[2];
+          const double X = Fx[0], Yv = Fy[0], Z = Fz[0];
+          const double gyz = gm * Yv * Z, gxz = gm * X * Z, gxy = gm * X * Yv;
 #pragma unroll
           for (int k = 0; k < 3; ++k) {
             acc[3 * k + 0] = fma(gyz, Fx[(k + 1) * n1d], acc[3 * k + 0]);
@@ -345,11 +351,11 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
           }
         }
       }
-      gsync(g, tpq);
     }
   }
+  gsync(g, tpq);
   // ---- reduce over the group, distribute to atoms (Distg1)
-  double* red = S;  // tpq/32 * 9 doubles (S holds at least 72)
+  double* red = U0;  // tpq/32 * 9 doubles
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
     double v = acc[k];
@@ -370,7 +376,7 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
 
 // ------------------------------------------------------------------ launch
 using GradFn = void (*)(const GradItem*, int, const DPair*, const double*, int, const double*, const double*, int,
-                        RysArgsG, double*, int, int, int);
+                        RysArgsG, double*, int, int, int, int);
 
 template <int A, int B>
 static GradFn gk() {
@@ -408,27 +414,33 @@ static GradFn pick_grad(int a, int b) {
 }
 
 
-// per-group shared memory (doubles) of one item with rw roots per wave
-static size_t grad_group_smem(const DPair& P, const DPair& Q, int nc, int rw) {
+// Per-group shared memory (doubles) of one work item with PAB x PCD tiles:
+//   Gam + Cab + Ccd + Y + max(stage-0 temp, tile (cf + Gp + F + S per quartet))
+static size_t grad_group_smem(const DPair& P, const DPair& Q, int nklc, int pab, int pcd) {
   const int la = P.la, lb = P.lb, lc = Q.la, ld = Q.lb;
   const int NI = la + lb + 2, NJ = lc + ld + 2;
   const int NR = (la + lb + lc + ld + 3) / 2;
   const size_t ncart4 = (size_t)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+  const size_t nsp4 = (size_t)ncomp(la) * ncomp(lb) * ncomp(lc) * ncomp(ld);
   const size_t n1d = (size_t)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
   const size_t scr = (size_t)NI * (lb + 2) * NJ + (size_t)(la + 2) * (lb + 2) * NJ * (ld + 1);
-  const size_t mainsz = (nc > 1 ? ncart4 : 0) + NR * 10 + 4 + nc + 3 * NR + rw * 12 * n1d +
-                        std::max<size_t>(3 * rw * scr, 8 * 9);
-  return nc * ncart4 + std::max(nc * ncart4, mainsz);
+  const size_t nij = (size_t)P.nci * P.ncj, nc = nij * nklc;
+  const bool multi = nc > 1;
+  const size_t fixed = nc * ncart4 + nij * P.np + (size_t)nklc * Q.np + (multi ? nij * pcd * ncart4 : 0);
+  const size_t nt = (size_t)pab * pcd;
+  const size_t tile = nt * ((size_t)NR * 10 + 4 + (multi ? ncart4 : 0) + (size_t)NR * 12 * n1d + 3 * (size_t)NR * scr);
+  return fixed + std::max({nc * std::max(ncart4, nsp4), tile, (size_t)8 * 9});
 }
 
-static int grad_roots(const DPair& P, const DPair& Q) { return (P.la + P.lb + Q.la + Q.lb + 3) / 2; }
+// Shared-memory target per CTA: ~3 CTAs per SM when the work item allows.
+static const size_t kGradCtaBudget = 72 * 1024 / 8;
+static const size_t kGradMaxBudget = 224 * 1024 / 8;
 
 int grad_build(Handle* h, double cutint, GradPlan& plan) {
   const int ns = h->sh.size();
-  const size_t budget = 224 * 1024 / 8;
   std::vector<std::vector<GradItem>> byc(64);
-  std::vector<size_t> mx(64, 0);
-  std::vector<int> rwmin(64, 99);
+  struct Mx { int npab = 0, npcd = 0; };
+  std::vector<Mx> mx(64);
   for (int i = 0; i < ns; ++i)
     for (int j = 0; j <= i; ++j) {
       const int p = pair_id(i, j);
@@ -441,18 +453,20 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
           // all four on one atom: the gradient contribution vanishes
           if (P.atom_a == P.atom_b && P.atom_a == Q.atom_a && P.atom_a == Q.atom_b) continue;
           const int deg = (i == j ? 1 : 2) * (k == l ? 1 : 2) * (p == q ? 1 : 2);
-          const int nijkl = P.nci * P.ncj * Q.nci * Q.ncj;
-          const int NR = grad_roots(P, Q);
-          int nc = nijkl, rw = NR;
-          while (nc > 1 && grad_group_smem(P, Q, nc, 1) > budget) nc = (nc + 1) / 2;
-          while (rw > 1 && grad_group_smem(P, Q, nc, rw) > budget) --rw;
-          if (grad_group_smem(P, Q, nc, rw) > budget) { h->err = "gradient quartet does not fit in shared memory"; return MG_ERR_ARG; }
+          const int nkl = Q.nci * Q.ncj;
+          int chunk = nkl;
+          while (chunk > 1 && grad_group_smem(P, Q, chunk, 1, 1) > kGradCtaBudget) chunk = (chunk + 1) / 2;
+          if (grad_group_smem(P, Q, chunk, 1, 1) > kGradMaxBudget) {
+            h->err = "gradient quartet does not fit in shared memory";
+            return MG_ERR_ARG;
+          }
           const int key = (P.la + P.lb + 1) * 8 + (Q.la + Q.lb + 1);
-          for (int c0 = 0; c0 < nijkl; c0 += nc) {
-            GradItem it{p, q, c0, std::min(nijkl, c0 + nc), 0.5 * deg};
+          Mx& m = mx[key];
+          for (int c0 = 0; c0 < nkl; c0 += chunk) {
+            GradItem it{p, q, c0, std::min(nkl, c0 + chunk), 0.5 * deg};
             byc[key].push_back(it);
-            mx[key] = std::max(mx[key], grad_group_smem(P, Q, it.c1 - it.c0, rw));
-            rwmin[key] = std::min(rwmin[key], rw);
+            m.npab = std::max(m.npab, P.np);
+            m.npcd = std::max(m.npcd, Q.np);
           }
         }
     }
@@ -464,15 +478,32 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
     std::stable_sort(v.begin(), v.end(), [&](const GradItem& a, const GradItem& b) {
       return (long long)h->pairs[a.p].np * h->pairs[a.q].np > (long long)h->pairs[b.p].np * h->pairs[b.q].np;
     });
+    // tile: largest PAB x PCD (<= 8 x 4 primitive quartets) whose worst item fits the CTA budget
+    auto worst = [&](int a, int c) {
+      size_t w = 0;
+      for (const GradItem& it : v) w = std::max(w, grad_group_smem(h->pairs[it.p], h->pairs[it.q], it.c1 - it.c0, a, c));
+      return w;
+    };
+    const size_t budget = std::max(kGradCtaBudget, worst(1, 1));
+    const Mx& m = mx[key];
+    int pab = std::max(1, std::min(m.npab, 8)), pcd = std::max(1, std::min(m.npcd, 4));
+    size_t need = worst(pab, pcd);
+    while (need > budget && (pab > 1 || pcd > 1)) {
+      if (pcd > 1) pcd = (pcd + 1) / 2;
+      else pab = (pab + 1) / 2;
+      need = worst(pab, pcd);
+    }
     GradClass c;
     c.nab1 = key / 8;
     c.ncd1 = key % 8;
     c.begin = plan.items.size();
     c.count = v.size();
     c.tpq = 64;
-    c.gsm = (int)((mx[key] + 1) & ~(size_t)1);
-    c.groups = (int)std::max<size_t>(1, std::min<size_t>(4, budget / c.gsm));
-    c.rw = rwmin[key];
+    c.gsm = (int)((need + 1) & ~(size_t)1);
+    c.groups = (int)std::max<size_t>(1, std::min<size_t>(4, kGradMaxBudget / c.gsm));
+    c.rw = 0;
+    c.pab = pab;
+    c.pcd = pcd;
     plan.items.insert(plan.items.end(), v.begin(), v.end());
     plan.classes.push_back(c);
   }
@@ -498,7 +529,7 @@ int grad_run(Handle* h, const GradPlan& plan, const double* d_D, double* d_grad,
     const int nblk = (c.count + c.groups - 1) / c.groups;
     k<<<nblk, c.tpq * c.groups, sizeof(double) * (size_t)c.gsm * c.groups, st>>>(
         plan.d_items + c.begin, c.count, h->d_pairs, h->d_prim, h->tot_np, h->d_coef, d_D, h->nbf, ra, d_grad, c.tpq,
-        c.gsm, c.rw);
+        c.gsm, c.pab, c.pcd);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (cudaGetLastError() != cudaSuccess) { h->err = "gradient kernel launch failed"; return MG_ERR_CUDA; }
   }
@@ -514,9 +545,10 @@ void grad_free(GradPlan* p) {
 // Algorithmic FP64 flop count of a gradient plan (FMA = 2): per primitive
 // quartet the Rys roots (2 x 7 FMA per root and weight + 30), per root and
 // direction the 2D recursion (4 NI NJ), 2D-level HRR (2 (lb+1) NI NJ +
-// 2 (la+2)(lb+2) NJ ld) and derivative factors (8 n1d), the primitive 2-PDM
-// (2 nc ncart4 when nc > 1) and Assg1 (24 flops per Cartesian quartet and
-// root); per work item the 2-PDM and its spherical->Cartesian transform.
+// 2 (la+2)(lb+2) NJ ld) and derivative factors (8 n1d), the bra half of the
+// primitive 2-PDM (2 nij ncart4 when nc > 1) and Assg1 (24 flops per
+// Cartesian quartet and root); per work item the 2-PDM, its spherical ->
+// Cartesian transform and the ket half of the de-contraction.
 double grad_plan_flops(const Handle* h, const GradPlan& plan) {
   double f = 0;
   for (const GradItem& it : plan.items) {
@@ -526,12 +558,13 @@ double grad_plan_flops(const Handle* h, const GradPlan& plan) {
     const double ncart4 = (double)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
     const double nsp4 = (double)ncomp(la) * ncomp(lb) * ncomp(lc) * ncomp(ld);
     const double n1d = (double)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-    const int nc = it.c1 - it.c0;
+    const int nij = P.nci * P.ncj, nklc = it.c1 - it.c0, nc = nij * nklc;
     const double per_prim = NR * 28.0 + 30.0 +
                             3.0 * NR * (4.0 * NI * NJ + 2.0 * (lb + 1) * NI * NJ + 2.0 * (la + 2) * (lb + 2) * NJ * ld +
                                         8.0 * n1d) +
-                            (nc > 1 ? 2.0 * nc * ncart4 : 0.0) + 24.0 * ncart4 * NR;
-    const double per_item = nc * nsp4 * 8.0 + 2.0 * nc * ncart4 * 4.0 * std::max(ncomp(la), ncomp(ld));
+                            (nc > 1 ? 2.0 * nij * ncart4 : 0.0) + 24.0 * ncart4 * NR;
+    const double per_item = nc * nsp4 * 8.0 + 2.0 * nc * ncart4 * 4.0 * std::max(ncomp(la), ncomp(ld)) +
+                            (nc > 1 ? 2.0 * nc * ncart4 * Q.np : 0.0);
     f += per_prim * (double)P.np * Q.np + per_item;
   }
   return f;

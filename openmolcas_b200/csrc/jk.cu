@@ -135,8 +135,9 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bflo
 }
 
 // Lhi/Llo[J][a][b] (= [J][b][a]) from the FP32 rs vectors of a block
+// (squares with leading dimension ld >= n; the padding stays zero)
 __global__ void k_unpack_block_split(const int* __restrict__ rs_a, const int* __restrict__ rs_b, int64_t nrs,
-                                     const float* __restrict__ L, int nb, int n, __nv_bfloat16* __restrict__ Lhi,
+                                     const float* __restrict__ L, int nb, int ld, __nv_bfloat16* __restrict__ Lhi,
                                      __nv_bfloat16* __restrict__ Llo) {
   int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (o >= nrs * nb) return;
@@ -145,22 +146,33 @@ __global__ void k_unpack_block_split(const int* __restrict__ rs_a, const int* __
   const int a = rs_a[t], b = rs_b[t];
   __nv_bfloat16 hi, lo;
   split_bf16(L[t + nrs * J], hi, lo);
-  const size_t base = (size_t)J * n * n;
-  Lhi[base + (size_t)a * n + b] = hi;
-  Llo[base + (size_t)a * n + b] = lo;
-  Lhi[base + (size_t)b * n + a] = hi;
-  Llo[base + (size_t)b * n + a] = lo;
+  const size_t base = (size_t)J * ld * ld;
+  Lhi[base + (size_t)a * ld + b] = hi;
+  Llo[base + (size_t)a * ld + b] = lo;
+  Lhi[base + (size_t)b * ld + a] = hi;
+  Llo[base + (size_t)b * ld + a] = lo;
 }
 
-__global__ void k_split_f64(const double* __restrict__ x, int64_t n, __nv_bfloat16* __restrict__ hi,
-                            __nv_bfloat16* __restrict__ lo) {
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  __nv_bfloat16 h, l;
-  split_bf16((float)x[t], h, l);
-  hi[t] = h;
-  lo[t] = l;
+// C (n x r, column-major FP64) -> split BF16 with leading dimension ld (padding zero)
+__global__ void k_split_c(const double* __restrict__ C, int n, int r, int ld, __nv_bfloat16* __restrict__ hi,
+                          __nv_bfloat16* __restrict__ lo) {
+  int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (o >= (int64_t)ld * r) return;
+  const int a = (int)(o % ld), k = (int)(o / ld);
+  __nv_bfloat16 h = __float2bfloat16_rn(0.0f), l = h;
+  if (a < n) split_bf16((float)C[a + (size_t)n * k], h, l);
+  hi[o] = h;
+  lo[o] = l;
 }
+
+// K (n x n FP64) += Kb (ld x ld FP32)
+__global__ void k_add_kb(const float* __restrict__ Kb, int ld, double* __restrict__ K, int n) {
+  int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (o >= (int64_t)n * n) return;
+  const int i = (int)(o % n), j = (int)(o / n);
+  K[o] += (double)Kb[(size_t)i + (size_t)ld * j];
+}
+
 
 __global__ void k_split_f32(const float* __restrict__ x, int64_t n, __nv_bfloat16* __restrict__ hi,
                             __nv_bfloat16* __restrict__ lo) {
@@ -172,12 +184,15 @@ __global__ void k_split_f32(const float* __restrict__ x, int64_t n, __nv_bfloat1
   lo[t] = l;
 }
 
-// V[J] = sum_t L[t,J] dw[t]   (FP32 loads, FP64 accumulation); one CTA per vector
+// V[J] += sum_t L[t,J] dw[t] over one row chunk (FP32 loads, FP64 accumulation);
+// grid (vectors, row chunks); V must be zeroed first
 __global__ void k_jvec(const float* __restrict__ L, int64_t nrs, const double* __restrict__ dw, double* __restrict__ V) {
   const int J = blockIdx.x;
   const float* l = L + nrs * J;
+  const int64_t chunk = (nrs + gridDim.y - 1) / gridDim.y;
+  const int64_t t0 = chunk * blockIdx.y, t1 = min(nrs, t0 + chunk);
   double s = 0.0;
-  for (int64_t t = threadIdx.x; t < nrs; t += blockDim.x) s = fma((double)l[t], dw[t], s);
+  for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) s = fma((double)l[t], dw[t], s);
   __shared__ double red[32];
   for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -185,7 +200,7 @@ __global__ void k_jvec(const float* __restrict__ L, int64_t nrs, const double* _
   if (threadIdx.x < 32) {
     s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
     for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-    if (threadIdx.x == 0) V[J] = s;
+    if (threadIdx.x == 0) atomicAdd(&V[J], s);
   }
 }
 
@@ -199,16 +214,13 @@ __global__ void k_jacc(const float* __restrict__ L, int64_t nrs, int nb, const d
   jrs[t] += s;
 }
 
-__global__ void k_add_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, int64_t n) {
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t < n) b[t] += (double)a[t];
-}
 
 int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block) {
   ChoState* c = h->cho;
   const int64_t nrs = cho_nrs(c);
   const int M = cho_nvec(c);
   const int n = h->nbf;
+  const int ld = (n + 63) / 64 * 64;  // padded leading dimension for the tensor-core GEMMs
   if (!cho_vec_ptr32(c, 0, 1)) {
     int rc = cho_make_fp32(c, st);
     if (rc) { h->err = "FP32 vector copy failed"; return rc; }
@@ -217,11 +229,9 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   cublasSetStream(cb, st);
   const int* d_ra = cho_rs_a_dev(c);
   const int* d_rb = cho_rs_b_dev(c);
-  // scratch (bytes): dw, jrs (f64 nrs), V (f64 block), D (f64 n*n), Chi/Clo (bf16 n*r),
-  // Lhi/Llo (bf16 block*n*n), X (f32 n*block*r), Xhi/Xlo (bf16 n*block*r), Kb (f32 n*n)
-  const size_t nn = (size_t)n * n, nbr = (size_t)n * block * r;
-  size_t need = 8 * ((size_t)2 * nrs + block + nn) + 2 * (2 * (size_t)n * r) + 2 * (2 * (size_t)block * nn) +
-                4 * nbr + 2 * (2 * nbr) + 4 * nn + 1024;
+  const size_t nn = (size_t)n * n, ll = (size_t)ld * ld, lbr = (size_t)ld * block * r;
+  size_t need = 8 * ((size_t)2 * nrs + block + nn) + 2 * (2 * (size_t)ld * r) + 2 * (2 * (size_t)block * ll) +
+                4 * lbr + 2 * (2 * lbr) + 4 * ll + 16 * 256;
   char* ws = (char*)ws_get(h, need, st);
   if (!ws) { h->err = "jk workspace allocation failed"; return MG_ERR_MEMORY; }
   auto take = [&](size_t bytes) { char* p = ws; ws += (bytes + 255) & ~(size_t)255; return (void*)p; };
@@ -229,50 +239,56 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   double* jrs = (double*)take(8 * nrs);
   double* V = (double*)take(8 * block);
   double* D = (double*)take(8 * nn);
-  __nv_bfloat16* Chi = (__nv_bfloat16*)take(2 * (size_t)n * r);
-  __nv_bfloat16* Clo = (__nv_bfloat16*)take(2 * (size_t)n * r);
-  __nv_bfloat16* Lhi = (__nv_bfloat16*)take(2 * (size_t)block * nn);
-  __nv_bfloat16* Llo = (__nv_bfloat16*)take(2 * (size_t)block * nn);
-  float* X = (float*)take(4 * nbr);
-  __nv_bfloat16* Xhi = (__nv_bfloat16*)take(2 * nbr);
-  __nv_bfloat16* Xlo = (__nv_bfloat16*)take(2 * nbr);
-  float* Kb = (float*)take(4 * nn);
+  __nv_bfloat16* Chi = (__nv_bfloat16*)take(2 * (size_t)ld * r);
+  __nv_bfloat16* Clo = (__nv_bfloat16*)take(2 * (size_t)ld * r);
+  __nv_bfloat16* Lhi = (__nv_bfloat16*)take(2 * (size_t)block * ll);
+  __nv_bfloat16* Llo = (__nv_bfloat16*)take(2 * (size_t)block * ll);
+  float* X = (float*)take(4 * lbr);
+  __nv_bfloat16* Xhi = (__nv_bfloat16*)take(2 * lbr);
+  __nv_bfloat16* Xlo = (__nv_bfloat16*)take(2 * lbr);
+  float* Kb = (float*)take(4 * ll);
   const double one = 1.0, zero = 0.0;
   const float onef = 1.0f, zerof = 0.0f;
   cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, r, &one, d_C, n, d_C, n, &zero, D, n);
   k_pack_density<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, D, n, dw);
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_split_f64<<<nb256((int64_t)n * r), 256, 0, st>>>(d_C, (int64_t)n * r, Chi, Clo);
+  k_split_c<<<nb256((int64_t)ld * r), 256, 0, st>>>(d_C, n, r, ld, Chi, Clo);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   cudaMemsetAsync(jrs, 0, 8 * nrs, st);
   cudaMemsetAsync(d_K, 0, 8 * nn, st);
+  if (ld != n) {  // padding rows/columns of the squares stay zero
+    cudaMemsetAsync(Lhi, 0, 2 * (size_t)block * ll, st);
+    cudaMemsetAsync(Llo, 0, 2 * (size_t)block * ll, st);
+  }
+  const unsigned jchunks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(64, nrs / 8192));
   for (int J0 = 0; J0 < M; J0 += block) {
     const int nb = std::min(block, M - J0);
     const float* Lb = cho_vec_ptr32(c, J0, nb);
     if (!Lb) { h->err = "vector block straddles storage blocks"; return MG_ERR_ARG; }
     // Coulomb
-    k_jvec<<<nb, 256, 0, st>>>(Lb, nrs, dw, V);
+    cudaMemsetAsync(V, 0, 8 * nb, st);
+    k_jvec<<<dim3(nb, jchunks), 256, 0, st>>>(Lb, nrs, dw, V);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     k_jacc<<<nb256(nrs), 256, 0, st>>>(Lb, nrs, nb, V, jrs);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     // Exchange: X_J = L_J C  (3 split products, FP32 accumulation)
-    k_unpack_block_split<<<nb256(nrs * nb), 256, 0, st>>>(d_ra, d_rb, nrs, Lb, nb, n, Lhi, Llo);
+    k_unpack_block_split<<<nb256(nrs * nb), 256, 0, st>>>(d_ra, d_rb, nrs, Lb, nb, ld, Lhi, Llo);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     const __nv_bfloat16* As[3] = {Lhi, Lhi, Llo};
     const __nv_bfloat16* Bs[3] = {Chi, Clo, Chi};
     for (int q = 0; q < 3; ++q)
-      cublasGemmStridedBatchedEx(cb, CUBLAS_OP_N, CUBLAS_OP_N, n, r, n, &onef, As[q], CUDA_R_16BF, n, (long long)nn,
-                                 Bs[q], CUDA_R_16BF, n, 0, q == 0 ? &zerof : &onef, X, CUDA_R_32F, n,
-                                 (long long)n * r, nb, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
+      cublasGemmStridedBatchedEx(cb, CUBLAS_OP_N, CUBLAS_OP_N, ld, r, ld, &onef, As[q], CUDA_R_16BF, ld, (long long)ll,
+                                 Bs[q], CUDA_R_16BF, ld, 0, q == 0 ? &zerof : &onef, X, CUDA_R_32F, ld,
+                                 (long long)ld * r, nb, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
     // K_b = X X^T over this block (3 split products), then K += K_b in FP64
-    k_split_f32<<<nb256((int64_t)n * nb * r), 256, 0, st>>>(X, (int64_t)n * nb * r, Xhi, Xlo);
+    k_split_f32<<<nb256((int64_t)ld * nb * r), 256, 0, st>>>(X, (int64_t)ld * nb * r, Xhi, Xlo);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     const __nv_bfloat16* Ps[3] = {Xhi, Xhi, Xlo};
     const __nv_bfloat16* Qs[3] = {Xhi, Xlo, Xhi};
     for (int q = 0; q < 3; ++q)
-      cublasGemmEx(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, nb * r, &onef, Ps[q], CUDA_R_16BF, n, Qs[q], CUDA_R_16BF, n,
-                   q == 0 ? &zerof : &onef, Kb, CUDA_R_32F, n, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
-    k_add_f32_to_f64<<<nb256((int64_t)nn), 256, 0, st>>>(Kb, d_K, (int64_t)nn);
+      cublasGemmEx(cb, CUBLAS_OP_N, CUBLAS_OP_T, ld, ld, nb * r, &onef, Ps[q], CUDA_R_16BF, ld, Qs[q], CUDA_R_16BF, ld,
+                   q == 0 ? &zerof : &onef, Kb, CUDA_R_32F, ld, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
+    k_add_kb<<<nb256((int64_t)nn), 256, 0, st>>>(Kb, ld, d_K, n);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
   k_unpack_sym<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, jrs, n, d_J);

@@ -103,11 +103,11 @@ struct Handle {
 
 struct GradItem {
   int p, q;      // bra / ket canonical pairs
-  int c0, c1;    // contracted ijkl range
+  int c0, c1;    // ket contracted-pair (kl) range
   double scale;  // 1/2 * degeneracy
 };
 struct GradClass {
-  int nab1, ncd1, begin, count, tpq, gsm, groups, rw;
+  int nab1, ncd1, begin, count, tpq, gsm, groups, rw, pab, pcd;
 };
 struct GradPlan {
   std::vector<GradItem> items;
