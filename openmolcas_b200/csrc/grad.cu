@@ -101,7 +101,8 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
                                                    const DPair* __restrict__ pairs, const double* __restrict__ prim,
                                                    int tot_np, const double* __restrict__ coef,
                                                    const double* __restrict__ Dm, int nbf, RysArgsG ra,
-                                                   double* __restrict__ grad, int tpq, int gsm, int PAB, int PCD) {
+                                                   double* __restrict__ grad, int tpq, int gsm, int PAB, int PCD,
+                                                   int RW) {
   constexpr int NR = (NAB1 + NCD1 + 1) / 2;
   constexpr int NI = NAB1 + 1, NJ = NCD1 + 1;
   extern __shared__ double smem_all[];
@@ -135,8 +136,8 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
   double* Tmp = U0;                            // stage-0 temp (nc * ncart4)
   double* cf = U0;                             // NT * CFT
   double* Gp = cf + NT * CFT;                  // NT * ncart4 (multi only)
-  double* F = Gp + (multi ? NT * ncart4 : 0);  // NT * NR * 12 * n1d
-  double* S = F + NT * NR * 12 * n1d;          // NT * 3 * NR * scr
+  double* F = Gp + (multi ? NT * ncart4 : 0);  // NT * RW * 12 * n1d  (RW roots per wave)
+  double* S = F + NT * RW * 12 * n1d;          // NT * 3 * RW * scr
   for (int o = tid; o < nij * npab; o += tpq) Cab[o] = coef[P.coef_off + o];
   for (int o = tid; o < nklc * npcd; o += tpq) Ccd[o] = coef[Q.coef_off + (size_t)it.c0 * npcd + o];
   // ---- stage 0: contracted 2-PDM (PGet1), spherical, then -> Cartesian
@@ -274,9 +275,11 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
         }
       }
       gsync(g, tpq);
+      for (int r0 = 0; r0 < NR; r0 += RW) {
+      const int nrw = min(RW, NR - r0);
       // ---- (2) 2D recursion, 2D-level HRR and derivative factors per (quartet, root, direction)
-      for (int job = tid; job < nt * NR * 3; job += tpq) {
-        const int d = job % 3, tr = job / 3, r = tr % NR, t = tr / NR;
+      for (int job = tid; job < nt * nrw * 3; job += tpq) {
+        const int d = job % 3, tr = job / 3, rl = tr % nrw, t = tr / nrw, r = r0 + rl;
         const double* c = cf + t * CFT + r * 10;
         const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
         double* T = S + (size_t)job * scr;   // T[a][b][f]
@@ -308,7 +311,7 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
           }
         const double* e = cf + t * CFT + NR * 10;
         const double ta = e[0], tb = e[1], tg = e[2];
-        double* Fo = F + ((size_t)(t * NR + r) * 3 + d) * 4 * n1d;
+        double* Fo = F + ((size_t)(t * nrw + rl) * 3 + d) * 4 * n1d;
         for (int dd = 0; dd <= ld; ++dd)
           for (int cc = 0; cc <= lc; ++cc)
             for (int b = 0; b <= lb; ++b)
@@ -335,9 +338,8 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
         int idx[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) idx[d] = ea[d] + (la + 1) * (eb[d] + (lb + 1) * (ec[d] + (lc + 1) * ed[d]));
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-          const double* Fb = F + (size_t)(t * NR + r) * 3 * 4 * n1d;
+        for (int rl = 0; rl < nrw; ++rl) {
+          const double* Fb = F + (size_t)(t * nrw + rl) * 3 * 4 * n1d;
           const double* Fx = Fb + idx[0];
           const double* Fy = Fb + 4 * n1d + idx[1];
           const double* Fz = Fb + 8 * n1d + idx[2];
@@ -351,6 +353,8 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
           }
         }
       }
+      gsync(g, tpq);
+      }  // root waves
     }
   }
   gsync(g, tpq);
@@ -376,7 +380,7 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
 
 // ------------------------------------------------------------------ launch
 using GradFn = void (*)(const GradItem*, int, const DPair*, const double*, int, const double*, const double*, int,
-                        RysArgsG, double*, int, int, int, int);
+                        RysArgsG, double*, int, int, int, int, int);
 
 template <int A, int B>
 static GradFn gk() {
@@ -416,7 +420,7 @@ static GradFn pick_grad(int a, int b) {
 
 // Per-group shared memory (doubles) of one work item with PAB x PCD tiles:
 //   Gam + Cab + Ccd + Y + max(stage-0 temp, tile (cf + Gp + F + S per quartet))
-static size_t grad_group_smem(const DPair& P, const DPair& Q, int nklc, int pab, int pcd) {
+static size_t grad_group_smem(const DPair& P, const DPair& Q, int nklc, int pab, int pcd, int rw) {
   const int la = P.la, lb = P.lb, lc = Q.la, ld = Q.lb;
   const int NI = la + lb + 2, NJ = lc + ld + 2;
   const int NR = (la + lb + lc + ld + 3) / 2;
@@ -428,9 +432,13 @@ static size_t grad_group_smem(const DPair& P, const DPair& Q, int nklc, int pab,
   const bool multi = nc > 1;
   const size_t fixed = nc * ncart4 + nij * P.np + (size_t)nklc * Q.np + (multi ? nij * pcd * ncart4 : 0);
   const size_t nt = (size_t)pab * pcd;
-  const size_t tile = nt * ((size_t)NR * 10 + 4 + (multi ? ncart4 : 0) + (size_t)NR * 12 * n1d + 3 * (size_t)NR * scr);
+  const size_t w = std::min<size_t>(rw, NR);
+  const size_t tile = nt * ((size_t)NR * 10 + 4 + (multi ? ncart4 : 0) + w * 12 * n1d + 3 * w * scr);
   return fixed + std::max({nc * std::max(ncart4, nsp4), tile, (size_t)8 * 9});
 }
+
+static inline int c_nab1(int key) { return key / 8; }
+static inline int c_ncd1(int key) { return key % 8; }
 
 // Shared-memory target per CTA: ~3 CTAs per SM when the work item allows.
 static const size_t kGradCtaBudget = 72 * 1024 / 8;
@@ -455,8 +463,8 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
           const int deg = (i == j ? 1 : 2) * (k == l ? 1 : 2) * (p == q ? 1 : 2);
           const int nkl = Q.nci * Q.ncj;
           int chunk = nkl;
-          while (chunk > 1 && grad_group_smem(P, Q, chunk, 1, 1) > kGradCtaBudget) chunk = (chunk + 1) / 2;
-          if (grad_group_smem(P, Q, chunk, 1, 1) > kGradMaxBudget) {
+          while (chunk > 1 && grad_group_smem(P, Q, chunk, 1, 1, 1) > kGradCtaBudget) chunk = (chunk + 1) / 2;
+          if (grad_group_smem(P, Q, chunk, 1, 1, 1) > kGradMaxBudget) {
             h->err = "gradient quartet does not fit in shared memory";
             return MG_ERR_ARG;
           }
@@ -479,19 +487,22 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
       return (long long)h->pairs[a.p].np * h->pairs[a.q].np > (long long)h->pairs[b.p].np * h->pairs[b.q].np;
     });
     // tile: largest PAB x PCD (<= 8 x 4 primitive quartets) whose worst item fits the CTA budget
-    auto worst = [&](int a, int c) {
+    auto worst = [&](int a, int c, int rw) {
       size_t w = 0;
-      for (const GradItem& it : v) w = std::max(w, grad_group_smem(h->pairs[it.p], h->pairs[it.q], it.c1 - it.c0, a, c));
+      for (const GradItem& it : v)
+        w = std::max(w, grad_group_smem(h->pairs[it.p], h->pairs[it.q], it.c1 - it.c0, a, c, rw));
       return w;
     };
-    const size_t budget = std::max(kGradCtaBudget, worst(1, 1));
+    const int NRc = (c_nab1(key) + c_ncd1(key) + 1) / 2;
+    const size_t budget = std::max(kGradCtaBudget, std::min(kGradMaxBudget, worst(1, 1, NRc)));
     const Mx& m = mx[key];
-    int pab = std::max(1, std::min(m.npab, 8)), pcd = std::max(1, std::min(m.npcd, 4));
-    size_t need = worst(pab, pcd);
-    while (need > budget && (pab > 1 || pcd > 1)) {
+    int pab = std::max(1, std::min(m.npab, 8)), pcd = std::max(1, std::min(m.npcd, 4)), rw = NRc;
+    size_t need = worst(pab, pcd, rw);
+    while (need > budget && (pab > 1 || pcd > 1 || rw > 1)) {
       if (pcd > 1) pcd = (pcd + 1) / 2;
-      else pab = (pab + 1) / 2;
-      need = worst(pab, pcd);
+      else if (pab > 1) pab = (pab + 1) / 2;
+      else --rw;
+      need = worst(pab, pcd, rw);
     }
     GradClass c;
     c.nab1 = key / 8;
@@ -501,7 +512,7 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
     c.tpq = 64;
     c.gsm = (int)((need + 1) & ~(size_t)1);
     c.groups = (int)std::max<size_t>(1, std::min<size_t>(4, kGradMaxBudget / c.gsm));
-    c.rw = 0;
+    c.rw = rw;
     c.pab = pab;
     c.pcd = pcd;
     plan.items.insert(plan.items.end(), v.begin(), v.end());
@@ -529,7 +540,7 @@ int grad_run(Handle* h, const GradPlan& plan, const double* d_D, double* d_grad,
     const int nblk = (c.count + c.groups - 1) / c.groups;
     k<<<nblk, c.tpq * c.groups, sizeof(double) * (size_t)c.gsm * c.groups, st>>>(
         plan.d_items + c.begin, c.count, h->d_pairs, h->d_prim, h->tot_np, h->d_coef, d_D, h->nbf, ra, d_grad, c.tpq,
-        c.gsm, c.pab, c.pcd);
+        c.gsm, c.pab, c.pcd, c.rw);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (cudaGetLastError() != cudaSuccess) { h->err = "gradient kernel launch failed"; return MG_ERR_CUDA; }
   }
