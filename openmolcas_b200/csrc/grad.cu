@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
   const int nca = d_ncart(la), ncb = d_ncart(lb), ncc = d_ncart(lc), ncd = d_ncart(ld);
   const int nsa = d_ncomp(la), nsb = d_ncomp(lb), nsc = d_ncomp(lc), nsd = d_ncomp(ld);
   const int ncart4 = nca * ncb * ncc * ncd;
-  const int nij = P.nci * P.ncj;
+  const int nij = it.i1 - it.i0;   // bra contracted pairs [i0, i1)
   const int nklc = it.c1 - it.c0;  // ket contracted pairs [c0, c1)
   const int nc = nij * nklc;
   const bool multi = nc > 1;
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
   double* Gp = cf + NT * CFT;                  // NT * ncart4 (multi only)
   double* F = Gp + (multi ? NT * ncart4 : 0);  // NT * RW * 12 * n1d  (RW roots per wave)
   double* S = F + NT * RW * 12 * n1d;          // NT * 3 * RW * scr
-  for (int o = tid; o < nij * npab; o += tpq) Cab[o] = coef[P.coef_off + o];
+  for (int o = tid; o < nij * npab; o += tpq) Cab[o] = coef[P.coef_off + (size_t)it.i0 * npab + o];
   for (int o = tid; o < nklc * npcd; o += tpq) Ccd[o] = coef[Q.coef_off + (size_t)it.c0 * npcd + o];
   // ---- stage 0: contracted 2-PDM (PGet1), spherical, then -> Cartesian
   {
@@ -146,8 +146,7 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
     for (int o = tid; o < nc * nsp4; o += tpq) {
       const int il = o % nc, r1 = o / nc;
       const int sa = r1 % nsa, r2 = r1 / nsa, sb = r2 % nsb, r3 = r2 / nsb, sc = r3 % nsc, sd = r3 / nsc;
-      const int ijkl = nij * it.c0 + il;
-      const int kl = ijkl / nij, ij = ijkl - kl * nij;
+      const int ij = it.i0 + il % nij, kl = it.c0 + il / nij;
       const int ki = ij % P.nci, kj = ij / P.nci, kk = kl % Q.nci, kq = kl / Q.nci;
       const int pa = P.ao_a + sa * P.nci + ki, pb = P.ao_b + sb * P.ncj + kj;
       const int pc = Q.ao_a + sc * Q.nci + kk, pd = Q.ao_b + sd * Q.ncj + kq;
@@ -420,7 +419,7 @@ static GradFn pick_grad(int a, int b) {
 
 // Per-group shared memory (doubles) of one work item with PAB x PCD tiles:
 //   Gam + Cab + Ccd + Y + max(stage-0 temp, tile (cf + Gp + F + S per quartet))
-static size_t grad_group_smem(const DPair& P, const DPair& Q, int nklc, int pab, int pcd, int rw) {
+static size_t grad_group_smem(const DPair& P, const DPair& Q, int nijc, int nklc, int pab, int pcd, int rw) {
   const int la = P.la, lb = P.lb, lc = Q.la, ld = Q.lb;
   const int NI = la + lb + 2, NJ = lc + ld + 2;
   const int NR = (la + lb + lc + ld + 3) / 2;
@@ -428,7 +427,7 @@ static size_t grad_group_smem(const DPair& P, const DPair& Q, int nklc, int pab,
   const size_t nsp4 = (size_t)ncomp(la) * ncomp(lb) * ncomp(lc) * ncomp(ld);
   const size_t n1d = (size_t)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
   const size_t scr = (size_t)NI * (lb + 2) * NJ + (size_t)(la + 2) * (lb + 2) * NJ * (ld + 1);
-  const size_t nij = (size_t)P.nci * P.ncj, nc = nij * nklc;
+  const size_t nij = nijc, nc = nij * nklc;
   const bool multi = nc > 1;
   const size_t fixed = nc * ncart4 + nij * P.np + (size_t)nklc * Q.np + (multi ? nij * pcd * ncart4 : 0);
   const size_t nt = (size_t)pab * pcd;
@@ -461,21 +460,26 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
           // all four on one atom: the gradient contribution vanishes
           if (P.atom_a == P.atom_b && P.atom_a == Q.atom_a && P.atom_a == Q.atom_b) continue;
           const int deg = (i == j ? 1 : 2) * (k == l ? 1 : 2) * (p == q ? 1 : 2);
-          const int nkl = Q.nci * Q.ncj;
-          int chunk = nkl;
-          while (chunk > 1 && grad_group_smem(P, Q, chunk, 1, 1, 1) > kGradCtaBudget) chunk = (chunk + 1) / 2;
-          if (grad_group_smem(P, Q, chunk, 1, 1, 1) > kGradMaxBudget) {
+          const int nkl = Q.nci * Q.ncj, nij = P.nci * P.ncj;
+          // chunk the contracted block (kl first, then ij) until one quartet tile fits
+          int ckl = nkl, cij = nij;
+          while ((ckl > 1 || cij > 1) && grad_group_smem(P, Q, cij, ckl, 1, 1, 1) > kGradCtaBudget) {
+            if (ckl > 1) ckl = (ckl + 1) / 2;
+            else cij = (cij + 1) / 2;
+          }
+          if (grad_group_smem(P, Q, cij, ckl, 1, 1, 1) > kGradMaxBudget) {
             h->err = "gradient quartet does not fit in shared memory";
             return MG_ERR_ARG;
           }
           const int key = (P.la + P.lb + 1) * 8 + (Q.la + Q.lb + 1);
           Mx& m = mx[key];
-          for (int c0 = 0; c0 < nkl; c0 += chunk) {
-            GradItem it{p, q, c0, std::min(nkl, c0 + chunk), 0.5 * deg};
-            byc[key].push_back(it);
-            m.npab = std::max(m.npab, P.np);
-            m.npcd = std::max(m.npcd, Q.np);
-          }
+          for (int i0 = 0; i0 < nij; i0 += cij)
+            for (int c0 = 0; c0 < nkl; c0 += ckl) {
+              GradItem it{p, q, c0, std::min(nkl, c0 + ckl), i0, std::min(nij, i0 + cij), 0.5 * deg};
+              byc[key].push_back(it);
+              m.npab = std::max(m.npab, P.np);
+              m.npcd = std::max(m.npcd, Q.np);
+            }
         }
     }
   plan.items.clear();
@@ -490,7 +494,7 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
     auto worst = [&](int a, int c, int rw) {
       size_t w = 0;
       for (const GradItem& it : v)
-        w = std::max(w, grad_group_smem(h->pairs[it.p], h->pairs[it.q], it.c1 - it.c0, a, c, rw));
+        w = std::max(w, grad_group_smem(h->pairs[it.p], h->pairs[it.q], it.i1 - it.i0, it.c1 - it.c0, a, c, rw));
       return w;
     };
     const int NRc = (c_nab1(key) + c_ncd1(key) + 1) / 2;
@@ -569,7 +573,7 @@ double grad_plan_flops(const Handle* h, const GradPlan& plan) {
     const double ncart4 = (double)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
     const double nsp4 = (double)ncomp(la) * ncomp(lb) * ncomp(lc) * ncomp(ld);
     const double n1d = (double)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-    const int nij = P.nci * P.ncj, nklc = it.c1 - it.c0, nc = nij * nklc;
+    const int nij = it.i1 - it.i0, nklc = it.c1 - it.c0, nc = nij * nklc;
     const double per_prim = NR * 28.0 + 30.0 +
                             3.0 * NR * (4.0 * NI * NJ + 2.0 * (lb + 1) * NI * NJ + 2.0 * (la + 2) * (lb + 2) * NJ * ld +
                                         8.0 * n1d) +

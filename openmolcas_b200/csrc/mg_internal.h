@@ -104,6 +104,7 @@ struct Handle {
 struct GradItem {
   int p, q;      // bra / ket canonical pairs
   int c0, c1;    // ket contracted-pair (kl) range
+  int i0, i1;    // bra contracted-pair (ij) range
   double scale;  // 1/2 * degeneracy
 };
 struct GradClass {
