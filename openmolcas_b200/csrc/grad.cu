@@ -37,6 +37,8 @@ struct RysArgsG {
 __constant__ double c_sph[1 + 9 + 30 + 70];
 __constant__ int c_sph_off[4];
 __constant__ unsigned char c_cartg[120][3];
+// binomial coefficients C(n, k), n, k <= 8
+__constant__ double c_binom[9][9];
 
 static void init_grad_tables(const Handle* h) {
   static bool done = false;
@@ -58,6 +60,12 @@ static void init_grad_tables(const Handle* h) {
         ++k;
       }
   cudaMemcpyToSymbol(c_cartg, t, sizeof(t));
+  double bn[9][9] = {};
+  for (int n = 0; n <= 8; ++n) {
+    bn[n][0] = 1.0;
+    for (int k = 1; k <= n; ++k) bn[n][k] = bn[n][k - 1] * (n - k + 1) / k;
+  }
+  cudaMemcpyToSymbol(c_binom, bn, sizeof(bn));
   done = true;
 }
 
@@ -97,7 +105,7 @@ __device__ __forceinline__ void rys_one(const RysArgsG& ra, double T, int r, dou
 }
 
 template <int NAB1, int NCD1>
-__global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ items, int nitems,
+__global__ void __launch_bounds__(256, 2) grad_kernel(const GradItem* __restrict__ items, int nitems,
                                                    const DPair* __restrict__ pairs, const double* __restrict__ prim,
                                                    int tot_np, const double* __restrict__ coef,
                                                    const double* __restrict__ Dm, int nbf, RysArgsG ra,
@@ -124,7 +132,8 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
   const bool multi = nc > 1;
   const int npab = P.np, npcd = Q.np;
   const int n1d = (la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-  const int scr = NI * (lb + 2) * NJ + (la + 2) * (lb + 2) * NJ * (ld + 1);
+  const int nU = (la + 2) * (lb + 2) * (lc + 2) * (ld + 1);  // 2D-HRR table per (quartet, root, direction)
+  const int scr = NI * NJ + nU;                              // G (2D integrals) + U per job
   const int NT = PAB * PCD;
   const int CFT = NR * 10 + 4;  // per-quartet coefficient record
   // shared layout: Gam | Cab | Ccd | Y | union{ stage-0 temp | tile: cf, Gp, F, S }
@@ -211,7 +220,6 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
   const double ABx[3] = {P.A[0] - P.B[0], P.A[1] - P.B[1], P.A[2] - P.B[2]};
   const double CDx[3] = {Q.A[0] - Q.B[0], Q.A[1] - Q.B[1], Q.A[2] - Q.B[2]};
   const int ca0 = d_ccum(la), cb0 = d_ccum(lb), cc0 = d_ccum(lc), cd0 = d_ccum(ld);
-  const int LB2 = lb + 2, LD1 = ld + 1;
   for (int pcd0 = 0; pcd0 < npcd; pcd0 += PCD) {
     const int npc = min(PCD, npcd - pcd0);
     gsync(g, tpq);
@@ -276,52 +284,61 @@ __global__ void __launch_bounds__(256) grad_kernel(const GradItem* __restrict__ 
       gsync(g, tpq);
       for (int r0 = 0; r0 < NR; r0 += RW) {
       const int nrw = min(RW, NR - r0);
-      // ---- (2) 2D recursion, 2D-level HRR and derivative factors per (quartet, root, direction)
+      // ---- (2a) 2D recursion per (quartet, root, direction): G[e][f], e at A, f at C
       for (int job = tid; job < nt * nrw * 3; job += tpq) {
         const int d = job % 3, tr = job / 3, rl = tr % nrw, t = tr / nrw, r = r0 + rl;
         const double* c = cf + t * CFT + r * 10;
         const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
-        double* T = S + (size_t)job * scr;   // T[a][b][f]
-        double* U = T + NI * LB2 * NJ;       // U[a][b][c][d]
-        // 2D recursion written into the b = 0 plane of T
-        T[0] = d == 2 ? c[9] : 1.0;
-        if (NI > 1) T[LB2 * NJ] = C00 * T[0];
-        for (int i = 1; i < NI - 1; ++i) T[((i + 1) * LB2) * NJ] = C00 * T[(i * LB2) * NJ] + i * B10 * T[((i - 1) * LB2) * NJ];
+        double* G = S + (size_t)job * scr;
+        G[0] = d == 2 ? c[9] : 1.0;
+        if (NI > 1) G[NJ] = C00 * G[0];
+        for (int i = 1; i < NI - 1; ++i) G[(i + 1) * NJ] = C00 * G[i * NJ] + i * B10 * G[(i - 1) * NJ];
         for (int j = 0; j < NJ - 1; ++j)
           for (int i = 0; i < NI; ++i) {
-            double v = D00 * T[(i * LB2) * NJ + j];
-            if (j > 0) v += j * B01 * T[(i * LB2) * NJ + j - 1];
-            if (i > 0) v += i * B00 * T[((i - 1) * LB2) * NJ + j];
-            T[(i * LB2) * NJ + j + 1] = v;
+            double v = D00 * G[i * NJ + j];
+            if (j > 0) v += j * B01 * G[i * NJ + j - 1];
+            if (i > 0) v += i * B00 * G[(i - 1) * NJ + j];
+            G[i * NJ + j + 1] = v;
           }
+      }
+      gsync(g, tpq);
+      // ---- (2b) 2D-level HRR (HRR2Da/HRR2Db) in closed form, one table element per thread:
+      //      U[a][b][c][d] = sum_k C(b,k) AB^(b-k) sum_l C(d,l) CD^(d-l) G[a+k][c+l]
+      for (int o = tid; o < nt * nrw * 3 * nU; o += tpq) {
+        const int u = o % nU, job = o / nU, d = job % 3;
+        const int a = u % (la + 2), r1 = u / (la + 2), b = r1 % (lb + 2), r2 = r1 / (lb + 2);
+        const int cc = r2 % (lc + 2), dd = r2 / (lc + 2);
+        double* Gj = S + (size_t)job * scr;
+        if (a + b > NAB1 || cc + dd > NCD1) { Gj[NI * NJ + u] = 0.0; continue; }
         const double ab = ABx[d], cdv = CDx[d];
-        for (int b = 1; b < LB2; ++b)
-          for (int a = 0; a + b <= NAB1; ++a)
-            for (int f = 0; f < NJ; ++f)
-              T[(a * LB2 + b) * NJ + f] = T[((a + 1) * LB2 + b - 1) * NJ + f] + ab * T[(a * LB2 + b - 1) * NJ + f];
-        for (int a = 0; a < la + 2; ++a)
-          for (int b = 0; b < LB2; ++b) {
-            if (a + b > NAB1) continue;
-            double* u = U + ((a * LB2 + b) * NJ) * LD1;
-            for (int cc = 0; cc < NJ; ++cc) u[cc * LD1] = T[(a * LB2 + b) * NJ + cc];
-            for (int dd = 1; dd < LD1; ++dd)
-              for (int cc = 0; cc + dd <= NCD1; ++cc)
-                u[cc * LD1 + dd] = u[(cc + 1) * LD1 + dd - 1] + cdv * u[cc * LD1 + dd - 1];
+        double sum = 0.0, pk = 1.0;
+        for (int k = b; k >= 0; --k) {  // pk = AB^(b-k)
+          const double* gr = Gj + (a + k) * NJ + cc;
+          double inner = 0.0, pl = 1.0;
+          for (int l = dd; l >= 0; --l) {
+            inner = fma(c_binom[dd][l] * pl, gr[l], inner);
+            pl *= cdv;
           }
+          sum = fma(c_binom[b][k] * pk, inner, sum);
+          pk *= ab;
+        }
+        Gj[NI * NJ + u] = sum;
+      }
+      gsync(g, tpq);
+      // ---- (2c) derivative factors (Rys2Dg): 2a I(a+1) - a I(a-1) etc., one element per thread
+      for (int o = tid; o < nt * nrw * 3 * n1d; o += tpq) {
+        const int e1 = o % n1d, job = o / n1d, t = job / 3 / nrw;
+        const int a = e1 % (la + 1), r1 = e1 / (la + 1), b = r1 % (lb + 1), r2 = r1 / (lb + 1);
+        const int cc = r2 % (lc + 1), dd = r2 / (lc + 1);
+        const double* U = S + (size_t)job * scr + NI * NJ;
+        const int sa = 1, sb = la + 2, sc = (la + 2) * (lb + 2), sd = sc * (lc + 2);
+        const double* u0 = U + a * sa + b * sb + cc * sc + dd * sd;
         const double* e = cf + t * CFT + NR * 10;
-        const double ta = e[0], tb = e[1], tg = e[2];
-        double* Fo = F + ((size_t)(t * nrw + rl) * 3 + d) * 4 * n1d;
-        for (int dd = 0; dd <= ld; ++dd)
-          for (int cc = 0; cc <= lc; ++cc)
-            for (int b = 0; b <= lb; ++b)
-              for (int a = 0; a <= la; ++a) {
-                const int o = a + (la + 1) * (b + (lb + 1) * (cc + (lc + 1) * dd));
-                const double* u0 = U + (((a * LB2 + b) * NJ) + cc) * LD1 + dd;
-                Fo[o] = u0[0];
-                Fo[n1d + o] = ta * u0[LB2 * NJ * LD1] - (a ? a * u0[-LB2 * NJ * LD1] : 0.0);
-                Fo[2 * n1d + o] = tb * u0[NJ * LD1] - (b ? b * u0[-NJ * LD1] : 0.0);
-                Fo[3 * n1d + o] = tg * u0[LD1] - (cc ? cc * u0[-LD1] : 0.0);
-              }
+        double* Fo = F + (size_t)job * 4 * n1d;
+        Fo[e1] = u0[0];
+        Fo[n1d + e1] = e[0] * u0[sa] - (a ? a * u0[-sa] : 0.0);
+        Fo[2 * n1d + e1] = e[1] * u0[sb] - (b ? b * u0[-sb] : 0.0);
+        Fo[3 * n1d + e1] = e[2] * u0[sc] - (cc ? cc * u0[-sc] : 0.0);
       }
       gsync(g, tpq);
       // ---- (4) Assg1: sum over Cartesian components and roots
@@ -426,7 +443,7 @@ static size_t grad_group_smem(const DPair& P, const DPair& Q, int nijc, int nklc
   const size_t ncart4 = (size_t)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
   const size_t nsp4 = (size_t)ncomp(la) * ncomp(lb) * ncomp(lc) * ncomp(ld);
   const size_t n1d = (size_t)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-  const size_t scr = (size_t)NI * (lb + 2) * NJ + (size_t)(la + 2) * (lb + 2) * NJ * (ld + 1);
+  const size_t scr = (size_t)NI * NJ + (size_t)(la + 2) * (lb + 2) * (lc + 2) * (ld + 1);
   const size_t nij = nijc, nc = nij * nklc;
   const bool multi = nc > 1;
   const size_t fixed = nc * ncart4 + nij * P.np + (size_t)nklc * Q.np + (multi ? nij * pcd * ncart4 : 0);
@@ -498,27 +515,47 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
       return w;
     };
     const int NRc = (c_nab1(key) + c_ncd1(key) + 1) / 2;
-    const size_t budget = std::max(kGradCtaBudget, std::min(kGradMaxBudget, worst(1, 1, NRc)));
     const Mx& m = mx[key];
-    int pab = std::max(1, std::min(m.npab, 8)), pcd = std::max(1, std::min(m.npcd, 4)), rw = NRc;
-    size_t need = worst(pab, pcd, rw);
-    while (need > budget && (pab > 1 || pcd > 1 || rw > 1)) {
-      if (pcd > 1) pcd = (pcd + 1) / 2;
-      else if (pab > 1) pab = (pab + 1) / 2;
-      else --rw;
-      need = worst(pab, pcd, rw);
+    // widest per-quartet stage of the class (threads that can work at once)
+    size_t wmax = 0;
+    for (const GradItem& it : v) {
+      const DPair &P = h->pairs[it.p], &Q = h->pairs[it.q];
+      const size_t n4 = (size_t)ncart(P.la) * ncart(P.lb) * ncart(Q.la) * ncart(Q.lb);
+      const size_t nU = (size_t)(P.la + 2) * (P.lb + 2) * (Q.la + 2) * (Q.lb + 1);
+      wmax = std::max({wmax, n4, (size_t)3 * NRc * nU});
     }
     GradClass c;
+    c.tpq = 0;
+    // try budgets (per CTA) and thread counts per quartet; 256 threads per CTA
+    const size_t budgets[3] = {kGradCtaBudget, 112 * 1024 / 8, kGradMaxBudget};
+    for (size_t cta : budgets) {
+      for (int tpq = wmax <= 64 ? 64 : wmax <= 512 ? 128 : 256; tpq <= 256 && !c.tpq; tpq *= 2) {
+        const int groups = 256 / tpq;
+        const size_t gb = cta / groups;
+        int pab = std::max(1, std::min(m.npab, 8)), pcd = std::max(1, std::min(m.npcd, 4)), rw = NRc;
+        size_t need = worst(pab, pcd, rw);
+        while (need > gb && (pab > 1 || pcd > 1 || rw > 1)) {
+          if (pcd > 1) pcd = (pcd + 1) / 2;
+          else if (pab > 1) pab = (pab + 1) / 2;
+          else --rw;
+          need = worst(pab, pcd, rw);
+        }
+        if (need <= gb) {
+          c.tpq = tpq;
+          c.groups = groups;
+          c.gsm = (int)((need + 1) & ~(size_t)1);
+          c.rw = rw;
+          c.pab = pab;
+          c.pcd = pcd;
+        }
+      }
+      if (c.tpq) break;
+    }
+    if (!c.tpq) { h->err = "gradient class does not fit in shared memory"; return MG_ERR_ARG; }
     c.nab1 = key / 8;
     c.ncd1 = key % 8;
     c.begin = plan.items.size();
     c.count = v.size();
-    c.tpq = 64;
-    c.gsm = (int)((need + 1) & ~(size_t)1);
-    c.groups = (int)std::max<size_t>(1, std::min<size_t>(4, kGradMaxBudget / c.gsm));
-    c.rw = rw;
-    c.pab = pab;
-    c.pcd = pcd;
     plan.items.insert(plan.items.end(), v.begin(), v.end());
     plan.classes.push_back(c);
   }
