@@ -105,7 +105,7 @@ __device__ __forceinline__ void rys_one(const RysArgsG& ra, double T, int r, dou
 }
 
 template <int NAB1, int NCD1>
-__global__ void __launch_bounds__(256, 2) grad_kernel(const GradItem* __restrict__ items, int nitems,
+__global__ void __launch_bounds__(256, 3) grad_kernel(const GradItem* __restrict__ items, int nitems,
                                                    const DPair* __restrict__ pairs, const double* __restrict__ prim,
                                                    int tot_np, const double* __restrict__ coef,
                                                    const double* __restrict__ Dm, int nbf, RysArgsG ra,
@@ -478,9 +478,10 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
           if (P.atom_a == P.atom_b && P.atom_a == Q.atom_a && P.atom_a == Q.atom_b) continue;
           const int deg = (i == j ? 1 : 2) * (k == l ? 1 : 2) * (p == q ? 1 : 2);
           const int nkl = Q.nci * Q.ncj, nij = P.nci * P.ncj;
-          // chunk the contracted block (kl first, then ij) until one quartet tile fits
+          // chunk the contracted block (kl first, then ij) only when one quartet tile
+          // cannot fit at all: every chunk repeats the primitive-quartet work
           int ckl = nkl, cij = nij;
-          while ((ckl > 1 || cij > 1) && grad_group_smem(P, Q, cij, ckl, 1, 1, 1) > kGradCtaBudget) {
+          while ((ckl > 1 || cij > 1) && grad_group_smem(P, Q, cij, ckl, 1, 1, 1) > kGradMaxBudget) {
             if (ckl > 1) ckl = (ckl + 1) / 2;
             else cij = (cij + 1) / 2;
           }
