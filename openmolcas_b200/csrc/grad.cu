@@ -132,8 +132,8 @@ __global__ void __launch_bounds__(256, 3) grad_kernel(const GradItem* __restrict
   const bool multi = nc > 1;
   const int npab = P.np, npcd = Q.np;
   const int n1d = (la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-  const int nU = (la + 2) * (lb + 2) * (lc + 2) * (ld + 1);  // 2D-HRR table per (quartet, root, direction)
-  const int scr = NI * NJ + nU;                              // G (2D integrals) + U per job
+  const int nV = NI * (lc + 2) * (ld + 1);  // ket-transferred 2D integrals per job
+  const int scr = NI * NJ + nV;             // G + V per job
   const int NT = PAB * PCD;
   const int CFT = NR * 10 + 4;  // per-quartet coefficient record
   // shared layout: Gam | Cab | Ccd | Y | union{ stage-0 temp | tile: cf, Gp, F, S }
@@ -302,43 +302,47 @@ __global__ void __launch_bounds__(256, 3) grad_kernel(const GradItem* __restrict
           }
       }
       gsync(g, tpq);
-      // ---- (2b) 2D-level HRR (HRR2Da/HRR2Db) in closed form, one table element per thread:
-      //      U[a][b][c][d] = sum_k C(b,k) AB^(b-k) sum_l C(d,l) CD^(d-l) G[a+k][c+l]
-      for (int o = tid; o < nt * nrw * 3 * nU; o += tpq) {
-        const int u = o % nU, job = o / nU, d = job % 3;
-        const int a = u % (la + 2), r1 = u / (la + 2), b = r1 % (lb + 2), r2 = r1 / (lb + 2);
-        const int cc = r2 % (lc + 2), dd = r2 / (lc + 2);
+      // ---- (2b) ket 2D-level HRR (HRR2Db): V[e][c][d] = sum_l C(d,l) CD^(d-l) G[e][c+l]
+      for (int o = tid; o < nt * nrw * 3 * nV; o += tpq) {
+        const int v = o % nV, job = o / nV, d = job % 3;
+        const int e = v % NI, r1 = v / NI, cc = r1 % (lc + 2), dd = r1 / (lc + 2);
         double* Gj = S + (size_t)job * scr;
-        if (a + b > NAB1 || cc + dd > NCD1) { Gj[NI * NJ + u] = 0.0; continue; }
-        const double ab = ABx[d], cdv = CDx[d];
-        double sum = 0.0, pk = 1.0;
-        for (int k = b; k >= 0; --k) {  // pk = AB^(b-k)
-          const double* gr = Gj + (a + k) * NJ + cc;
-          double inner = 0.0, pl = 1.0;
+        double out = 0.0;
+        if (cc + dd <= NCD1) {
+          const double cdv = CDx[d];
+          const double* gr = Gj + e * NJ + cc;
+          double pl = 1.0;
           for (int l = dd; l >= 0; --l) {
-            inner = fma(c_binom[dd][l] * pl, gr[l], inner);
+            out = fma(c_binom[dd][l] * pl, gr[l], out);
             pl *= cdv;
           }
-          sum = fma(c_binom[b][k] * pk, inner, sum);
-          pk *= ab;
         }
-        Gj[NI * NJ + u] = sum;
+        Gj[NI * NJ + v] = out;
       }
       gsync(g, tpq);
-      // ---- (2c) derivative factors (Rys2Dg): 2a I(a+1) - a I(a-1) etc., one element per thread
+      // ---- (2c) bra 2D-level HRR (HRR2Da) folded into the derivative factors (Rys2Dg):
+      //      U(a,b,c,d) = sum_k C(b,k) AB^(b-k) V[a+k][c][d];  F = U, 2a U(a+1) - a U(a-1), ...
       for (int o = tid; o < nt * nrw * 3 * n1d; o += tpq) {
-        const int e1 = o % n1d, job = o / n1d, t = job / 3 / nrw;
+        const int e1 = o % n1d, job = o / n1d, d = job % 3, t = job / 3 / nrw;
         const int a = e1 % (la + 1), r1 = e1 / (la + 1), b = r1 % (lb + 1), r2 = r1 / (lb + 1);
         const int cc = r2 % (lc + 1), dd = r2 / (lc + 1);
-        const double* U = S + (size_t)job * scr + NI * NJ;
-        const int sa = 1, sb = la + 2, sc = (la + 2) * (lb + 2), sd = sc * (lc + 2);
-        const double* u0 = U + a * sa + b * sb + cc * sc + dd * sd;
+        const double* Vj = S + (size_t)job * scr + NI * NJ;
+        const double ab = ABx[d];
+        auto U = [&](int ua, int ub, int uc) {
+          const double* V = Vj + uc * NI + dd * NI * (lc + 2);
+          double sum = 0.0, pk = 1.0;
+          for (int k = ub; k >= 0; --k) {
+            sum = fma(c_binom[ub][k] * pk, V[ua + k], sum);
+            pk *= ab;
+          }
+          return sum;
+        };
         const double* e = cf + t * CFT + NR * 10;
         double* Fo = F + (size_t)job * 4 * n1d;
-        Fo[e1] = u0[0];
-        Fo[n1d + e1] = e[0] * u0[sa] - (a ? a * u0[-sa] : 0.0);
-        Fo[2 * n1d + e1] = e[1] * u0[sb] - (b ? b * u0[-sb] : 0.0);
-        Fo[3 * n1d + e1] = e[2] * u0[sc] - (cc ? cc * u0[-sc] : 0.0);
+        Fo[e1] = U(a, b, cc);
+        Fo[n1d + e1] = e[0] * U(a + 1, b, cc) - (a ? a * U(a - 1, b, cc) : 0.0);
+        Fo[2 * n1d + e1] = e[1] * U(a, b + 1, cc) - (b ? b * U(a, b - 1, cc) : 0.0);
+        Fo[3 * n1d + e1] = e[2] * U(a, b, cc + 1) - (cc ? cc * U(a, b, cc - 1) : 0.0);
       }
       gsync(g, tpq);
       // ---- (4) Assg1: sum over Cartesian components and roots
@@ -443,7 +447,7 @@ static size_t grad_group_smem(const DPair& P, const DPair& Q, int nijc, int nklc
   const size_t ncart4 = (size_t)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
   const size_t nsp4 = (size_t)ncomp(la) * ncomp(lb) * ncomp(lc) * ncomp(ld);
   const size_t n1d = (size_t)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-  const size_t scr = (size_t)NI * NJ + (size_t)(la + 2) * (lb + 2) * (lc + 2) * (ld + 1);
+  const size_t scr = (size_t)NI * NJ + (size_t)NI * (lc + 2) * (ld + 1);
   const size_t nij = nijc, nc = nij * nklc;
   const bool multi = nc > 1;
   const size_t fixed = nc * ncart4 + nij * P.np + (size_t)nklc * Q.np + (multi ? nij * pcd * ncart4 : 0);
