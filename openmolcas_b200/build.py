@@ -7,15 +7,18 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmolgpu.so")
-SOURCES = ["basis_host.cu", "eri.cu", "cholesky.cu", "grad.cu", "jk.cu", "capi.cu", "eri_noalloc.cu"]
+OBJ = os.path.join(HERE, "_build")
+SOURCES = ["basis_host.cu", "eri.cu", "cholesky.cu", "grad.cu", "grad_k1.cu", "grad_k2.cu", "grad_k3.cu", "jk.cu",
+           "capi.cu", "eri_noalloc.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
 
 
@@ -32,17 +35,33 @@ def needs_build():
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, verbose=False):
+def build(force=False, verbose=False, jobs=None):
+    """Compile every source to an object (in parallel), then link the shared library."""
     if not force and not needs_build():
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB + ".tmp"] + sources() + ["-lcublas"]
+    os.makedirs(OBJ, exist_ok=True)
+
+    def compile_one(src):
+        obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
+        r = subprocess.run([nvcc] + NVCC_FLAGS + ["-c", src, "-o", obj], cwd=CSRC, capture_output=True, text=True)
+        return obj, r
+
+    with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
+        results = list(ex.map(compile_one, sources()))
+    log = ""
+    for obj, r in results:
+        log += r.stdout + r.stderr
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp"] + \
+        [o for o, _ in results] + ["-lcublas"]
     r = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     os.replace(LIB + ".tmp", LIB)
     if verbose:
-        print(r.stdout + r.stderr)
+        print(log + r.stdout + r.stderr)
     return LIB
 
 

@@ -1,0 +1,7 @@
+// Gradient kernel instantiations for 2 resident CTA(s) per SM (register
+// budget of __launch_bounds__(256, 2)); see grad_kernel.cuh.
+#include "grad_kernel.cuh"
+
+namespace mg {
+GradFn grad_kernel_m2(int nab1, int ncd1) { return grad_pick<2>(nab1, ncd1); }
+}  // namespace mg

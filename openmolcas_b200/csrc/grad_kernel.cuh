@@ -1,0 +1,472 @@
+// Two-electron gradient kernel (FP64), one template instantiated per
+// (la+lb+1, lc+ld+1) class and per occupancy target (minimum CTAs per SM,
+// which sets the register budget).  The algorithm and its reference anchors
+// are described in grad.cu; the instantiations live in grad_k{1,2,3}.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "mg_internal.h"
+
+namespace mg {
+
+struct RysArgsG {
+  RysMeta m[MG_MAX_RYS];
+  const double* tab;
+};
+
+// Per-CTA table block (doubles), copied from global memory at kernel start:
+// Cartesian -> spherical matrices for l = 0..3 (column m, row Cartesian),
+// binomial coefficients C(n, k) for n, k <= 8, and the Cartesian exponents of
+// l = 0..7 in C3 order packed as x | y << 8 | z << 16 (ints).
+constexpr int kGTabSph = 0;
+constexpr int kGTabBinom = 110;
+constexpr int kGTabCart = 191;  // 120 ints = 60 doubles
+constexpr int kGTabD = 252;
+
+struct GradArgs {
+  const GradItem* items;
+  int nitems;
+  const DPair* pairs;
+  const double* prim;
+  int tot_np;
+  const double* coef;
+  const double* Dm;
+  int nbf;
+  const double* gtab;
+  double* grad;
+  int tpq, gsm, PAB, PCD, RW;
+};
+
+using GradFn = void (*)(GradArgs, RysArgsG);
+GradFn grad_kernel_m1(int nab1, int ncd1);
+GradFn grad_kernel_m2(int nab1, int ncd1);
+GradFn grad_kernel_m3(int nab1, int ncd1);
+
+__device__ __forceinline__ void gsync(int g, int tpq) {
+  if (tpq == 32) __syncwarp();
+  else asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(tpq) : "memory");
+}
+
+__device__ __forceinline__ int d_ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__device__ __forceinline__ int d_ncomp(int l) { return l >= 2 ? 2 * l + 1 : d_ncart(l); }
+__device__ __forceinline__ int d_ccum(int l) { return l * (l + 1) * (l + 2) / 6; }
+__device__ __forceinline__ int d_sph_off(int l) { return l == 0 ? 0 : l == 1 ? 1 : l == 2 ? 10 : 40; }
+__device__ __forceinline__ int ev2(int x) { return (x + 1) & ~1; }
+
+// Division by a run-time divisor n through a multiply-high:
+// q = floor(o * ceil(2^32 / n) / 2^32), exact for o < 2^32 / n (the host
+// planner checks every loop extent against that bound); n = 1 uses the mask.
+struct FDiv {
+  unsigned m, k, n;
+};
+__device__ __forceinline__ FDiv fdiv(unsigned n) {
+  FDiv f;
+  f.n = n;
+  f.m = n == 1 ? 0u : 0xFFFFFFFFu / n + 1u;
+  f.k = n == 1 ? 0xFFFFFFFFu : 0u;
+  return f;
+}
+__device__ __forceinline__ unsigned fq(unsigned o, const FDiv& f) { return __umulhi(o, f.m) + (o & f.k); }
+
+// one Rys root/weight of order N at T (table or asymptotic)
+template <int N>
+__device__ __forceinline__ void rys_one(const RysArgsG& ra, double T, int r, double& x, double& w) {
+  const RysMeta& m = ra.m[N - 1];
+  if (T >= m.tmax) {
+    const double ai = 1.0 / T;
+    x = m.hx[r] * ai;
+    w = m.hw[r] * sqrt(ai);
+  } else {
+    int k = (int)(T * m.invh);
+    k = k < m.K ? k : m.K - 1;
+    const double s = 2.0 * (T - k * m.h) * m.invh - 1.0;
+    const double* c = ra.tab + m.off + (size_t)k * (2 * N * 8);
+    const double* cx = c + r * 8;
+    const double* cw = c + (N + r) * 8;
+    double ax = __ldg(cx + 7), aw = __ldg(cw + 7);
+#pragma unroll
+    for (int j = 6; j >= 0; --j) {
+      ax = fma(ax, s, __ldg(cx + j));
+      aw = fma(aw, s, __ldg(cw + j));
+    }
+    x = ax;
+    w = aw;
+  }
+}
+
+// Per-group shared layout (doubles, every region starts on an even offset):
+//   hdr[8] (AB, CD) | Gam | Cab | Ccd | Y | union{ stage-0 temp | reduction |
+//   tile: cf | Gp | F | S }
+// F holds, per (quartet, root, direction), the 2D integral and its three
+// centre derivatives interleaved: F[(job * n1d + e1) * 4 + {0: I, 1: dA, 2: dB, 3: dC}].
+template <int NAB1, int NCD1, int MINB>
+__global__ void __launch_bounds__(256, MINB) grad_kernel(const GradArgs a, const RysArgsG ra) {
+  constexpr int NR = (NAB1 + NCD1 + 1) / 2;
+  constexpr int NI = NAB1 + 1, NJ = NCD1 + 1;
+  extern __shared__ __align__(16) double smem_all[];
+  double* tabs = smem_all;
+  for (int o = threadIdx.x; o < kGTabD; o += blockDim.x) tabs[o] = a.gtab[o];
+  __syncthreads();
+  const int tpq = a.tpq;
+  const int g = threadIdx.x / tpq;
+  const int item = blockIdx.x * (blockDim.x / tpq) + g;
+  if (item >= a.nitems) return;
+  const int tid = threadIdx.x - g * tpq;
+  double* sm = smem_all + kGTabD + (size_t)g * a.gsm;
+  const double* bn = tabs + kGTabBinom;
+  const int* cart = reinterpret_cast<const int*>(tabs + kGTabCart);
+  const double* prim = a.prim;
+  const int tot_np = a.tot_np;
+  const GradItem it = a.items[item];
+  const DPair& P = a.pairs[it.p];
+  const DPair& Q = a.pairs[it.q];
+  const int la = P.la, lb = P.lb, lc = Q.la, ld = Q.lb;
+  const int nca = d_ncart(la), ncb = d_ncart(lb), ncc = d_ncart(lc), ncd = d_ncart(ld);
+  const int nsa = d_ncomp(la), nsb = d_ncomp(lb), nsc = d_ncomp(lc), nsd = d_ncomp(ld);
+  const int ncart4 = nca * ncb * ncc * ncd;
+  const int nij = it.i1 - it.i0;   // bra contracted pairs [i0, i1)
+  const int nklc = it.c1 - it.c0;  // ket contracted pairs [c0, c1)
+  const int nc = nij * nklc;
+  const bool multi = nc > 1;
+  const int npab = P.np, npcd = Q.np;
+  const int n1d = (la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
+  const int nV = NI * (lc + 2) * (ld + 1);  // ket-transferred 2D integrals per job
+  const int scr = NI * NJ + nV;             // G + V per job
+  const int PAB = a.PAB, PCD = a.PCD, RW = a.RW;
+  const int NT = PAB * PCD;
+  const int CFT = NR * 10 + 4;  // per-quartet coefficient record
+  double* hdr = sm;
+  double* Gam = hdr + 8;                              // nc * ncart4, index il + nc * abcd
+  double* Cab = Gam + ev2(nc * ncart4);               // nij * npab
+  double* Ccd = Cab + ev2(nij * npab);                // nklc * npcd
+  double* Y = Ccd + ev2(nklc * npcd);                 // nij * PCD * ncart4 (multi only)
+  double* U0 = Y + (multi ? ev2(nij * PCD * ncart4) : 0);
+  double* Tmp = U0;                                   // stage-0 temp (nc * ncart4)
+  double* cf = U0;                                    // NT * CFT
+  double* Gp = cf + ev2(NT * CFT);                    // NT * ncart4 (multi only)
+  double* F = Gp + (multi ? ev2(NT * ncart4) : 0);    // NT * RW * 3 * 4 * n1d
+  double* S = F + NT * RW * 12 * n1d;                 // NT * 3 * RW * scr
+  if (tid < 3) {
+    hdr[tid] = P.A[tid] - P.B[tid];
+    hdr[3 + tid] = Q.A[tid] - Q.B[tid];
+  }
+  for (int o = tid; o < nij * npab; o += tpq) Cab[o] = a.coef[P.coef_off + (size_t)it.i0 * npab + o];
+  for (int o = tid; o < nklc * npcd; o += tpq) Ccd[o] = a.coef[Q.coef_off + (size_t)it.c0 * npcd + o];
+  // ---- stage 0: contracted 2-PDM (PGet1), spherical, then -> Cartesian
+  {
+    const double* Dm = a.Dm;
+    const size_t nbf = a.nbf;
+    const int nsp4 = nsa * nsb * nsc * nsd;
+    for (int o = tid; o < nc * nsp4; o += tpq) {
+      const int il = o % nc, r1 = o / nc;
+      const int sa = r1 % nsa, r2 = r1 / nsa, sb = r2 % nsb, r3 = r2 / nsb, sc = r3 % nsc, sd = r3 / nsc;
+      const int ij = it.i0 + il % nij, kl = it.c0 + il / nij;
+      const int ki = ij % P.nci, kj = ij / P.nci, kk = kl % Q.nci, kq = kl / Q.nci;
+      const int pa = P.ao_a + sa * P.nci + ki, pb = P.ao_b + sb * P.ncj + kj;
+      const int pc = Q.ao_a + sc * Q.nci + kk, pd = Q.ao_b + sd * Q.ncj + kq;
+      Tmp[o] = Dm[pa * nbf + pb] * Dm[pc * nbf + pd] -
+               0.25 * (Dm[pa * nbf + pc] * Dm[pb * nbf + pd] + Dm[pa * nbf + pd] * Dm[pb * nbf + pc]);
+    }
+    gsync(g, tpq);
+    const double* Sd = tabs + kGTabSph + d_sph_off(ld);
+    const double* Sc = tabs + kGTabSph + d_sph_off(lc);
+    const double* Sb = tabs + kGTabSph + d_sph_off(lb);
+    const double* Sa = tabs + kGTabSph + d_sph_off(la);
+    {  // d: [il][sa][sb][sc][sd] -> [il][sa][sb][sc][cd]   (Tmp -> Gam)
+      const int inner = nc * nsa * nsb * nsc;
+      for (int o = tid; o < inner * ncd; o += tpq) {
+        const int in = o % inner, cd = o / inner;
+        double s = 0;
+        for (int m = 0; m < nsd; ++m) s = fma(Sd[cd + ncd * m], Tmp[in + inner * m], s);
+        Gam[o] = s;
+      }
+      gsync(g, tpq);
+    }
+    {  // c  (Gam -> Tmp)
+      const int inner = nc * nsa * nsb;
+      for (int o = tid; o < inner * ncc * ncd; o += tpq) {
+        const int in = o % inner, r1 = o / inner, cc = r1 % ncc, cd = r1 / ncc;
+        double s = 0;
+        for (int m = 0; m < nsc; ++m) s = fma(Sc[cc + ncc * m], Gam[in + inner * (m + nsc * cd)], s);
+        Tmp[o] = s;
+      }
+      gsync(g, tpq);
+    }
+    {  // b  (Tmp -> Gam)
+      const int inner = nc * nsa;
+      const int outer = ncc * ncd;
+      for (int o = tid; o < inner * ncb * outer; o += tpq) {
+        const int in = o % inner, r1 = o / inner, cb = r1 % ncb, ou = r1 / ncb;
+        double s = 0;
+        for (int m = 0; m < nsb; ++m) s = fma(Sb[cb + ncb * m], Tmp[in + inner * (m + nsb * ou)], s);
+        Gam[o] = s;
+      }
+      gsync(g, tpq);
+    }
+    {  // a  (Gam -> Tmp -> Gam)
+      const int outer = ncb * ncc * ncd;
+      for (int o = tid; o < nc * nca * outer; o += tpq) {
+        const int il = o % nc, r1 = o / nc, ca = r1 % nca, ou = r1 / nca;
+        double s = 0;
+        for (int m = 0; m < nsa; ++m) s = fma(Sa[ca + nca * m], Gam[il + nc * (m + nsa * ou)], s);
+        Tmp[o] = s;
+      }
+      gsync(g, tpq);
+      for (int o = tid; o < nc * ncart4; o += tpq) Gam[o] = Tmp[o];
+      gsync(g, tpq);
+    }
+  }
+  double acc[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+  const int ca0 = d_ccum(la), cb0 = d_ccum(lb), cc0 = d_ccum(lc), cd0 = d_ccum(ld);
+  // Assg1 thread map: TA threads over Cartesian quartets x TT threads over primitive quartets
+  const int TA = ncart4 < tpq ? ncart4 : tpq;
+  const int TT = tpq / TA;
+  const int aslot = tid % TA, tslot = tid / TA;
+  for (int pcd0 = 0; pcd0 < npcd; pcd0 += PCD) {
+    const int npc = min(PCD, npcd - pcd0);
+    gsync(g, tpq);
+    // ---- ket half-transform of the 2-PDM: Y[ij][pc][abcd] = sum_kl Ccd[kl][pc] Gam[ij,kl][abcd]
+    if (multi) {
+      for (int o = tid; o < nij * npc * ncart4; o += tpq) {
+        const int ij = o % nij, r1 = o / nij, pc = r1 % npc, abcd = r1 / npc;
+        double s = 0.0;
+        for (int klc = 0; klc < nklc; ++klc) s = fma(Ccd[klc * npcd + pcd0 + pc], Gam[ij + nij * klc + nc * abcd], s);
+        Y[ij + nij * (pc + PCD * abcd)] = s;
+      }
+    }
+    for (int pab0 = 0; pab0 < npab; pab0 += PAB) {
+      const int npa = min(PAB, npab - pab0);
+      const int nt = npa * npc;
+      const FDiv fnpa = fdiv(npa);
+      gsync(g, tpq);
+      // ---- (1) roots: one (quartet, root) per thread
+      for (int job = tid; job < nt * NR; job += tpq) {
+        const int r = job % NR, t = job / NR;
+        const int pc = fq(t, fnpa), pa = t - pc * npa;
+        const int ia = P.prim_off + pab0 + pa, ic = Q.prim_off + pcd0 + pc;
+        const double zeta = prim[ia], eta = prim[ic];
+        const double px = prim[2 * tot_np + ia], py = prim[3 * tot_np + ia], pz = prim[4 * tot_np + ia];
+        const double qx = prim[2 * tot_np + ic], qy = prim[3 * tot_np + ic], qz = prim[4 * tot_np + ic];
+        const double ze = zeta + eta, zei = 1.0 / ze, rho = zeta * eta * zei;
+        const double dx = px - qx, dy = py - qy, dz = pz - qz;
+        const double T = rho * (dx * dx + dy * dy + dz * dz);
+        const double fact = prim[tot_np + ia] * prim[tot_np + ic] * sqrt(zei);
+        double x, w;
+        rys_one<NR>(ra, T, r, x, w);
+        const double U2 = x * zei;
+        double* c = cf + t * CFT + r * 10;
+        c[0] = 0.5 * U2;
+        c[1] = 0.5 * (1.0 - U2 * eta) / zeta;
+        c[2] = 0.5 * (1.0 - U2 * zeta) / eta;
+        c[3] = px - P.A[0] - eta * U2 * dx;
+        c[4] = py - P.A[1] - eta * U2 * dy;
+        c[5] = pz - P.A[2] - eta * U2 * dz;
+        c[6] = qx - Q.A[0] + zeta * U2 * dx;
+        c[7] = qy - Q.A[1] + zeta * U2 * dy;
+        c[8] = qz - Q.A[2] + zeta * U2 * dz;
+        c[9] = w * fact;
+        if (r == 0) {
+          double* e = cf + t * CFT + NR * 10;
+          e[0] = 2.0 * prim[5 * tot_np + ia];         // 2 alpha
+          e[1] = 2.0 * prim[6 * tot_np + ia];         // 2 beta
+          e[2] = 2.0 * prim[5 * tot_np + ic];         // 2 gamma
+          e[3] = Cab[pab0 + pa] * Ccd[pcd0 + pc];     // single-contraction coefficient
+        }
+      }
+      // ---- (3) primitive 2-PDM (Tcrtnc) by the bra half-transform
+      if (multi) {
+        const FDiv f4 = fdiv(ncart4);
+        for (int o = tid; o < nt * ncart4; o += tpq) {
+          const int t = fq(o, f4), abcd = o - t * ncart4;
+          const int pc = fq(t, fnpa), pa = t - pc * npa;
+          const double* y = Y + nij * (pc + PCD * abcd);
+          double s = 0.0;
+          for (int ij = 0; ij < nij; ++ij) s = fma(Cab[ij * npab + pab0 + pa], y[ij], s);
+          Gp[t * ncart4 + abcd] = s;
+        }
+      }
+      gsync(g, tpq);
+      for (int r0 = 0; r0 < NR; r0 += RW) {
+        const int nrw = min(RW, NR - r0);
+        const FDiv fnrw = fdiv(nrw);
+        // ---- (2a) 2D recursion per (quartet, root, direction): G[e][f], e at A, f at C
+        for (int job = tid; job < nt * nrw * 3; job += tpq) {
+          const int d = job % 3, tr = job / 3, t = fq(tr, fnrw), rl = tr - t * nrw, r = r0 + rl;
+          const double* c = cf + t * CFT + r * 10;
+          const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
+          double* G = S + (size_t)job * scr;
+          G[0] = d == 2 ? c[9] : 1.0;
+          if (NI > 1) G[NJ] = C00 * G[0];
+          for (int i = 1; i < NI - 1; ++i) G[(i + 1) * NJ] = C00 * G[i * NJ] + i * B10 * G[(i - 1) * NJ];
+          for (int j = 0; j < NJ - 1; ++j)
+            for (int i = 0; i < NI; ++i) {
+              double v = D00 * G[i * NJ + j];
+              if (j > 0) v += j * B01 * G[i * NJ + j - 1];
+              if (i > 0) v += i * B00 * G[(i - 1) * NJ + j];
+              G[i * NJ + j + 1] = v;
+            }
+        }
+        gsync(g, tpq);
+        // ---- (2b) ket 2D-level HRR (HRR2Db): V[e][c][d] = sum_l C(d,l) CD^(d-l) G[e][c+l]
+        {
+          const FDiv fnv = fdiv(nV), flc2 = fdiv(lc + 2);
+          for (int o = tid; o < nt * nrw * 3 * nV; o += tpq) {
+            const int job = fq(o, fnv), v = o - job * nV, d = job % 3;
+            const int e = v % NI, r1 = v / NI, dd = fq(r1, flc2), cc = r1 - dd * (lc + 2);
+            double* Gj = S + (size_t)job * scr;
+            double out = 0.0;
+            if (cc + dd <= NCD1) {
+              const double cdv = hdr[3 + d];
+              const double* gr = Gj + e * NJ + cc;
+              const double* bd = bn + 9 * dd;
+              double pl = 1.0;
+              for (int l = dd; l >= 0; --l) {
+                out = fma(bd[l] * pl, gr[l], out);
+                pl *= cdv;
+              }
+            }
+            Gj[NI * NJ + v] = out;
+          }
+        }
+        gsync(g, tpq);
+        // ---- (2c) bra 2D-level HRR (HRR2Da) folded into the derivative factors (Rys2Dg):
+        //      U(a,b,c,d) = sum_k C(b,k) AB^(b-k) V[a+k][c][d];  F = U, 2a U(a+1) - a U(a-1), ...
+        {
+          const FDiv fn1 = fdiv(n1d), fa1 = fdiv(la + 1), fb1 = fdiv(lb + 1), fc1 = fdiv(lc + 1);
+          const FDiv f3rw = fdiv(3 * nrw);
+          for (int o = tid; o < nt * nrw * 3 * n1d; o += tpq) {
+            const int job = fq(o, fn1), e1 = o - job * n1d, d = job % 3, t = fq(job, f3rw);
+            const int r1 = fq(e1, fa1), aa = e1 - r1 * (la + 1);
+            const int r2 = fq(r1, fb1), b = r1 - r2 * (lb + 1);
+            const int dd = fq(r2, fc1), cc = r2 - dd * (lc + 1);
+            const double* Vj = S + (size_t)job * scr + NI * NJ + dd * NI * (lc + 2);
+            const double ab = hdr[d];
+            auto U = [&](int ua, int ub, int uc) {
+              const double* V = Vj + uc * NI + ua;
+              const double* bu = bn + 9 * ub;
+              double sum = 0.0, pk = 1.0;
+              for (int k = ub; k >= 0; --k) {
+                sum = fma(bu[k] * pk, V[k], sum);
+                pk *= ab;
+              }
+              return sum;
+            };
+            const double* e = cf + t * CFT + NR * 10;
+            double2* Fo = reinterpret_cast<double2*>(F + ((size_t)job * n1d + e1) * 4);
+            double2 v01, v23;
+            v01.x = U(aa, b, cc);
+            v01.y = e[0] * U(aa + 1, b, cc) - (aa ? aa * U(aa - 1, b, cc) : 0.0);
+            v23.x = e[1] * U(aa, b + 1, cc) - (b ? b * U(aa, b - 1, cc) : 0.0);
+            v23.y = e[2] * U(aa, b, cc + 1) - (cc ? cc * U(aa, b, cc - 1) : 0.0);
+            Fo[0] = v01;
+            Fo[1] = v23;
+          }
+        }
+        gsync(g, tpq);
+        // ---- (4) Assg1: sum over Cartesian components and roots; each thread
+        //      decomposes its Cartesian quartets once and walks the primitive quartets
+        if (tslot < TT) {
+          const FDiv fca = fdiv(nca), fcb = fdiv(ncb), fcc = fdiv(ncc);
+          const int n1d4 = 4 * n1d;
+          for (int abcd = aslot; abcd < ncart4; abcd += TA) {
+            const int r1 = fq(abcd, fca), ca = abcd - r1 * nca;
+            const int r2 = fq(r1, fcb), cb = r1 - r2 * ncb;
+            const int cd = fq(r2, fcc), cc = r2 - cd * ncc;
+            const int ea = cart[ca0 + ca], eb = cart[cb0 + cb], ec = cart[cc0 + cc], ed = cart[cd0 + cd];
+            int idx[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const int sh = 8 * d;
+              idx[d] = 4 * (((ea >> sh) & 255) +
+                            (la + 1) * (((eb >> sh) & 255) +
+                                        (lb + 1) * (((ec >> sh) & 255) + (lc + 1) * ((ed >> sh) & 255))));
+            }
+            for (int t = tslot; t < nt; t += TT) {
+              const double gm = multi ? Gp[t * ncart4 + abcd] : cf[t * CFT + NR * 10 + 3] * Gam[abcd];
+              if (gm == 0.0) continue;
+              const double* Fb = F + (size_t)t * nrw * 3 * n1d4;
+              for (int rl = 0; rl < nrw; ++rl, Fb += 3 * n1d4) {
+                const double2 x01 = *reinterpret_cast<const double2*>(Fb + idx[0]);
+                const double2 x23 = *reinterpret_cast<const double2*>(Fb + idx[0] + 2);
+                const double2 y01 = *reinterpret_cast<const double2*>(Fb + n1d4 + idx[1]);
+                const double2 y23 = *reinterpret_cast<const double2*>(Fb + n1d4 + idx[1] + 2);
+                const double2 z01 = *reinterpret_cast<const double2*>(Fb + 2 * n1d4 + idx[2]);
+                const double2 z23 = *reinterpret_cast<const double2*>(Fb + 2 * n1d4 + idx[2] + 2);
+                const double gyz = gm * y01.x * z01.x, gxz = gm * x01.x * z01.x, gxy = gm * x01.x * y01.x;
+                acc[0] = fma(gyz, x01.y, acc[0]);
+                acc[1] = fma(gxz, y01.y, acc[1]);
+                acc[2] = fma(gxy, z01.y, acc[2]);
+                acc[3] = fma(gyz, x23.x, acc[3]);
+                acc[4] = fma(gxz, y23.x, acc[4]);
+                acc[5] = fma(gxy, z23.x, acc[5]);
+                acc[6] = fma(gyz, x23.y, acc[6]);
+                acc[7] = fma(gxz, y23.y, acc[7]);
+                acc[8] = fma(gxy, z23.y, acc[8]);
+              }
+            }
+          }
+        }
+        gsync(g, tpq);
+      }  // root waves
+    }
+  }
+  gsync(g, tpq);
+  // ---- reduce over the group, distribute to atoms (Distg1)
+  double* red = U0;  // tpq/32 * 9 doubles
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    double v = acc[k];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if ((tid & 31) == 0) red[(tid >> 5) * 9 + k] = v;
+  }
+  gsync(g, tpq);
+  if (tid < 9) {
+    double v = 0.0;
+    for (int w = 0; w < tpq / 32; ++w) v += red[w * 9 + tid];
+    v *= it.scale;
+    const int X = tid / 3, d = tid % 3;
+    const int atom = X == 0 ? P.atom_a : X == 1 ? P.atom_b : Q.atom_a;
+    atomicAdd(&a.grad[3 * atom + d], v);
+    atomicAdd(&a.grad[3 * Q.atom_b + d], -v);  // translational invariance
+  }
+}
+
+template <int MINB, int A, int B>
+GradFn grad_fn() {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(grad_kernel<A, B, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    attr = true;
+  }
+  return grad_kernel<A, B, MINB>;
+}
+template <int MINB, int A>
+GradFn grad_fn_b(int b) {
+  switch (b) {
+    case 1: return grad_fn<MINB, A, 1>();
+    case 2: return grad_fn<MINB, A, 2>();
+    case 3: return grad_fn<MINB, A, 3>();
+    case 4: return grad_fn<MINB, A, 4>();
+    case 5: return grad_fn<MINB, A, 5>();
+    case 6: return grad_fn<MINB, A, 6>();
+    case 7: return grad_fn<MINB, A, 7>();
+  }
+  return nullptr;
+}
+template <int MINB>
+GradFn grad_pick(int a, int b) {
+  switch (a) {
+    case 1: return grad_fn_b<MINB, 1>(b);
+    case 2: return grad_fn_b<MINB, 2>(b);
+    case 3: return grad_fn_b<MINB, 3>(b);
+    case 4: return grad_fn_b<MINB, 4>(b);
+    case 5: return grad_fn_b<MINB, 5>(b);
+    case 6: return grad_fn_b<MINB, 6>(b);
+    case 7: return grad_fn_b<MINB, 7>(b);
+  }
+  return nullptr;
+}
+
+}  // namespace mg

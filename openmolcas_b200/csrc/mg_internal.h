@@ -109,11 +109,13 @@ struct GradItem {
 };
 struct GradClass {
   int nab1, ncd1, begin, count, tpq, gsm, groups, rw, pab, pcd;
+  int minb;  // resident CTAs per SM the kernel variant is compiled for (1..3)
 };
 struct GradPlan {
   std::vector<GradItem> items;
   std::vector<GradClass> classes;
   GradItem* d_items = nullptr;
+  double* d_tab = nullptr;  // per-CTA tables of the gradient kernel
   double cutint = -1;
 };
 int grad_build(Handle* h, double cutint, GradPlan& plan);
