@@ -32,15 +32,7 @@ static int make_grad_tables(const Handle* h, double** d_tab) {
   int o = kGTabSph;
   for (int l = 0; l <= 3; ++l)
     for (double v : h->sph[l]) t[o++] = v;
-  if (o != kGTabBinom) return MG_ERR_ARG;
-  for (int n = 0; n <= 8; ++n) {
-    double c = 1.0;
-    t[kGTabBinom + 9 * n] = 1.0;
-    for (int k = 1; k <= n; ++k) {
-      c = c * (n - k + 1) / k;
-      t[kGTabBinom + 9 * n + k] = c;
-    }
-  }
+  if (o != kGTabCart) return MG_ERR_ARG;
   int* cart = reinterpret_cast<int*>(t.data() + kGTabCart);
   int k = 0;
   for (int l = 0; l <= 7; ++l)
@@ -244,12 +236,13 @@ void grad_free(GradPlan* p) {
 }
 
 // Algorithmic FP64 flop count of a gradient plan (FMA = 2): per primitive
-// quartet the Rys roots (2 x 7 FMA per root and weight + 30), per root and
-// direction the 2D recursion (4 NI NJ), 2D-level HRR (2 (lb+1) NI NJ +
-// 2 (la+2)(lb+2) NJ ld) and derivative factors (8 n1d), the bra half of the
-// primitive 2-PDM (2 nij ncart4 when nc > 1) and Assg1 (24 flops per
-// Cartesian quartet and root); per work item the 2-PDM, its spherical ->
-// Cartesian transform and the ket half of the de-contraction.
+// quartet the Rys roots (2 x 7 FMA per root and weight + 30); per root and
+// direction the 2D recursion (4 NI NJ), the ket transfer (2 NI NJ ld) and, per
+// (c, d) column, the bra transfer with the derivative factors
+// (3 NI + (lb+1)(8 (la+1) + 4 NI)); the bra half of the primitive 2-PDM
+// (2 nij ncart4 when nc > 1) and Assg1 (24 flops per Cartesian quartet and
+// root); per work item the 2-PDM, its spherical -> Cartesian transform and
+// the ket half of the de-contraction.
 double grad_plan_flops(const Handle* h, const GradPlan& plan) {
   double f = 0;
   for (const GradItem& it : plan.items) {
@@ -258,11 +251,10 @@ double grad_plan_flops(const Handle* h, const GradPlan& plan) {
     const int NI = la + lb + 2, NJ = lc + ld + 2, NR = (la + lb + lc + ld + 3) / 2;
     const double ncart4 = (double)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
     const double nsp4 = (double)ncomp(la) * ncomp(lb) * ncomp(lc) * ncomp(ld);
-    const double n1d = (double)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
     const int nij = it.i1 - it.i0, nklc = it.c1 - it.c0, nc = nij * nklc;
     const double per_prim = NR * 28.0 + 30.0 +
-                            3.0 * NR * (4.0 * NI * NJ + 2.0 * (lb + 1) * NI * NJ + 2.0 * (la + 2) * (lb + 2) * NJ * ld +
-                                        8.0 * n1d) +
+                            3.0 * NR * (4.0 * NI * NJ + 2.0 * NI * NJ * ld +
+                                        (lc + 1.0) * (ld + 1.0) * (3.0 * NI + (lb + 1.0) * (8.0 * (la + 1) + 4.0 * NI))) +
                             (nc > 1 ? 2.0 * nij * ncart4 : 0.0) + 24.0 * ncart4 * NR;
     const double per_item = nc * nsp4 * 8.0 + 2.0 * nc * ncart4 * 4.0 * std::max(ncomp(la), ncomp(ld)) +
                             (nc > 1 ? 2.0 * nc * ncart4 * Q.np : 0.0);

@@ -15,13 +15,12 @@ struct RysArgsG {
 };
 
 // Per-CTA table block (doubles), copied from global memory at kernel start:
-// Cartesian -> spherical matrices for l = 0..3 (column m, row Cartesian),
-// binomial coefficients C(n, k) for n, k <= 8, and the Cartesian exponents of
-// l = 0..7 in C3 order packed as x | y << 8 | z << 16 (ints).
+// Cartesian -> spherical matrices for l = 0..3 (column m, row Cartesian) and
+// the Cartesian exponents of l = 0..7 in C3 order packed as
+// x | y << 8 | z << 16 (ints).
 constexpr int kGTabSph = 0;
-constexpr int kGTabBinom = 110;
-constexpr int kGTabCart = 191;  // 120 ints = 60 doubles
-constexpr int kGTabD = 252;
+constexpr int kGTabCart = 110;  // 120 ints = 60 doubles
+constexpr int kGTabD = 170;
 
 struct GradArgs {
   const GradItem* items;
@@ -113,7 +112,6 @@ __global__ void __launch_bounds__(256, MINB) grad_kernel(const GradArgs a, const
   if (item >= a.nitems) return;
   const int tid = threadIdx.x - g * tpq;
   double* sm = smem_all + kGTabD + (size_t)g * a.gsm;
-  const double* bn = tabs + kGTabBinom;
   const int* cart = reinterpret_cast<const int*>(tabs + kGTabCart);
   const double* prim = a.prim;
   const int tot_np = a.tot_np;
@@ -309,59 +307,75 @@ __global__ void __launch_bounds__(256, MINB) grad_kernel(const GradArgs a, const
             }
         }
         gsync(g, tpq);
-        // ---- (2b) ket 2D-level HRR (HRR2Db): V[e][c][d] = sum_l C(d,l) CD^(d-l) G[e][c+l]
-        {
-          const FDiv fnv = fdiv(nV), flc2 = fdiv(lc + 2);
-          for (int o = tid; o < nt * nrw * 3 * nV; o += tpq) {
-            const int job = fq(o, fnv), v = o - job * nV, d = job % 3;
-            const int e = v % NI, r1 = v / NI, dd = fq(r1, flc2), cc = r1 - dd * (lc + 2);
-            double* Gj = S + (size_t)job * scr;
-            double out = 0.0;
-            if (cc + dd <= NCD1) {
-              const double cdv = hdr[3 + d];
-              const double* gr = Gj + e * NJ + cc;
-              const double* bd = bn + 9 * dd;
-              double pl = 1.0;
-              for (int l = dd; l >= 0; --l) {
-                out = fma(bd[l] * pl, gr[l], out);
-                pl *= cdv;
-              }
+        // ---- (2b) ket 2D-level HRR (HRR2Db), one thread per (job, e) row in registers:
+        //      V[e][c][0] = G[e][c],  V[e][c][d+1] = V[e][c+1][d] + CD V[e][c][d]
+        for (int o = tid; o < nt * nrw * 3 * NI; o += tpq) {
+          const int job = o / NI, e = o - job * NI, d = job % 3;
+          const double* gr = S + (size_t)job * scr + e * NJ;
+          double* Vo = S + (size_t)job * scr + NI * NJ + e;
+          const double cdv = hdr[3 + d];
+          double L[NJ];
+#pragma unroll
+          for (int f = 0; f < NJ; ++f) L[f] = gr[f];
+#pragma unroll
+          for (int m = 0; m < NJ; ++m) {
+            if (m > ld) break;
+            if (m > 0) {
+#pragma unroll
+              for (int c = 0; c + m < NJ; ++c) L[c] = fma(cdv, L[c], L[c + 1]);
             }
-            Gj[NI * NJ + v] = out;
+#pragma unroll
+            for (int c = 0; c + m < NJ; ++c)
+              if (c <= lc + 1) Vo[NI * (c + (lc + 2) * m)] = L[c];
           }
         }
         gsync(g, tpq);
-        // ---- (2c) bra 2D-level HRR (HRR2Da) folded into the derivative factors (Rys2Dg):
-        //      U(a,b,c,d) = sum_k C(b,k) AB^(b-k) V[a+k][c][d];  F = U, 2a U(a+1) - a U(a-1), ...
+        // ---- (2c) bra 2D-level HRR (HRR2Da) with the derivative factors (Rys2Dg), one thread
+        //      per (job, c, d) column in registers: U(a,0) = V[a][c][d],
+        //      U(a,b+1) = U(a+1,b) + AB U(a,b);  F = U,  dA = 2alpha U(a+1,b) - a U(a-1,b),
+        //      dB = 2beta U(a,b+1) - b U(a,b-1), dC = the same transfer applied to
+        //      W[a] = 2gamma V[a][c+1][d] - c V[a][c-1][d]
         {
-          const FDiv fn1 = fdiv(n1d), fa1 = fdiv(la + 1), fb1 = fdiv(lb + 1), fc1 = fdiv(lc + 1);
-          const FDiv f3rw = fdiv(3 * nrw);
-          for (int o = tid; o < nt * nrw * 3 * n1d; o += tpq) {
-            const int job = fq(o, fn1), e1 = o - job * n1d, d = job % 3, t = fq(job, f3rw);
-            const int r1 = fq(e1, fa1), aa = e1 - r1 * (la + 1);
-            const int r2 = fq(r1, fb1), b = r1 - r2 * (lb + 1);
-            const int dd = fq(r2, fc1), cc = r2 - dd * (lc + 1);
-            const double* Vj = S + (size_t)job * scr + NI * NJ + dd * NI * (lc + 2);
+          const int ncd1 = (lc + 1) * (ld + 1);
+          const FDiv fcd = fdiv(ncd1), fc1 = fdiv(lc + 1), f3rw = fdiv(3 * nrw);
+          for (int o = tid; o < nt * nrw * 3 * ncd1; o += tpq) {
+            const int job = fq(o, fcd), r = o - job * ncd1, dd = fq(r, fc1), cc = r - dd * (lc + 1);
+            const int d = job % 3, t = fq(job, f3rw);
+            const double* V = S + (size_t)job * scr + NI * NJ + NI * ((lc + 2) * dd + cc);
             const double ab = hdr[d];
-            auto U = [&](int ua, int ub, int uc) {
-              const double* V = Vj + uc * NI + ua;
-              const double* bu = bn + 9 * ub;
-              double sum = 0.0, pk = 1.0;
-              for (int k = ub; k >= 0; --k) {
-                sum = fma(bu[k] * pk, V[k], sum);
-                pk *= ab;
+            const double* ex = cf + t * CFT + NR * 10;
+            const double e2a = ex[0], e2b = ex[1], e2c = ex[2];
+            double Lp[NI], Lc[NI], W[NI];
+#pragma unroll
+            for (int k = 0; k < NI; ++k) {
+              Lc[k] = V[k];
+              W[k] = e2c * V[NI + k] - (cc ? cc * V[k - NI] : 0.0);
+              Lp[k] = 0.0;
+            }
+            double2* Fo = reinterpret_cast<double2*>(F) + 2 * ((size_t)job * n1d + (la + 1) * (lb + 1) * (cc + (lc + 1) * dd));
+#pragma unroll
+            for (int b = 0; b < NI - 1; ++b) {
+              if (b > lb) break;
+#pragma unroll
+              for (int aa = 0; aa + b < NI - 1; ++aa) {
+                if (aa <= la) {
+                  double2 v01, v23;
+                  v01.x = Lc[aa];
+                  v01.y = e2a * Lc[aa + 1] - (aa > 0 ? aa * Lc[aa > 0 ? aa - 1 : 0] : 0.0);
+                  v23.x = e2b * fma(ab, Lc[aa], Lc[aa + 1]) - (b > 0 ? b * Lp[aa] : 0.0);
+                  v23.y = W[aa];
+                  Fo[2 * (aa + (la + 1) * b)] = v01;
+                  Fo[2 * (aa + (la + 1) * b) + 1] = v23;
+                }
               }
-              return sum;
-            };
-            const double* e = cf + t * CFT + NR * 10;
-            double2* Fo = reinterpret_cast<double2*>(F + ((size_t)job * n1d + e1) * 4);
-            double2 v01, v23;
-            v01.x = U(aa, b, cc);
-            v01.y = e[0] * U(aa + 1, b, cc) - (aa ? aa * U(aa - 1, b, cc) : 0.0);
-            v23.x = e[1] * U(aa, b + 1, cc) - (b ? b * U(aa, b - 1, cc) : 0.0);
-            v23.y = e[2] * U(aa, b, cc + 1) - (cc ? cc * U(aa, b, cc - 1) : 0.0);
-            Fo[0] = v01;
-            Fo[1] = v23;
+              // next transfer level in place: Lp <- Lc, Lc(a) <- Lc(a+1) + AB Lc(a), W likewise
+#pragma unroll
+              for (int k = 0; k + b + 1 < NI; ++k) {
+                Lp[k] = Lc[k];
+                Lc[k] = fma(ab, Lc[k], Lc[k + 1]);
+                W[k] = fma(ab, W[k], W[k + 1]);
+              }
+            }
           }
         }
         gsync(g, tpq);
