@@ -46,7 +46,7 @@ static int make_grad_tables(const Handle* h, double** d_tab) {
 static inline size_t ev2(size_t x) { return (x + 1) & ~(size_t)1; }
 
 // Per-group shared memory (doubles) of one work item with PAB x PCD tiles:
-//   hdr + Gam + Cab + Ccd + Y + max(stage-0 temp, reduction, tile (cf + Gp + F + S))
+//   hdr + Cab + Ccd + Y + max(reduction, tile (cf + Gp + F + S))
 // (the layout of grad_kernel, every region rounded to an even count)
 static size_t grad_group_smem(const DPair& P, const DPair& Q, int nijc, int nklc, int pab, int pcd, int rw) {
   const int la = P.la, lb = P.lb, lc = Q.la, ld = Q.lb;
@@ -58,34 +58,42 @@ static size_t grad_group_smem(const DPair& P, const DPair& Q, int nijc, int nklc
   const size_t scr = (size_t)NI * NJ + (size_t)NI * (lc + 2) * (ld + 1);
   const size_t nij = nijc, nc = nij * nklc;
   const bool multi = nc > 1;
-  const size_t fixed = 8 + ev2(nc * ncart4) + ev2(nij * P.np) + ev2((size_t)nklc * Q.np) +
-                       (multi ? ev2(nij * pcd * ncart4) : 0);
+  (void)nsp4;
+  const size_t fixed = 8 + ev2(nij * P.np) + ev2((size_t)nklc * Q.np) + (multi ? ev2(nij * pcd * ncart4) : 0);
   const size_t nt = (size_t)pab * pcd;
   const size_t w = std::min<size_t>(rw, NR);
-  const size_t tile = ev2(nt * ((size_t)NR * 10 + 4)) + (multi ? ev2(nt * ncart4) : 0) + nt * w * 12 * n1d +
-                      nt * 3 * w * scr;
-  return ev2(fixed + std::max({nc * std::max(ncart4, nsp4), tile, (size_t)8 * 9}));
+  const size_t tile = ev2(nt * ((size_t)NR * 10 + 4)) + ev2(nt * ncart4) + nt * w * 12 * n1d + nt * 3 * w * scr;
+  return ev2(fixed + std::max(tile, (size_t)16 * 9));
+}
+
+// Global scratch (doubles) of one work item: contracted Cartesian 2-PDM and
+// the stage-0 temporaries.
+static size_t grad_item_scratch(const DPair& P, const DPair& Q, int nijc, int nklc) {
+  const size_t ncart4 = (size_t)ncart(P.la) * ncart(P.lb) * ncart(Q.la) * ncart(Q.lb);
+  const size_t nsp4 = (size_t)ncomp(P.la) * ncomp(P.lb) * ncomp(Q.la) * ncomp(Q.lb);
+  const size_t nc = (size_t)nijc * nklc;
+  return ev2(nc * ncart4) + nc * std::max(ncart4, nsp4);
 }
 
 // Largest run-time loop extent x divisor of one work item (the kernel's
 // multiply-high division is exact below 2^32).
-static double grad_div_bound(const DPair& P, const DPair& Q, int pab, int pcd, int rw) {
+static double grad_div_bound(const DPair& P, const DPair& Q, int nij, int pab, int pcd, int rw) {
   const int la = P.la, lb = P.lb, lc = Q.la, ld = Q.lb;
   const int NI = la + lb + 2, NR = (la + lb + lc + ld + 3) / 2;
   const double ncart4 = (double)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
   const double n1d = (double)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
   const double nV = (double)NI * (lc + 2) * (ld + 1);
   const double nt = (double)pab * pcd, w = std::min(rw, NR);
-  return std::max({nt * ncart4 * ncart4, nt * w * 3 * nV * nV, nt * w * 3 * n1d * n1d, nt * NR * pab});
+  return std::max({nt * ncart4 * ncart4, (double)nij * pcd * ncart4 * ncart4, nt * w * 3 * nV * nV,
+                   nt * w * 3 * n1d * n1d, nt * NR * pab});
 }
 
 static inline int c_nab1(int key) { return key / 8; }
 static inline int c_ncd1(int key) { return key % 8; }
 
-// Shared memory per CTA (bytes, tables included) for 3, 2 and 1 resident
-// CTAs per SM: 228 KB per SM, 1 KB reserved per CTA, 227 KB per CTA at most.
-static const size_t kCtaLimit[3] = {75 * 1024, 113 * 1024, 227 * 1024};
-static const size_t kGradMaxBudget = kCtaLimit[2] / 8 - kGTabD;  // one group, doubles
+// Shared memory of the one CTA per SM (bytes, tables included): 227 KB.
+static const size_t kCtaLimit = 227 * 1024;
+static const size_t kGradMaxBudget = kCtaLimit / 8 - kGTabD;  // one group, doubles
 
 int grad_build(Handle* h, double cutint, GradPlan& plan) {
   const int ns = h->sh.size();
@@ -129,6 +137,7 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
     }
   plan.items.clear();
   plan.classes.clear();
+  size_t scratch_need = 0;
   for (int key = 0; key < 64; ++key) {
     if (byc[key].empty()) continue;
     auto& v = byc[key];
@@ -154,13 +163,15 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
     }
     GradClass c;
     c.tpq = 0;
-    // try occupancies (3, 2, 1 CTAs per SM) and thread counts per quartet; 256 threads per CTA
-    for (int occ = 0; occ < 3 && !c.tpq; ++occ) {
-      const size_t cta = kCtaLimit[occ] / 8 - kGTabD;
-      for (int tpq = wmax <= 64 ? 64 : wmax <= 512 ? 128 : 256; tpq <= 256 && !c.tpq; tpq *= 2) {
-        const int groups = 256 / tpq;
+    // one 512-thread CTA per SM (128 registers per thread; measured faster than
+    // 2 or 3 smaller CTAs whose register budgets spill); groups of tpq threads
+    {
+      const size_t cta = kCtaLimit / 8 - kGTabD;
+      const int nthr = GradThreads<1>::value;
+      for (int tpq = wmax <= 64 ? 64 : wmax <= 512 ? 128 : 256; tpq <= nthr && !c.tpq; tpq *= 2) {
+        const int groups = nthr / tpq;
         const size_t gb = (cta / groups) & ~(size_t)1;
-        int pab = std::max(1, std::min(m.npab, 8)), pcd = std::max(1, std::min(m.npcd, 4)), rw = NRc;
+        int pab = std::max(1, std::min(m.npab, 16)), pcd = std::max(1, std::min(m.npcd, 8)), rw = NRc;
         size_t need = worst(pab, pcd, rw);
         while (need > gb && (pab > 1 || pcd > 1 || rw > 1)) {
           if (pcd > 1) pcd = (pcd + 1) / 2;
@@ -175,15 +186,13 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
           c.rw = rw;
           c.pab = pab;
           c.pcd = pcd;
-          // resident CTAs per SM at this size sets the register budget of the variant
-          const size_t bytes = 8 * (kGTabD + (size_t)need * groups);
-          c.minb = bytes <= kCtaLimit[0] ? 3 : bytes <= kCtaLimit[1] ? 2 : 1;
+          c.minb = 1;
         }
       }
     }
     if (!c.tpq) { h->err = "gradient class does not fit in shared memory"; return MG_ERR_ARG; }
     for (const GradItem& it : v)
-      if (grad_div_bound(h->pairs[it.p], h->pairs[it.q], c.pab, c.pcd, c.rw) >= 4294967296.0) {
+      if (grad_div_bound(h->pairs[it.p], h->pairs[it.q], it.i1 - it.i0, c.pab, c.pcd, c.rw) >= 4294967296.0) {
         h->err = "gradient work item exceeds the kernel's index range";
         return MG_ERR_ARG;
       }
@@ -191,6 +200,21 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
     c.ncd1 = key % 8;
     c.begin = plan.items.size();
     c.count = v.size();
+    c.scr = 0;
+    for (const GradItem& it : v)
+      c.scr = std::max<long long>(c.scr, grad_item_scratch(h->pairs[it.p], h->pairs[it.q], it.i1 - it.i0, it.c1 - it.c0));
+    c.scr = (c.scr + 31) & ~31LL;  // 256-byte aligned slots
+    {  // persistent grid: the CTAs that are resident at once
+      GradFn k = grad_kernel_m1(c.nab1, c.ncd1);
+      if (!k) { h->err = "gradient class out of range"; return MG_ERR_ARG; }
+      int per_sm = 0, nsm = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, c.tpq * c.groups,
+                                                    sizeof(double) * (kGTabD + (size_t)c.gsm * c.groups));
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+      if (per_sm < 1) { h->err = "gradient kernel cannot be resident"; return MG_ERR_CUDA; }
+      c.grid = std::min<long long>((c.count + c.groups - 1) / c.groups, (long long)per_sm * nsm);
+    }
+    scratch_need = std::max<size_t>(scratch_need, (size_t)c.grid * c.groups * c.scr);
     plan.items.insert(plan.items.end(), v.begin(), v.end());
     plan.classes.push_back(c);
   }
@@ -199,6 +223,15 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
   if (!plan.items.empty()) {
     if (cudaMalloc(&plan.d_items, sizeof(GradItem) * plan.items.size()) != cudaSuccess) return MG_ERR_MEMORY;
     cudaMemcpy(plan.d_items, plan.items.data(), sizeof(GradItem) * plan.items.size(), cudaMemcpyHostToDevice);
+  }
+  cudaFree(plan.d_scratch);
+  cudaFree(plan.d_counters);
+  plan.d_scratch = nullptr;
+  plan.d_counters = nullptr;
+  if (cudaMalloc(&plan.d_scratch, sizeof(double) * std::max<size_t>(scratch_need, 32)) != cudaSuccess ||
+      cudaMalloc(&plan.d_counters, sizeof(int) * std::max<size_t>(plan.classes.size(), 1)) != cudaSuccess) {
+    h->err = "gradient scratch allocation failed";
+    return MG_ERR_MEMORY;
   }
   if (!plan.d_tab) {
     const int rc = make_grad_tables(h, &plan.d_tab);
@@ -213,15 +246,14 @@ int grad_run(Handle* h, const GradPlan& plan, const double* d_D, double* d_grad,
   for (int i = 0; i < MG_MAX_RYS; ++i) ra.m[i] = h->rys_meta[i];
   ra.tab = h->d_rys;
   cudaMemsetAsync(d_grad, 0, sizeof(double) * 3 * h->natom, st);
-  for (const GradClass& c : plan.classes) {
-    GradFn k = c.minb == 3   ? grad_kernel_m3(c.nab1, c.ncd1)
-               : c.minb == 2 ? grad_kernel_m2(c.nab1, c.ncd1)
-                             : grad_kernel_m1(c.nab1, c.ncd1);
+  cudaMemsetAsync(plan.d_counters, 0, sizeof(int) * plan.classes.size(), st);
+  for (size_t ci = 0; ci < plan.classes.size(); ++ci) {
+    const GradClass& c = plan.classes[ci];
+    GradFn k = grad_kernel_m1(c.nab1, c.ncd1);
     if (!k) { h->err = "gradient class out of range"; return MG_ERR_ARG; }
     GradArgs a{plan.d_items + c.begin, c.count, h->d_pairs, h->d_prim, h->tot_np, h->d_coef, d_D, h->nbf,
-               plan.d_tab, d_grad, c.tpq, c.gsm, c.pab, c.pcd, c.rw};
-    const int nblk = (c.count + c.groups - 1) / c.groups;
-    k<<<nblk, c.tpq * c.groups, sizeof(double) * (kGTabD + (size_t)c.gsm * c.groups), st>>>(a, ra);
+               plan.d_tab, d_grad, plan.d_scratch, c.scr, plan.d_counters + ci, c.tpq, c.gsm, c.pab, c.pcd, c.rw};
+    k<<<(unsigned)c.grid, c.tpq * c.groups, sizeof(double) * (kGTabD + (size_t)c.gsm * c.groups), st>>>(a, ra);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (cudaGetLastError() != cudaSuccess) { h->err = "gradient kernel launch failed"; return MG_ERR_CUDA; }
   }
@@ -232,6 +264,8 @@ void grad_free(GradPlan* p) {
   if (!p) return;
   cudaFree(p->d_items);
   cudaFree(p->d_tab);
+  cudaFree(p->d_scratch);
+  cudaFree(p->d_counters);
   delete p;
 }
 

@@ -1,5 +1,5 @@
-// Gradient kernel instantiations for 1 resident CTA(s) per SM (register
-// budget of __launch_bounds__(256, 1)); see grad_kernel.cuh.
+// Gradient kernel instantiations: one 512-thread CTA per SM (register
+// budget of the __launch_bounds__ of grad_kernel); see grad_kernel.cuh.
 #include "grad_kernel.cuh"
 
 namespace mg {

@@ -1,7 +1,7 @@
 // Two-electron gradient kernel (FP64), one template instantiated per
-// (la+lb+1, lc+ld+1) class and per occupancy target (minimum CTAs per SM,
-// which sets the register budget).  The algorithm and its reference anchors
-// are described in grad.cu; the instantiations live in grad_k{1,2,3}.cu.
+// (la+lb+1, lc+ld+1) class; MINB (resident CTAs per SM) sets the threads per
+// CTA and the register budget.  The algorithm and its reference anchors are
+// described in grad.cu; the instantiations live in grad_k1.cu.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -33,13 +33,14 @@ struct GradArgs {
   int nbf;
   const double* gtab;
   double* grad;
+  double* scratch;       // per-group global slots: contracted 2-PDM + stage-0 temp
+  long long scr_stride;  // doubles per slot
+  int* counter;          // work-item counter of this launch (starts at 0)
   int tpq, gsm, PAB, PCD, RW;
 };
 
 using GradFn = void (*)(GradArgs, RysArgsG);
 GradFn grad_kernel_m1(int nab1, int ncd1);
-GradFn grad_kernel_m2(int nab1, int ncd1);
-GradFn grad_kernel_m3(int nab1, int ncd1);
 
 __device__ __forceinline__ void gsync(int g, int tpq) {
   if (tpq == 32) __syncwarp();
@@ -67,39 +68,51 @@ __device__ __forceinline__ FDiv fdiv(unsigned n) {
 }
 __device__ __forceinline__ unsigned fq(unsigned o, const FDiv& f) { return __umulhi(o, f.m) + (o & f.k); }
 
-// one Rys root/weight of order N at T (table or asymptotic)
+// all N Rys roots/weights of order N at T (one table interval shared by the roots)
 template <int N>
-__device__ __forceinline__ void rys_one(const RysArgsG& ra, double T, int r, double& x, double& w) {
+__device__ __forceinline__ void rys_all(const RysArgsG& ra, double T, double* x, double* w) {
   const RysMeta& m = ra.m[N - 1];
   if (T >= m.tmax) {
-    const double ai = 1.0 / T;
-    x = m.hx[r] * ai;
-    w = m.hw[r] * sqrt(ai);
+    const double ai = 1.0 / T, si = sqrt(ai);
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      x[r] = m.hx[r] * ai;
+      w[r] = m.hw[r] * si;
+    }
   } else {
     int k = (int)(T * m.invh);
     k = k < m.K ? k : m.K - 1;
     const double s = 2.0 * (T - k * m.h) * m.invh - 1.0;
     const double* c = ra.tab + m.off + (size_t)k * (2 * N * 8);
-    const double* cx = c + r * 8;
-    const double* cw = c + (N + r) * 8;
-    double ax = __ldg(cx + 7), aw = __ldg(cw + 7);
 #pragma unroll
-    for (int j = 6; j >= 0; --j) {
-      ax = fma(ax, s, __ldg(cx + j));
-      aw = fma(aw, s, __ldg(cw + j));
+    for (int q = 0; q < 2 * N; ++q) {
+      const double* cq = c + q * 8;
+      double acc = __ldg(cq + 7);
+#pragma unroll
+      for (int j = 6; j >= 0; --j) acc = fma(acc, s, __ldg(cq + j));
+      if (q < N) x[q] = acc;
+      else w[q - N] = acc;
     }
-    x = ax;
-    w = aw;
   }
 }
 
+// Persistent kernel: each group of tpq threads takes work items from a
+// counter until none are left.  The contracted Cartesian 2-PDM of an item
+// (Gam[il][abcd]) and the stage-0 temporaries live in the group's global
+// scratch slot (L2 resident); the per-tile data in shared memory.
 // Per-group shared layout (doubles, every region starts on an even offset):
-//   hdr[8] (AB, CD) | Gam | Cab | Ccd | Y | union{ stage-0 temp | reduction |
-//   tile: cf | Gp | F | S }
+//   hdr[8] (AB, CD, item) | Cab | Ccd | Y | union{ reduction | tile: cf | Gp | F | S }
 // F holds, per (quartet, root, direction), the 2D integral and its three
 // centre derivatives interleaved: F[(job * n1d + e1) * 4 + {0: I, 1: dA, 2: dB, 3: dC}].
+// Threads per CTA of a variant: 512 when one CTA fills the SM (128 registers
+// per thread), 256 otherwise.
+template <int MINB>
+struct GradThreads {
+  static constexpr int value = MINB == 1 ? 512 : 256;
+};
+
 template <int NAB1, int NCD1, int MINB>
-__global__ void __launch_bounds__(256, MINB) grad_kernel(const GradArgs a, const RysArgsG ra) {
+__global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(const GradArgs a, const RysArgsG ra) {
   constexpr int NR = (NAB1 + NCD1 + 1) / 2;
   constexpr int NI = NAB1 + 1, NJ = NCD1 + 1;
   extern __shared__ __align__(16) double smem_all[];
@@ -108,10 +121,15 @@ __global__ void __launch_bounds__(256, MINB) grad_kernel(const GradArgs a, const
   __syncthreads();
   const int tpq = a.tpq;
   const int g = threadIdx.x / tpq;
-  const int item = blockIdx.x * (blockDim.x / tpq) + g;
-  if (item >= a.nitems) return;
   const int tid = threadIdx.x - g * tpq;
   double* sm = smem_all + kGTabD + (size_t)g * a.gsm;
+  double* Gg = a.scratch + (size_t)(blockIdx.x * (blockDim.x / tpq) + g) * a.scr_stride;
+  int* slot = reinterpret_cast<int*>(sm + 6);
+  for (;;) {
+  if (tid == 0) *slot = atomicAdd(a.counter, 1);
+  gsync(g, tpq);
+  const int item = *slot;
+  if (item >= a.nitems) break;
   const int* cart = reinterpret_cast<const int*>(tabs + kGTabCart);
   const double* prim = a.prim;
   const int tot_np = a.tot_np;
@@ -134,16 +152,16 @@ __global__ void __launch_bounds__(256, MINB) grad_kernel(const GradArgs a, const
   const int NT = PAB * PCD;
   const int CFT = NR * 10 + 4;  // per-quartet coefficient record
   double* hdr = sm;
-  double* Gam = hdr + 8;                              // nc * ncart4, index il + nc * abcd
-  double* Cab = Gam + ev2(nc * ncart4);               // nij * npab
+  double* Cab = hdr + 8;                              // nij * npab
   double* Ccd = Cab + ev2(nij * npab);                // nklc * npcd
-  double* Y = Ccd + ev2(nklc * npcd);                 // nij * PCD * ncart4 (multi only)
+  double* Y = Ccd + ev2(nklc * npcd);                 // [ij][pc][abcd] (multi only)
   double* U0 = Y + (multi ? ev2(nij * PCD * ncart4) : 0);
-  double* Tmp = U0;                                   // stage-0 temp (nc * ncart4)
   double* cf = U0;                                    // NT * CFT
-  double* Gp = cf + ev2(NT * CFT);                    // NT * ncart4 (multi only)
-  double* F = Gp + (multi ? ev2(NT * ncart4) : 0);    // NT * RW * 3 * 4 * n1d
+  double* Gp = cf + ev2(NT * CFT);                    // [t][abcd] primitive 2-PDM
+  double* F = Gp + ev2(NT * ncart4);                  // NT * RW * 3 * 4 * n1d
   double* S = F + NT * RW * 12 * n1d;                 // NT * 3 * RW * scr
+  double* Gam = Gg;                                   // [il][abcd] (global scratch)
+  double* Tmp = Gg + ev2(nc * ncart4);                // stage-0 temp (global scratch)
   if (tid < 3) {
     hdr[tid] = P.A[tid] - P.B[tid];
     hdr[3 + tid] = Q.A[tid] - Q.B[tid];
@@ -210,7 +228,10 @@ __global__ void __launch_bounds__(256, MINB) grad_kernel(const GradArgs a, const
         Tmp[o] = s;
       }
       gsync(g, tpq);
-      for (int o = tid; o < nc * ncart4; o += tpq) Gam[o] = Tmp[o];
+      for (int o = tid; o < nc * ncart4; o += tpq) {  // transpose to [il][abcd]
+        const int il = o / ncart4, abcd = o - il * ncart4;
+        Gam[o] = Tmp[il + nc * abcd];
+      }
       gsync(g, tpq);
     }
   }
@@ -227,11 +248,14 @@ __global__ void __launch_bounds__(256, MINB) grad_kernel(const GradArgs a, const
     gsync(g, tpq);
     // ---- ket half-transform of the 2-PDM: Y[ij][pc][abcd] = sum_kl Ccd[kl][pc] Gam[ij,kl][abcd]
     if (multi) {
+      const FDiv f4 = fdiv(ncart4), fpc = fdiv(npc);
       for (int o = tid; o < nij * npc * ncart4; o += tpq) {
-        const int ij = o % nij, r1 = o / nij, pc = r1 % npc, abcd = r1 / npc;
+        const int r1 = fq(o, f4), abcd = o - r1 * ncart4, ij = fq(r1, fpc), pc = r1 - ij * npc;
+        const double* gm = Gam + (size_t)ij * ncart4 + abcd;
         double s = 0.0;
-        for (int klc = 0; klc < nklc; ++klc) s = fma(Ccd[klc * npcd + pcd0 + pc], Gam[ij + nij * klc + nc * abcd], s);
-        Y[ij + nij * (pc + PCD * abcd)] = s;
+        for (int klc = 0; klc < nklc; ++klc)
+          s = fma(Ccd[klc * npcd + pcd0 + pc], gm[(size_t)nij * klc * ncart4], s);
+        Y[abcd + ncart4 * (pc + PCD * ij)] = s;
       }
     }
     for (int pab0 = 0; pab0 < npab; pab0 += PAB) {
@@ -239,50 +263,60 @@ __global__ void __launch_bounds__(256, MINB) grad_kernel(const GradArgs a, const
       const int nt = npa * npc;
       const FDiv fnpa = fdiv(npa);
       gsync(g, tpq);
-      // ---- (1) roots: one (quartet, root) per thread
-      for (int job = tid; job < nt * NR; job += tpq) {
-        const int r = job % NR, t = job / NR;
+      // ---- (1) roots: one primitive quartet per thread, all NR roots
+      for (int t = tid; t < nt; t += tpq) {
         const int pc = fq(t, fnpa), pa = t - pc * npa;
         const int ia = P.prim_off + pab0 + pa, ic = Q.prim_off + pcd0 + pc;
         const double zeta = prim[ia], eta = prim[ic];
         const double px = prim[2 * tot_np + ia], py = prim[3 * tot_np + ia], pz = prim[4 * tot_np + ia];
         const double qx = prim[2 * tot_np + ic], qy = prim[3 * tot_np + ic], qz = prim[4 * tot_np + ic];
         const double ze = zeta + eta, zei = 1.0 / ze, rho = zeta * eta * zei;
+        const double hz = 0.5 / zeta, he = 0.5 / eta;
         const double dx = px - qx, dy = py - qy, dz = pz - qz;
         const double T = rho * (dx * dx + dy * dy + dz * dz);
         const double fact = prim[tot_np + ia] * prim[tot_np + ic] * sqrt(zei);
-        double x, w;
-        rys_one<NR>(ra, T, r, x, w);
-        const double U2 = x * zei;
-        double* c = cf + t * CFT + r * 10;
-        c[0] = 0.5 * U2;
-        c[1] = 0.5 * (1.0 - U2 * eta) / zeta;
-        c[2] = 0.5 * (1.0 - U2 * zeta) / eta;
-        c[3] = px - P.A[0] - eta * U2 * dx;
-        c[4] = py - P.A[1] - eta * U2 * dy;
-        c[5] = pz - P.A[2] - eta * U2 * dz;
-        c[6] = qx - Q.A[0] + zeta * U2 * dx;
-        c[7] = qy - Q.A[1] + zeta * U2 * dy;
-        c[8] = qz - Q.A[2] + zeta * U2 * dz;
-        c[9] = w * fact;
-        if (r == 0) {
-          double* e = cf + t * CFT + NR * 10;
-          e[0] = 2.0 * prim[5 * tot_np + ia];         // 2 alpha
-          e[1] = 2.0 * prim[6 * tot_np + ia];         // 2 beta
-          e[2] = 2.0 * prim[5 * tot_np + ic];         // 2 gamma
-          e[3] = Cab[pab0 + pa] * Ccd[pcd0 + pc];     // single-contraction coefficient
+        const double pax = px - P.A[0], pay = py - P.A[1], paz = pz - P.A[2];
+        const double qcx = qx - Q.A[0], qcy = qy - Q.A[1], qcz = qz - Q.A[2];
+        double x[NR], w[NR];
+        rys_all<NR>(ra, T, x, w);
+        double* cr = cf + t * CFT;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          const double U2 = x[r] * zei;
+          double* c = cr + r * 10;
+          c[0] = 0.5 * U2;
+          c[1] = hz - hz * U2 * eta;
+          c[2] = he - he * U2 * zeta;
+          c[3] = pax - eta * U2 * dx;
+          c[4] = pay - eta * U2 * dy;
+          c[5] = paz - eta * U2 * dz;
+          c[6] = qcx + zeta * U2 * dx;
+          c[7] = qcy + zeta * U2 * dy;
+          c[8] = qcz + zeta * U2 * dz;
+          c[9] = w[r] * fact;
         }
+        double* e = cr + NR * 10;
+        e[0] = 2.0 * prim[5 * tot_np + ia];         // 2 alpha
+        e[1] = 2.0 * prim[6 * tot_np + ia];         // 2 beta
+        e[2] = 2.0 * prim[5 * tot_np + ic];         // 2 gamma
+        e[3] = Cab[pab0 + pa] * Ccd[pcd0 + pc];     // single-contraction coefficient
       }
-      // ---- (3) primitive 2-PDM (Tcrtnc) by the bra half-transform
-      if (multi) {
+      gsync(g, tpq);
+      // ---- (3) primitive 2-PDM (Tcrtnc): bra half-transform of Y, or the single
+      //      contraction coefficient times the contracted 2-PDM
+      {
         const FDiv f4 = fdiv(ncart4);
         for (int o = tid; o < nt * ncart4; o += tpq) {
           const int t = fq(o, f4), abcd = o - t * ncart4;
-          const int pc = fq(t, fnpa), pa = t - pc * npa;
-          const double* y = Y + nij * (pc + PCD * abcd);
           double s = 0.0;
-          for (int ij = 0; ij < nij; ++ij) s = fma(Cab[ij * npab + pab0 + pa], y[ij], s);
-          Gp[t * ncart4 + abcd] = s;
+          if (multi) {
+            const int pc = fq(t, fnpa), pa = t - pc * npa;
+            const double* y = Y + abcd + ncart4 * pc;
+            for (int ij = 0; ij < nij; ++ij) s = fma(Cab[ij * npab + pab0 + pa], y[(size_t)ncart4 * PCD * ij], s);
+          } else {
+            s = cf[t * CFT + NR * 10 + 3] * Gam[abcd];
+          }
+          Gp[o] = s;
         }
       }
       gsync(g, tpq);
@@ -398,7 +432,7 @@ __global__ void __launch_bounds__(256, MINB) grad_kernel(const GradArgs a, const
                                         (lb + 1) * (((ec >> sh) & 255) + (lc + 1) * ((ed >> sh) & 255))));
             }
             for (int t = tslot; t < nt; t += TT) {
-              const double gm = multi ? Gp[t * ncart4 + abcd] : cf[t * CFT + NR * 10 + 3] * Gam[abcd];
+              const double gm = Gp[t * ncart4 + abcd];
               if (gm == 0.0) continue;
               const double* Fb = F + (size_t)t * nrw * 3 * n1d4;
               for (int rl = 0; rl < nrw; ++rl, Fb += 3 * n1d4) {
@@ -428,7 +462,7 @@ __global__ void __launch_bounds__(256, MINB) grad_kernel(const GradArgs a, const
   }
   gsync(g, tpq);
   // ---- reduce over the group, distribute to atoms (Distg1)
-  double* red = U0;  // tpq/32 * 9 doubles
+  double* red = U0;  // tpq/32 * 9 doubles (<= 144)
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
     double v = acc[k];
@@ -445,6 +479,8 @@ __global__ void __launch_bounds__(256, MINB) grad_kernel(const GradArgs a, const
     atomicAdd(&a.grad[3 * atom + d], v);
     atomicAdd(&a.grad[3 * Q.atom_b + d], -v);  // translational invariance
   }
+  gsync(g, tpq);
+  }  // work items
 }
 
 template <int MINB, int A, int B>

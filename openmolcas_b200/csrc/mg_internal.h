@@ -109,13 +109,17 @@ struct GradItem {
 };
 struct GradClass {
   int nab1, ncd1, begin, count, tpq, gsm, groups, rw, pab, pcd;
-  int minb;  // resident CTAs per SM the kernel variant is compiled for (1..3)
+  int minb;       // resident CTAs per SM the kernel variant is compiled for (1..3)
+  long long scr;  // global scratch per group (doubles)
+  long long grid; // persistent CTAs
 };
 struct GradPlan {
   std::vector<GradItem> items;
   std::vector<GradClass> classes;
   GradItem* d_items = nullptr;
-  double* d_tab = nullptr;  // per-CTA tables of the gradient kernel
+  double* d_tab = nullptr;       // per-CTA tables of the gradient kernel
+  double* d_scratch = nullptr;   // per-group 2-PDM slots
+  int* d_counters = nullptr;     // one work counter per class
   double cutint = -1;
 };
 int grad_build(Handle* h, double cutint, GradPlan& plan);

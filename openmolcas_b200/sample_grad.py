@@ -3,6 +3,7 @@ profiling driver).
 
     python -m openmolcas_b200.sample_grad c4 [repeats]
     python -m openmolcas_b200.sample_grad small [repeats]     # 4 atoms of 4s3p2d
+    python -m openmolcas_b200.sample_grad medium [repeats]    # 8 atoms of 4s3p2d
 """
 import sys
 
@@ -18,6 +19,9 @@ def main(argv):
     if cfg == "small":
         m = B.make_molecule("small4s3p2d", 4, [("4s3p2d", 4)], 4)
         rank = 10
+    elif cfg == "medium":
+        m = B.make_molecule("medium4s3p2d", 8, [("4s3p2d", 8)], 4)
+        rank = 20
     else:
         m = B.config_molecule(cfg)
         rank = B.CONFIGS[cfg]["rank"] or 40
