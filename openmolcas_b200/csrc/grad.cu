@@ -46,7 +46,7 @@ static int make_grad_tables(const Handle* h, double** d_tab) {
 static inline size_t ev2(size_t x) { return (x + 1) & ~(size_t)1; }
 
 // Per-group shared memory (doubles) of one work item with PAB x PCD tiles:
-//   hdr + Cab + Ccd + Y + max(reduction, tile (cf + Gp + F + S))
+//   hdr + Cab + Ccd + Y + IX + max(reduction, tile (cf + Gp + F + S))
 // (the layout of grad_kernel, every region rounded to an even count)
 static size_t grad_group_smem(const DPair& P, const DPair& Q, int nijc, int nklc, int pab, int pcd, int rw) {
   const int la = P.la, lb = P.lb, lc = Q.la, ld = Q.lb;
@@ -59,10 +59,12 @@ static size_t grad_group_smem(const DPair& P, const DPair& Q, int nijc, int nklc
   const size_t nij = nijc, nc = nij * nklc;
   const bool multi = nc > 1;
   (void)nsp4;
-  const size_t fixed = 8 + ev2(nij * P.np) + ev2((size_t)nklc * Q.np) + (multi ? ev2(nij * pcd * ncart4) : 0);
+  const size_t fixed = 8 + ev2(nij * P.np) + ev2((size_t)nklc * Q.np) + (multi ? ev2(nij * pcd * ncart4) : 0) +
+                       ev2((ncart4 + 1) / 2);
   const size_t nt = (size_t)pab * pcd;
   const size_t w = std::min<size_t>(rw, NR);
-  const size_t tile = ev2(nt * ((size_t)NR * 10 + 4)) + ev2(nt * ncart4) + nt * w * 12 * n1d + nt * 3 * w * scr;
+  const size_t gs = ncart4 | 1, st = w * 12 * n1d + 2;  // padded strides of Gp and F
+  const size_t tile = ev2(nt * ((size_t)NR * 10 + 4)) + ev2(nt * gs) + nt * st + nt * 3 * w * scr;
   return ev2(fixed + std::max(tile, (size_t)16 * 9));
 }
 

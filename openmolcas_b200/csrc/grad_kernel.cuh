@@ -155,11 +155,15 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
   double* Cab = hdr + 8;                              // nij * npab
   double* Ccd = Cab + ev2(nij * npab);                // nklc * npcd
   double* Y = Ccd + ev2(nklc * npcd);                 // [ij][pc][abcd] (multi only)
-  double* U0 = Y + (multi ? ev2(nij * PCD * ncart4) : 0);
+  int* IX = reinterpret_cast<int*>(Y + (multi ? ev2(nij * PCD * ncart4) : 0));  // [abcd] packed 2D indices
+  double* U0 = reinterpret_cast<double*>(IX) + ev2((ncart4 + 1) / 2);
+  // padded strides: consecutive primitive quartets fall in different bank groups
+  const int Gs = ncart4 | 1;                          // Gp row (odd)
+  const int St = RW * 12 * n1d + 2;                   // F block of one quartet (= 2 mod 4)
   double* cf = U0;                                    // NT * CFT
-  double* Gp = cf + ev2(NT * CFT);                    // [t][abcd] primitive 2-PDM
-  double* F = Gp + ev2(NT * ncart4);                  // NT * RW * 3 * 4 * n1d
-  double* S = F + NT * RW * 12 * n1d;                 // NT * 3 * RW * scr
+  double* Gp = cf + ev2(NT * CFT);                    // [t][abcd] primitive 2-PDM, row stride Gs
+  double* F = Gp + ev2(NT * Gs);                      // [t][rl][dir][e1][4], quartet stride St
+  double* S = F + NT * St;                            // NT * 3 * RW * scr
   double* Gam = Gg;                                   // [il][abcd] (global scratch)
   double* Tmp = Gg + ev2(nc * ncart4);                // stage-0 temp (global scratch)
   if (tid < 3) {
@@ -239,10 +243,25 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
 #pragma unroll
   for (int k = 0; k < 9; ++k) acc[k] = 0.0;
   const int ca0 = d_ccum(la), cb0 = d_ccum(lb), cc0 = d_ccum(lc), cd0 = d_ccum(ld);
-  // Assg1 thread map: TA threads over Cartesian quartets x TT threads over primitive quartets
-  const int TA = ncart4 < tpq ? ncart4 : tpq;
-  const int TT = tpq / TA;
-  const int aslot = tid % TA, tslot = tid / TA;
+  // packed 2D-integral offsets of every Cartesian quartet: x | y << 8 | z << 16
+  {
+    const FDiv fca = fdiv(nca), fcb = fdiv(ncb), fcc = fdiv(ncc);
+    for (int abcd = tid; abcd < ncart4; abcd += tpq) {
+      const int r1 = fq(abcd, fca), ca = abcd - r1 * nca;
+      const int r2 = fq(r1, fcb), cb = r1 - r2 * ncb;
+      const int cd = fq(r2, fcc), cc = r2 - cd * ncc;
+      const int ea = cart[ca0 + ca], eb = cart[cb0 + cb], ec = cart[cc0 + cc], ed = cart[cd0 + cd];
+      int pk = 0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const int sh = 8 * d;
+        pk |= (((ea >> sh) & 255) +
+               (la + 1) * (((eb >> sh) & 255) + (lb + 1) * (((ec >> sh) & 255) + (lc + 1) * ((ed >> sh) & 255))))
+              << sh;
+      }
+      IX[abcd] = pk;
+    }
+  }
   for (int pcd0 = 0; pcd0 < npcd; pcd0 += PCD) {
     const int npc = min(PCD, npcd - pcd0);
     gsync(g, tpq);
@@ -316,7 +335,7 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
           } else {
             s = cf[t * CFT + NR * 10 + 3] * Gam[abcd];
           }
-          Gp[o] = s;
+          Gp[t * Gs + abcd] = s;
         }
       }
       gsync(g, tpq);
@@ -386,7 +405,8 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
               W[k] = e2c * V[NI + k] - (cc ? cc * V[k - NI] : 0.0);
               Lp[k] = 0.0;
             }
-            double2* Fo = reinterpret_cast<double2*>(F) + 2 * ((size_t)job * n1d + (la + 1) * (lb + 1) * (cc + (lc + 1) * dd));
+            double2* Fo = reinterpret_cast<double2*>(F + (size_t)t * St) +
+                          2 * ((size_t)(job - 3 * nrw * t) * n1d + (la + 1) * (lb + 1) * (cc + (lc + 1) * dd));
 #pragma unroll
             for (int b = 0; b < NI - 1; ++b) {
               if (b > lb) break;
@@ -413,46 +433,35 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
           }
         }
         gsync(g, tpq);
-        // ---- (4) Assg1: sum over Cartesian components and roots; each thread
-        //      decomposes its Cartesian quartets once and walks the primitive quartets
-        if (tslot < TT) {
-          const FDiv fca = fdiv(nca), fcb = fdiv(ncb), fcc = fdiv(ncc);
+        // ---- (4) Assg1: sum over Cartesian components and roots; consecutive threads
+        //      take consecutive primitive quartets of one Cartesian quartet
+        {
+          const FDiv fnt = fdiv(nt);
           const int n1d4 = 4 * n1d;
-          for (int abcd = aslot; abcd < ncart4; abcd += TA) {
-            const int r1 = fq(abcd, fca), ca = abcd - r1 * nca;
-            const int r2 = fq(r1, fcb), cb = r1 - r2 * ncb;
-            const int cd = fq(r2, fcc), cc = r2 - cd * ncc;
-            const int ea = cart[ca0 + ca], eb = cart[cb0 + cb], ec = cart[cc0 + cc], ed = cart[cd0 + cd];
-            int idx[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              const int sh = 8 * d;
-              idx[d] = 4 * (((ea >> sh) & 255) +
-                            (la + 1) * (((eb >> sh) & 255) +
-                                        (lb + 1) * (((ec >> sh) & 255) + (lc + 1) * ((ed >> sh) & 255))));
-            }
-            for (int t = tslot; t < nt; t += TT) {
-              const double gm = Gp[t * ncart4 + abcd];
-              if (gm == 0.0) continue;
-              const double* Fb = F + (size_t)t * nrw * 3 * n1d4;
-              for (int rl = 0; rl < nrw; ++rl, Fb += 3 * n1d4) {
-                const double2 x01 = *reinterpret_cast<const double2*>(Fb + idx[0]);
-                const double2 x23 = *reinterpret_cast<const double2*>(Fb + idx[0] + 2);
-                const double2 y01 = *reinterpret_cast<const double2*>(Fb + n1d4 + idx[1]);
-                const double2 y23 = *reinterpret_cast<const double2*>(Fb + n1d4 + idx[1] + 2);
-                const double2 z01 = *reinterpret_cast<const double2*>(Fb + 2 * n1d4 + idx[2]);
-                const double2 z23 = *reinterpret_cast<const double2*>(Fb + 2 * n1d4 + idx[2] + 2);
-                const double gyz = gm * y01.x * z01.x, gxz = gm * x01.x * z01.x, gxy = gm * x01.x * y01.x;
-                acc[0] = fma(gyz, x01.y, acc[0]);
-                acc[1] = fma(gxz, y01.y, acc[1]);
-                acc[2] = fma(gxy, z01.y, acc[2]);
-                acc[3] = fma(gyz, x23.x, acc[3]);
-                acc[4] = fma(gxz, y23.x, acc[4]);
-                acc[5] = fma(gxy, z23.x, acc[5]);
-                acc[6] = fma(gyz, x23.y, acc[6]);
-                acc[7] = fma(gxz, y23.y, acc[7]);
-                acc[8] = fma(gxy, z23.y, acc[8]);
-              }
+          for (int w = tid; w < nt * ncart4; w += tpq) {
+            const int abcd = fq(w, fnt), t = w - abcd * nt;
+            const double gm = Gp[t * Gs + abcd];
+            if (gm == 0.0) continue;
+            const int pk = IX[abcd];
+            const int i0 = 4 * (pk & 255), i1 = n1d4 + 4 * ((pk >> 8) & 255), i2 = 2 * n1d4 + 4 * (pk >> 16);
+            const double* Fb = F + (size_t)t * St;
+            for (int rl = 0; rl < nrw; ++rl, Fb += 3 * n1d4) {
+              const double2 x01 = *reinterpret_cast<const double2*>(Fb + i0);
+              const double2 x23 = *reinterpret_cast<const double2*>(Fb + i0 + 2);
+              const double2 y01 = *reinterpret_cast<const double2*>(Fb + i1);
+              const double2 y23 = *reinterpret_cast<const double2*>(Fb + i1 + 2);
+              const double2 z01 = *reinterpret_cast<const double2*>(Fb + i2);
+              const double2 z23 = *reinterpret_cast<const double2*>(Fb + i2 + 2);
+              const double gyz = gm * y01.x * z01.x, gxz = gm * x01.x * z01.x, gxy = gm * x01.x * y01.x;
+              acc[0] = fma(gyz, x01.y, acc[0]);
+              acc[1] = fma(gxz, y01.y, acc[1]);
+              acc[2] = fma(gxy, z01.y, acc[2]);
+              acc[3] = fma(gyz, x23.x, acc[3]);
+              acc[4] = fma(gxz, y23.x, acc[4]);
+              acc[5] = fma(gxy, z23.x, acc[5]);
+              acc[6] = fma(gyz, x23.y, acc[6]);
+              acc[7] = fma(gxz, y23.y, acc[7]);
+              acc[8] = fma(gxy, z23.y, acc[8]);
             }
           }
         }
