@@ -55,7 +55,7 @@ static size_t grad_group_smem(const DPair& P, const DPair& Q, int nijc, int nklc
   const size_t ncart4 = (size_t)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
   const size_t nsp4 = (size_t)ncomp(la) * ncomp(lb) * ncomp(lc) * ncomp(ld);
   const size_t n1d = (size_t)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-  const size_t scr = (size_t)NI * NJ + (size_t)NI * (lc + 2) * (ld + 1);
+  const size_t scr = ((size_t)NI * NJ + (size_t)(NI | 1) * (lc + 2) * (ld + 1)) | 1;
   const size_t nij = nijc, nc = nij * nklc;
   const bool multi = nc > 1;
   (void)nsp4;
@@ -64,7 +64,7 @@ static size_t grad_group_smem(const DPair& P, const DPair& Q, int nijc, int nklc
   const size_t nt = (size_t)pab * pcd;
   const size_t w = std::min<size_t>(rw, NR);
   const size_t gs = ncart4 | 1, st = w * 12 * n1d + 2;  // padded strides of Gp and F
-  const size_t tile = ev2(nt * ((size_t)NR * 10 + 4)) + ev2(nt * gs) + nt * st + nt * 3 * w * scr;
+  const size_t tile = ev2(nt * ((size_t)NR * 10 + 5)) + ev2(nt * gs) + nt * st + nt * 3 * w * scr;
   return ev2(fixed + std::max(tile, (size_t)16 * 9));
 }
 

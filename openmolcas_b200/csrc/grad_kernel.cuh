@@ -146,11 +146,13 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
   const bool multi = nc > 1;
   const int npab = P.np, npcd = Q.np;
   const int n1d = (la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-  const int nV = NI * (lc + 2) * (ld + 1);  // ket-transferred 2D integrals per job
-  const int scr = NI * NJ + nV;             // G + V per job
+  // per (quartet, root, direction) job: G[f][e] (e fastest) and V[d][c][e] with row
+  // stride NIp; odd strides keep the lanes of a warp on distinct banks
+  constexpr int NIp = NI | 1;
+  const int scr = (NI * NJ + NIp * (lc + 2) * (ld + 1)) | 1;
   const int PAB = a.PAB, PCD = a.PCD, RW = a.RW;
   const int NT = PAB * PCD;
-  const int CFT = NR * 10 + 4;  // per-quartet coefficient record
+  const int CFT = NR * 10 + 5;  // per-quartet coefficient record (odd stride)
   double* hdr = sm;
   double* Cab = hdr + 8;                              // nij * npab
   double* Ccd = Cab + ev2(nij * npab);                // nklc * npcd
@@ -342,34 +344,51 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
       for (int r0 = 0; r0 < NR; r0 += RW) {
         const int nrw = min(RW, NR - r0);
         const FDiv fnrw = fdiv(nrw);
-        // ---- (2a) 2D recursion per (quartet, root, direction): G[e][f], e at A, f at C
+        // ---- (2a) 2D recursion per (quartet, root, direction), column by column in
+        //      registers: G[f][e], e at A, f at C
         for (int job = tid; job < nt * nrw * 3; job += tpq) {
           const int d = job % 3, tr = job / 3, t = fq(tr, fnrw), rl = tr - t * nrw, r = r0 + rl;
           const double* c = cf + t * CFT + r * 10;
           const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
           double* G = S + (size_t)job * scr;
-          G[0] = d == 2 ? c[9] : 1.0;
-          if (NI > 1) G[NJ] = C00 * G[0];
-          for (int i = 1; i < NI - 1; ++i) G[(i + 1) * NJ] = C00 * G[i * NJ] + i * B10 * G[(i - 1) * NJ];
-          for (int j = 0; j < NJ - 1; ++j)
+          double Cm[NI], Cc[NI], Cn[NI];
+          Cc[0] = d == 2 ? c[9] : 1.0;
+          if (NI > 1) Cc[1] = C00 * Cc[0];
+#pragma unroll
+          for (int i = 1; i < NI - 1; ++i) Cc[i + 1] = C00 * Cc[i] + i * B10 * Cc[i - 1];
+#pragma unroll
+          for (int i = 0; i < NI; ++i) {
+            G[i] = Cc[i];
+            Cm[i] = 0.0;
+          }
+#pragma unroll
+          for (int j = 0; j < NJ - 1; ++j) {
+#pragma unroll
             for (int i = 0; i < NI; ++i) {
-              double v = D00 * G[i * NJ + j];
-              if (j > 0) v += j * B01 * G[i * NJ + j - 1];
-              if (i > 0) v += i * B00 * G[(i - 1) * NJ + j];
-              G[i * NJ + j + 1] = v;
+              double v = D00 * Cc[i];
+              if (j > 0) v = fma(j * B01, Cm[i], v);
+              if (i > 0) v = fma(i * B00, Cc[i > 0 ? i - 1 : 0], v);
+              Cn[i] = v;
+              G[(j + 1) * NI + i] = v;
             }
+#pragma unroll
+            for (int i = 0; i < NI; ++i) {
+              Cm[i] = Cc[i];
+              Cc[i] = Cn[i];
+            }
+          }
         }
         gsync(g, tpq);
         // ---- (2b) ket 2D-level HRR (HRR2Db), one thread per (job, e) row in registers:
         //      V[e][c][0] = G[e][c],  V[e][c][d+1] = V[e][c+1][d] + CD V[e][c][d]
         for (int o = tid; o < nt * nrw * 3 * NI; o += tpq) {
           const int job = o / NI, e = o - job * NI, d = job % 3;
-          const double* gr = S + (size_t)job * scr + e * NJ;
+          const double* gr = S + (size_t)job * scr + e;
           double* Vo = S + (size_t)job * scr + NI * NJ + e;
           const double cdv = hdr[3 + d];
           double L[NJ];
 #pragma unroll
-          for (int f = 0; f < NJ; ++f) L[f] = gr[f];
+          for (int f = 0; f < NJ; ++f) L[f] = gr[f * NI];
 #pragma unroll
           for (int m = 0; m < NJ; ++m) {
             if (m > ld) break;
@@ -379,7 +398,7 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
             }
 #pragma unroll
             for (int c = 0; c + m < NJ; ++c)
-              if (c <= lc + 1) Vo[NI * (c + (lc + 2) * m)] = L[c];
+              if (c <= lc + 1) Vo[NIp * (c + (lc + 2) * m)] = L[c];
           }
         }
         gsync(g, tpq);
@@ -394,7 +413,7 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
           for (int o = tid; o < nt * nrw * 3 * ncd1; o += tpq) {
             const int job = fq(o, fcd), r = o - job * ncd1, dd = fq(r, fc1), cc = r - dd * (lc + 1);
             const int d = job % 3, t = fq(job, f3rw);
-            const double* V = S + (size_t)job * scr + NI * NJ + NI * ((lc + 2) * dd + cc);
+            const double* V = S + (size_t)job * scr + NI * NJ + NIp * ((lc + 2) * dd + cc);
             const double ab = hdr[d];
             const double* ex = cf + t * CFT + NR * 10;
             const double e2a = ex[0], e2b = ex[1], e2c = ex[2];
@@ -402,7 +421,7 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
 #pragma unroll
             for (int k = 0; k < NI; ++k) {
               Lc[k] = V[k];
-              W[k] = e2c * V[NI + k] - (cc ? cc * V[k - NI] : 0.0);
+              W[k] = e2c * V[NIp + k] - (cc ? cc * V[k - NIp] : 0.0);
               Lp[k] = 0.0;
             }
             double2* Fo = reinterpret_cast<double2*>(F + (size_t)t * St) +
