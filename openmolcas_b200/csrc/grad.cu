@@ -55,7 +55,7 @@ static size_t grad_group_smem(const DPair& P, const DPair& Q, int nijc, int nklc
   const size_t ncart4 = (size_t)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
   const size_t nsp4 = (size_t)ncomp(la) * ncomp(lb) * ncomp(lc) * ncomp(ld);
   const size_t n1d = (size_t)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-  const size_t scr = ((size_t)NI * NJ + (size_t)(NI | 1) * (lc + 2) * (ld + 1)) | 1;
+  const size_t scr = ((size_t)(NI | 1) * (lc + 2) * (ld + 1)) | 1;
   const size_t nij = nijc, nc = nij * nklc;
   const bool multi = nc > 1;
   (void)nsp4;

@@ -68,6 +68,32 @@ __device__ __forceinline__ FDiv fdiv(unsigned n) {
 }
 __device__ __forceinline__ unsigned fq(unsigned o, const FDiv& f) { return __umulhi(o, f.m) + (o & f.k); }
 
+// one Rys root/weight of order N at T (table or asymptotic)
+template <int N>
+__device__ __forceinline__ void rys_one(const RysArgsG& ra, double T, int r, double& x, double& w) {
+  const RysMeta& m = ra.m[N - 1];
+  if (T >= m.tmax) {
+    const double ai = 1.0 / T;
+    x = m.hx[r] * ai;
+    w = m.hw[r] * sqrt(ai);
+  } else {
+    int k = (int)(T * m.invh);
+    k = k < m.K ? k : m.K - 1;
+    const double s = 2.0 * (T - k * m.h) * m.invh - 1.0;
+    const double* c = ra.tab + m.off + (size_t)k * (2 * N * 8);
+    const double* cx = c + r * 8;
+    const double* cw = c + (N + r) * 8;
+    double ax = __ldg(cx + 7), aw = __ldg(cw + 7);
+#pragma unroll
+    for (int j = 6; j >= 0; --j) {
+      ax = fma(ax, s, __ldg(cx + j));
+      aw = fma(aw, s, __ldg(cw + j));
+    }
+    x = ax;
+    w = aw;
+  }
+}
+
 // all N Rys roots/weights of order N at T (one table interval shared by the roots)
 template <int N>
 __device__ __forceinline__ void rys_all(const RysArgsG& ra, double T, double* x, double* w) {
@@ -146,10 +172,10 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
   const bool multi = nc > 1;
   const int npab = P.np, npcd = Q.np;
   const int n1d = (la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-  // per (quartet, root, direction) job: G[f][e] (e fastest) and V[d][c][e] with row
-  // stride NIp; odd strides keep the lanes of a warp on distinct banks
+  // per (quartet, root, direction) job: V[d][c][e] with row stride NIp; odd strides
+  // keep the lanes of a warp on distinct banks
   constexpr int NIp = NI | 1;
-  const int scr = (NI * NJ + NIp * (lc + 2) * (ld + 1)) | 1;
+  const int scr = (NIp * (lc + 2) * (ld + 1)) | 1;
   const int PAB = a.PAB, PCD = a.PCD, RW = a.RW;
   const int NT = PAB * PCD;
   const int CFT = NR * 10 + 5;  // per-quartet coefficient record (odd stride)
@@ -284,43 +310,39 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
       const int nt = npa * npc;
       const FDiv fnpa = fdiv(npa);
       gsync(g, tpq);
-      // ---- (1) roots: one primitive quartet per thread, all NR roots
-      for (int t = tid; t < nt; t += tpq) {
+      // ---- (1) roots: one (primitive quartet, root) per thread
+      for (int job = tid; job < nt * NR; job += tpq) {
+        const int t = job / NR, r = job - t * NR;
         const int pc = fq(t, fnpa), pa = t - pc * npa;
         const int ia = P.prim_off + pab0 + pa, ic = Q.prim_off + pcd0 + pc;
         const double zeta = prim[ia], eta = prim[ic];
         const double px = prim[2 * tot_np + ia], py = prim[3 * tot_np + ia], pz = prim[4 * tot_np + ia];
         const double qx = prim[2 * tot_np + ic], qy = prim[3 * tot_np + ic], qz = prim[4 * tot_np + ic];
         const double ze = zeta + eta, zei = 1.0 / ze, rho = zeta * eta * zei;
-        const double hz = 0.5 / zeta, he = 0.5 / eta;
         const double dx = px - qx, dy = py - qy, dz = pz - qz;
         const double T = rho * (dx * dx + dy * dy + dz * dz);
+        double x, w;
+        rys_one<NR>(ra, T, r, x, w);
         const double fact = prim[tot_np + ia] * prim[tot_np + ic] * sqrt(zei);
-        const double pax = px - P.A[0], pay = py - P.A[1], paz = pz - P.A[2];
-        const double qcx = qx - Q.A[0], qcy = qy - Q.A[1], qcz = qz - Q.A[2];
-        double x[NR], w[NR];
-        rys_all<NR>(ra, T, x, w);
-        double* cr = cf + t * CFT;
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-          const double U2 = x[r] * zei;
-          double* c = cr + r * 10;
-          c[0] = 0.5 * U2;
-          c[1] = hz - hz * U2 * eta;
-          c[2] = he - he * U2 * zeta;
-          c[3] = pax - eta * U2 * dx;
-          c[4] = pay - eta * U2 * dy;
-          c[5] = paz - eta * U2 * dz;
-          c[6] = qcx + zeta * U2 * dx;
-          c[7] = qcy + zeta * U2 * dy;
-          c[8] = qcz + zeta * U2 * dz;
-          c[9] = w[r] * fact;
+        const double U2 = x * zei;
+        double* c = cf + t * CFT + r * 10;
+        c[0] = 0.5 * U2;
+        c[1] = 0.5 * (1.0 - U2 * eta) / zeta;
+        c[2] = 0.5 * (1.0 - U2 * zeta) / eta;
+        c[3] = px - P.A[0] - eta * U2 * dx;
+        c[4] = py - P.A[1] - eta * U2 * dy;
+        c[5] = pz - P.A[2] - eta * U2 * dz;
+        c[6] = qx - Q.A[0] + zeta * U2 * dx;
+        c[7] = qy - Q.A[1] + zeta * U2 * dy;
+        c[8] = qz - Q.A[2] + zeta * U2 * dz;
+        c[9] = w * fact;
+        if (r == 0) {
+          double* e = cf + t * CFT + NR * 10;
+          e[0] = 2.0 * prim[5 * tot_np + ia];         // 2 alpha
+          e[1] = 2.0 * prim[6 * tot_np + ia];         // 2 beta
+          e[2] = 2.0 * prim[5 * tot_np + ic];         // 2 gamma
+          e[3] = Cab[pab0 + pa] * Ccd[pcd0 + pc];     // single-contraction coefficient
         }
-        double* e = cr + NR * 10;
-        e[0] = 2.0 * prim[5 * tot_np + ia];         // 2 alpha
-        e[1] = 2.0 * prim[6 * tot_np + ia];         // 2 beta
-        e[2] = 2.0 * prim[5 * tot_np + ic];         // 2 gamma
-        e[3] = Cab[pab0 + pa] * Ccd[pcd0 + pc];     // single-contraction coefficient
       }
       gsync(g, tpq);
       // ---- (3) primitive 2-PDM (Tcrtnc): bra half-transform of Y, or the single
@@ -344,61 +366,54 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
       for (int r0 = 0; r0 < NR; r0 += RW) {
         const int nrw = min(RW, NR - r0);
         const FDiv fnrw = fdiv(nrw);
-        // ---- (2a) 2D recursion per (quartet, root, direction), column by column in
-        //      registers: G[f][e], e at A, f at C
-        for (int job = tid; job < nt * nrw * 3; job += tpq) {
-          const int d = job % 3, tr = job / 3, t = fq(tr, fnrw), rl = tr - t * nrw, r = r0 + rl;
-          const double* c = cf + t * CFT + r * 10;
-          const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
-          double* G = S + (size_t)job * scr;
-          double Cm[NI], Cc[NI], Cn[NI];
-          Cc[0] = d == 2 ? c[9] : 1.0;
-          if (NI > 1) Cc[1] = C00 * Cc[0];
-#pragma unroll
-          for (int i = 1; i < NI - 1; ++i) Cc[i + 1] = C00 * Cc[i] + i * B10 * Cc[i - 1];
-#pragma unroll
-          for (int i = 0; i < NI; ++i) {
-            G[i] = Cc[i];
-            Cm[i] = 0.0;
-          }
-#pragma unroll
-          for (int j = 0; j < NJ - 1; ++j) {
-#pragma unroll
-            for (int i = 0; i < NI; ++i) {
-              double v = D00 * Cc[i];
-              if (j > 0) v = fma(j * B01, Cm[i], v);
-              if (i > 0) v = fma(i * B00, Cc[i > 0 ? i - 1 : 0], v);
-              Cn[i] = v;
-              G[(j + 1) * NI + i] = v;
+        // ---- (2a+2b) 2D recursion and ket 2D-level HRR (HRR2Db): one 8-lane group per
+        //      (quartet, root, direction) job; lane e holds the row G[e][0..NJ-1] in registers
+        //      and takes G[e-1][j] from its neighbour:
+        //        G[e][j+1] = D00 G[e][j] + j B01 G[e][j-1] + e B00 G[e-1][j],
+        //        V[e][c][0] = G[e][c],  V[e][c][d+1] = V[e][c+1][d] + CD V[e][c][d]
+        {
+          const int njobs = nt * nrw * 3;
+          const int lane = tid & 31;
+          for (int ob = tid - lane; ob < njobs * 8; ob += tpq) {  // warp-uniform trip count
+            const int o = ob + lane;
+            const int e = o & 7;
+            const bool valid = (o >> 3) < njobs && e < NI;
+            const int job = min(o >> 3, njobs - 1);
+            const int d = job % 3, tr = job / 3, t = fq(tr, fnrw), rl = tr - t * nrw, r = r0 + rl;
+            const double* c = cf + t * CFT + r * 10;
+            const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
+            // column 0 by the recursion over e: G[i+1][0] = C00 G[i][0] + i B10 G[i-1][0]
+            double gm1 = 0.0, g0 = d == 2 ? c[9] : 1.0;
+            for (int i = 0; i < e; ++i) {
+              const double gn = fma(i * B10, gm1, C00 * g0);
+              gm1 = g0;
+              g0 = gn;
             }
+            double L[NJ];
+            L[0] = g0;
 #pragma unroll
-            for (int i = 0; i < NI; ++i) {
-              Cm[i] = Cc[i];
-              Cc[i] = Cn[i];
+            for (int j = 0; j < NJ - 1; ++j) {
+              const double up = __shfl_up_sync(0xffffffffu, L[j], 1, 8);  // G[e-1][j]
+              double v = D00 * L[j];
+              if (j > 0) v = fma(j * B01, L[j > 0 ? j - 1 : 0], v);
+              if (e > 0) v = fma(e * B00, up, v);
+              L[j + 1] = v;
             }
-          }
-        }
-        gsync(g, tpq);
-        // ---- (2b) ket 2D-level HRR (HRR2Db), one thread per (job, e) row in registers:
-        //      V[e][c][0] = G[e][c],  V[e][c][d+1] = V[e][c+1][d] + CD V[e][c][d]
-        for (int o = tid; o < nt * nrw * 3 * NI; o += tpq) {
-          const int job = o / NI, e = o - job * NI, d = job % 3;
-          const double* gr = S + (size_t)job * scr + e;
-          double* Vo = S + (size_t)job * scr + NI * NJ + e;
-          const double cdv = hdr[3 + d];
-          double L[NJ];
+            double* Vo = S + (size_t)job * scr + e;
+            const double cdv = hdr[3 + d];
 #pragma unroll
-          for (int f = 0; f < NJ; ++f) L[f] = gr[f * NI];
+            for (int m = 0; m < NJ; ++m) {
+              if (m > ld) break;
+              if (m > 0) {
 #pragma unroll
-          for (int m = 0; m < NJ; ++m) {
-            if (m > ld) break;
-            if (m > 0) {
+                for (int cc = 0; cc + m < NJ; ++cc) L[cc] = fma(cdv, L[cc], L[cc + 1]);
+              }
+              if (valid) {
 #pragma unroll
-              for (int c = 0; c + m < NJ; ++c) L[c] = fma(cdv, L[c], L[c + 1]);
+                for (int cc = 0; cc + m < NJ; ++cc)
+                  if (cc <= lc + 1) Vo[NIp * (cc + (lc + 2) * m)] = L[cc];
+              }
             }
-#pragma unroll
-            for (int c = 0; c + m < NJ; ++c)
-              if (c <= lc + 1) Vo[NIp * (c + (lc + 2) * m)] = L[c];
           }
         }
         gsync(g, tpq);
@@ -413,7 +428,7 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
           for (int o = tid; o < nt * nrw * 3 * ncd1; o += tpq) {
             const int job = fq(o, fcd), r = o - job * ncd1, dd = fq(r, fc1), cc = r - dd * (lc + 1);
             const int d = job % 3, t = fq(job, f3rw);
-            const double* V = S + (size_t)job * scr + NI * NJ + NIp * ((lc + 2) * dd + cc);
+            const double* V = S + (size_t)job * scr + NIp * ((lc + 2) * dd + cc);
             const double ab = hdr[d];
             const double* ex = cf + t * CFT + NR * 10;
             const double e2a = ex[0], e2b = ex[1], e2c = ex[2];
