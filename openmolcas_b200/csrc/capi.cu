@@ -64,6 +64,9 @@ int build_eri_items(Handle* h, const int32_t* q4, int64_t nq, const int64_t* off
       cs.max_npcd = std::max(cs.max_npcd, Q.np);
       cs.max_cab = std::max(cs.max_cab, nij * P.np);
       cs.max_ccd = std::max(cs.max_ccd, nklc * Q.np);
+      cs.max_ne = std::max(cs.max_ne, P.ne);
+      cs.max_nf = std::max(cs.max_nf, Q.ne);
+      cs.max_nc = std::max(cs.max_nc, nij * nklc);
     }
   }
   items.clear();
@@ -96,16 +99,19 @@ int build_eri_items(Handle* h, const int32_t* q4, int64_t nq, const int64_t* off
 int run_eri_items(Handle* h, const std::vector<EriItem>& items, const std::vector<EriClass>& classes, double* d_out,
                   cudaStream_t st) {
   if (items.empty()) return 0;
+  if (!h->d_eri_counters && cudaMalloc(&h->d_eri_counters, sizeof(int) * 64) != cudaSuccess) {
+    h->err = "ERI work counters: allocation failed";
+    return MG_ERR_MEMORY;
+  }
   EriItem* d_items = (EriItem*)ws_get(h, sizeof(EriItem) * items.size(), st);
   if (!d_items) { h->err = "workspace allocation failed"; return MG_ERR_MEMORY; }
   cudaMemcpyAsync(d_items, items.data(), sizeof(EriItem) * items.size(), cudaMemcpyHostToDevice, st);
-  for (const EriClass& c : classes) {
-    for (int b = 0; b < c.count; b += (1 << 28)) {
-      int n = std::min(c.count - b, 1 << 28);
-      if (eri_launch_class(h, d_items + c.begin + b, n, c.nab, c.ncd, c.plan, d_out, st)) {
-        h->err = std::string("ERI kernel launch failed: ") + cudaGetErrorString(cudaGetLastError());
-        return MG_ERR_CUDA;
-      }
+  cudaMemsetAsync(h->d_eri_counters, 0, sizeof(int) * 64, st);
+  for (size_t ci = 0; ci < classes.size(); ++ci) {
+    const EriClass& c = classes[ci];
+    if (eri_launch_class(h, d_items + c.begin, c.count, c.nab, c.ncd, c.plan, d_out, h->d_eri_counters + ci, st)) {
+      h->err = std::string("ERI kernel launch failed: ") + cudaGetErrorString(cudaGetLastError());
+      return MG_ERR_CUDA;
     }
   }
   return 0;
@@ -148,6 +154,7 @@ int mg_destroy(mg_handle* H) {
   cudaSetDevice(h->device);
   free_basis(h);
   cudaFree(h->d_rys);
+  cudaFree(h->d_eri_counters);
   if (h->ws.ptr) cudaFree(h->ws.ptr);
   delete H;
   return 0;

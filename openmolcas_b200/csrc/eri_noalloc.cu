@@ -28,19 +28,26 @@ namespace mg {
 static const int kNoAllocMaxItems = 65536;
 
 static __device__ __align__(256) EriItem g_noalloc_items[kNoAllocMaxItems];
+// work counters of the class launches (one per class, at most 64 classes)
+static __device__ int g_noalloc_counters[64];
 
 static const int kMaxDevices = 64;
 static EriItem* g_noalloc_ptr[kMaxDevices] = {nullptr};
+static int* g_noalloc_cnt[kMaxDevices] = {nullptr};
 static std::mutex g_noalloc_mutex;
 
-// Device address of g_noalloc_items on `device` (set up on first use; the
-// device must be current).  Returns nullptr on failure.
+// Device address of g_noalloc_items on `device` (set up on first use, with
+// that of g_noalloc_counters; the device must be current).  Returns nullptr
+// on failure.
 static EriItem* noalloc_items_ptr(int device) {
   if (device < 0 || device >= kMaxDevices) return nullptr;
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   if (!g_noalloc_ptr[device]) {
     void* p = nullptr;
+    void* c = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_items) != cudaSuccess) return nullptr;
+    if (cudaGetSymbolAddress(&c, g_noalloc_counters) != cudaSuccess) return nullptr;
+    g_noalloc_cnt[device] = (int*)c;
     g_noalloc_ptr[device] = (EriItem*)p;
   }
   return g_noalloc_ptr[device];
@@ -84,8 +91,14 @@ extern "C" int mg_eri_quartets_noalloc(mg_handle* H, const int32_t* q4, int64_t 
     h->err = "mg_eri_quartets_noalloc: work-item upload failed";
     return MG_ERR_CUDA;
   }
-  for (const EriClass& c : classes) {
-    if (eri_launch_class(h, d_items + c.begin, c.count, c.nab, c.ncd, c.plan, d_out, st)) {
+  int* d_cnt = g_noalloc_cnt[h->device];
+  if (cudaMemsetAsync(d_cnt, 0, sizeof(int) * 64, st) != cudaSuccess) {
+    h->err = "mg_eri_quartets_noalloc: counter reset failed";
+    return MG_ERR_CUDA;
+  }
+  for (size_t ci = 0; ci < classes.size(); ++ci) {
+    const EriClass& c = classes[ci];
+    if (eri_launch_class(h, d_items + c.begin, c.count, c.nab, c.ncd, c.plan, d_out, d_cnt + ci, st)) {
       h->err = std::string("ERI kernel launch failed: ") + cudaGetErrorString(cudaGetLastError());
       return MG_ERR_CUDA;
     }

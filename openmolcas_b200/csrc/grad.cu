@@ -244,7 +244,7 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
 }
 
 int grad_run(Handle* h, const GradPlan& plan, const double* d_D, double* d_grad, cudaStream_t st) {
-  RysArgsG ra;
+  RysArgs ra;
   for (int i = 0; i < MG_MAX_RYS; ++i) ra.m[i] = h->rys_meta[i];
   ra.tab = h->d_rys;
   cudaMemsetAsync(d_grad, 0, sizeof(double) * 3 * h->natom, st);

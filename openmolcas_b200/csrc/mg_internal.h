@@ -59,6 +59,7 @@ struct ClassPlan {
 };
 struct ClassStats {
   int max_acc = 0, max_nef = 0, max_tmp = 0, max_nij = 0, max_npab = 0, max_npcd = 0, max_cab = 0, max_ccd = 0;
+  int max_ne = 0, max_nf = 0, max_nc = 0;
 };
 struct EriClass {
   int nab, ncd, begin, count;
@@ -99,6 +100,7 @@ struct Handle {
   std::string err;
   struct ChoState* cho = nullptr;  // Cholesky vectors of the current basis
   struct GradPlan* grad = nullptr; // gradient work list (per Schwarz threshold)
+  int* d_eri_counters = nullptr;   // one work counter per ERI class launch (64)
 };
 
 struct GradItem {
@@ -167,7 +169,7 @@ void* ws_get(Handle* h, size_t bytes, cudaStream_t st);
 // ERI work lists (capi.cu) and launchers (eri.cu)
 ClassPlan eri_plan(int nab, int ncd, const ClassStats& cs);
 int eri_launch_class(Handle* h, const EriItem* d_items, int nitems, int nab, int ncd, const ClassPlan& pl, double* out,
-                     cudaStream_t st);
+                     int* d_counter, cudaStream_t st);
 int build_eri_items(Handle* h, const int32_t* q4, int64_t nq, const int64_t* offsets, std::vector<EriItem>& items,
                     std::vector<EriClass>& classes);
 int run_eri_items(Handle* h, const std::vector<EriItem>& items, const std::vector<EriClass>& classes, double* d_out,
