@@ -10,6 +10,11 @@ beside it, with the energy difference between the two.  Inputs are seeded
 synthetic molecules (no data files).  Set-up (integrals, Cholesky
 decomposition) is outside the timed region.
 
+Second metric (key "eri"): FP64 ERI throughput in quartets/s of the batched
+Drv2El-style entry point over a seeded 2 000 000-quartet sample of the
+Schwarz-screened (1e-12) unique shell quartets of the 40-atom / 600-function
+cluster with uneven classes (l <= 3, 1-12 primitives per shell).
+
 Prints one JSON line (rank 0).  --impl reference times the CPU restatement
 of the reference path (oracle port) on a bounded sample instead.
 """
@@ -31,6 +36,9 @@ sys.path.insert(0, ROOT)
 
 JK_CFG = "c3"
 GRAD_CFG = "c4"
+ERI_CFG = "c2"
+ERI_SAMPLE = 2_000_000
+C3_NVEC = 12865  # Cholesky vectors of the 1500-function cluster at ThrCom 1e-6
 THRCOM = 1e-6
 CUTINT = 1e-12
 
@@ -147,6 +155,72 @@ extern "C" float run_peak(int blocks, int threads, int iters) {
 
 
 # --------------------------------------------------------------- workload
+def eri_leg(torch, device, reps=2):
+    """FP64 ERI throughput over a seeded sample of the screened unique quartets
+    (one warm-up call, then `reps` timed calls through MolGpu.eri_quartets;
+    host quartet lists, device output)."""
+    from openmolcas_b200 import basis as B
+    from openmolcas_b200.molgpu import MolGpu, unique_quartets, lib as mglib
+    m2 = B.config_molecule(ERI_CFG)
+    g2 = MolGpu(m2, device)
+    tm = g2.schwarz()
+    q = unique_quartets(len(m2.shells), tm, CUTINT)
+    rng = np.random.default_rng(0)
+    sel = q[np.sort(rng.choice(len(q), min(ERI_SAMPLE, len(q)), replace=False))]
+    off = g2.quartet_offsets(sel)
+    out = torch.empty(int(off[-1]), dtype=torch.float64, device=f"cuda:{device}")
+    g2.eri_quartets(sel, out)
+    torch.cuda.synchronize()
+    ms = []
+    n0 = mglib().mg_kernel_launches()
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g2.eri_quartets(sel, out)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    launches = (mglib().mg_kernel_launches() - n0) // reps
+    ms_mean = float(np.mean(ms))
+    res = {"value": len(sel) / (ms_mean / 1e3), "unit": "quartets/s", "ms": ms_mean, "quartets": int(len(sel)),
+           "screened_unique_quartets": int(len(q)), "integrals_gb": float(off[-1]) * 8 / 1e9,
+           "workload": f"{ERI_CFG}: 40 atoms, {m2.nbf} bf, Schwarz {CUTINT}, seeded sample of {len(sel)} of "
+                       f"{len(q)} unique quartets", "gpu_launches": int(launches), "dtype": "f64",
+           "sample_quartets": sel}
+    del out
+    torch.cuda.empty_cache()
+    return res
+
+
+def eri_cpu_baseline(sel, budget_s=10.0, threads=None):
+    """Oracle ERIs over random quartets of the same seeded sample, one quartet
+    per call on `threads` host threads (all cores by default), until the time
+    budget is used: quartets/s."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    from openmolcas_b200 import basis as B
+    threads = threads or os.cpu_count() or 1
+    o = O.Oracle(B.config_molecule(ERI_CFG))
+    order = np.random.default_rng(1).permutation(len(sel))
+    counts = [0] * threads
+    t0 = time.time()
+    stop = t0 + budget_s
+
+    def work(w):
+        for k in range(w, len(order), threads):
+            if time.time() > stop:
+                break
+            o.eri_quartet(*[int(v) for v in sel[order[k]]])
+            counts[w] += 1
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(work, range(threads)))
+    dt = time.time() - t0
+    n = sum(counts)
+    return {"value": n / dt, "unit": "quartets/s", "cores": threads, "kind": "port",
+            "sample": f"{n} random quartets of the same seeded sample in {dt:.1f}s"}
+
+
 def setup(torch, device):
     from openmolcas_b200 import basis as B
     from openmolcas_b200.molgpu import MolGpu
@@ -189,6 +263,14 @@ def run_gpu(args, rank, world):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from openmolcas_b200.molgpu import MolGpu, lib as mglib
+    if dist:
+        dist.barrier()
+    eri = eri_leg(torch, local)
+    if dist:  # replicas: every rank runs the same sample; whole-job throughput over the slowest rank
+        t = torch.tensor([eri["ms"]], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        eri["ms"] = float(t.item())
+        eri["value"] = world * eri["quartets"] / (eri["ms"] / 1e3)
     S = setup(torch, local)
     g3, g4, C3, D4 = S["g3"], S["g4"], S["C3"], S["D4"]
     dev = f"cuda:{local}"
@@ -295,6 +377,9 @@ def run_gpu(args, rank, world):
     roof["kernel"] = dom
     roof["traffic"] = None
     cpu = cpu_baseline(S)
+    eri_sel = eri.pop("sample_quartets")
+    if rank == 0 and world == 1:
+        eri["cpu_baseline"] = eri_cpu_baseline(eri_sel)
     res = {
         "metric": "J/K+grad seconds per step (J/K mixed @1500 bf + 2e gradient @460 bf)",
         "value": ms / 1e3 * 1.0,
@@ -323,6 +408,7 @@ def run_gpu(args, rank, world):
         "roofline_legs": legs,
         "clocks": clocks,
         "cpu_baseline": cpu,
+        "eri": eri,
     }
     if rank == 0:
         print(json.dumps(res), flush=True)
@@ -354,7 +440,9 @@ def cpu_baseline(S=None, budget_s=20.0, threads=None):
         os.environ["OMP_NUM_THREADS"] = str(threads)
     m3 = S["m3"] if S else B.config_molecule(JK_CFG)
     m4 = S["m4"] if S else B.config_molecule(GRAD_CFG)
-    M = S["cho"]["M"] if S else 7 * m3.nbf // 2  # typical vectors per function at ThrCom 1e-6
+    # without a GPU run: the vector count of this decomposition (ThrCom 1e-6), which the
+    # GPU arm reports as cholesky.M (its pivots equal the oracle's)
+    M = S["cho"]["M"] if S else C3_NVEC
     o3 = O.Oracle(m3)
     nrs = m3.nbf * (m3.nbf + 1) // 2
     rng = np.random.default_rng(0)
@@ -392,6 +480,19 @@ def run_reference(args):
         if k >= args.warmup:
             vals.append(cb["value"])
     v = float(np.mean(vals))
+    eri_ref = None
+    try:  # ERI throughput of the CPU restatement on the same seeded quartet sample
+        from oracle import oracle as O
+        from openmolcas_b200 import basis as B
+        from openmolcas_b200.molgpu import unique_quartets
+        m2 = B.config_molecule(ERI_CFG)
+        tm = O.Oracle(m2).schwarz()
+        q = unique_quartets(len(m2.shells), tm, CUTINT)
+        rng = np.random.default_rng(0)
+        sel = q[np.sort(rng.choice(len(q), min(ERI_SAMPLE, len(q)), replace=False))]
+        eri_ref = eri_cpu_baseline(sel, threads=cores)
+    except Exception as e:  # the main metric stands without it
+        eri_ref = {"unavailable": str(e)[:200]}
     res = {
         "metric": "J/K+grad seconds per step (J/K mixed @1500 bf + 2e gradient @460 bf)",
         "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -400,6 +501,7 @@ def run_reference(args):
         "config": {"workload": f"J/K {JK_CFG} + gradient {GRAD_CFG} (CPU restatement of the reference path)"},
         "cpu_baseline": {"value": v, "unit": "s", "cores": cb["cores"], "kind": "port", "sample": cb["sample"]},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "eri": eri_ref,
     }
     print(json.dumps(res), flush=True)
     return 0
