@@ -9,10 +9,11 @@
 // Mixed path: vectors stored FP32; per block of vectors the rs-packed L_J
 // are unpacked straight into split BF16 pairs (hi + lo, hi = bf16(x),
 // lo = bf16(x - hi)); both GEMMs run as 3 BF16 tensor-core products
-// (hi*hi + hi*lo + lo*hi) with FP32 accumulation; each block's partial K is
-// FP32 over nb*r terms and is added to the FP64 result, so accumulation error
-// does not grow with the number of vectors.  J uses FP32 loads with FP64
-// accumulation.
+// (hi*hi + hi*lo + lo*hi) with FP32 accumulation.  The exchange product
+// K += X X^T is the hand-written tcgen05 kernel of tc_syrk.cuh (TMA-fed,
+// lower-triangle tiles, FP32 in tensor memory over one block's nb*r terms,
+// FP64 atomic accumulation), so accumulation error does not grow with the
+// number of vectors.  J uses FP32 loads with FP64 accumulation.
 //
 // FP64 path ("plain FP64 GPU path"): vectors in FP64, per block of vectors
 // the rs-packed L_J are unpacked to dense symmetric nbf x nbf matrices, the
@@ -20,13 +21,16 @@
 // LK screening is not applied (dense tensor work is cheaper on the GPU than
 // the screening bookkeeping); the result equals the unscreened reference.
 #include <cublas_v2.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "mg_internal.h"
+#include "tc_syrk.cuh"
 
 namespace mg {
 
@@ -165,23 +169,54 @@ __global__ void k_split_c(const double* __restrict__ C, int n, int r, int ld, __
   lo[o] = l;
 }
 
-// K (n x n FP64) += Kb (ld x ld FP32)
-__global__ void k_add_kb(const float* __restrict__ Kb, int ld, double* __restrict__ K, int n) {
-  int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (o >= (int64_t)n * n) return;
-  const int i = (int)(o % n), j = (int)(o / n);
-  K[o] += (double)Kb[(size_t)i + (size_t)ld * j];
+// X^T split: XThi/XTlo[a][k] (row a < ldt, k < kpad, K index contiguous) from
+// X (column-major ld x kcols, FP32); zero outside X.  32 x 32 tiles through
+// shared memory so that both the read and the write are coalesced.
+__global__ void k_split_t(const float* __restrict__ X, int ld, int kcols, int ldt, int kpad,
+                          __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+  __shared__ float tile[32][33];
+  const int k0 = blockIdx.x * 32, a0 = blockIdx.y * 32;
+  for (int i = 0; i < 32; i += 8) {
+    const int a = a0 + threadIdx.x, k = k0 + threadIdx.y + i;
+    tile[threadIdx.y + i][threadIdx.x] = (a < ld && k < kcols) ? X[a + (size_t)ld * k] : 0.0f;
+  }
+  __syncthreads();
+  for (int i = 0; i < 32; i += 8) {
+    const int k = k0 + threadIdx.x, a = a0 + threadIdx.y + i;
+    if (a < ldt && k < kpad) {
+      __nv_bfloat16 h, l;
+      split_bf16(tile[threadIdx.x][threadIdx.y + i], h, l);
+      hi[(size_t)a * kpad + k] = h;
+      lo[(size_t)a * kpad + k] = l;
+    }
+  }
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on the driver library).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  });
+  return fn;
+}
 
-__global__ void k_split_f32(const float* __restrict__ x, int64_t n, __nv_bfloat16* __restrict__ hi,
-                            __nv_bfloat16* __restrict__ lo) {
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  __nv_bfloat16 h, l;
-  split_bf16(x[t], h, l);
-  hi[t] = h;
-  lo[t] = l;
+// 2D BF16 tensor map over rows x kpad (K contiguous), 64 x 128 boxes, 128-byte swizzle.
+static bool make_operand_map(CUtensorMap* m, const __nv_bfloat16* base, int rows, int kpad) {
+  auto enc = tensor_map_encoder();
+  if (!enc || ((uintptr_t)base & 15) || (kpad * 2) % 16) return false;
+  cuuint64_t gdim[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
+  cuuint64_t gstr[1] = {(cuuint64_t)kpad * 2};
+  cuuint32_t box[2] = {(cuuint32_t)kTcBK, (cuuint32_t)kTcTile}, es[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // V[J] += sum_t L[t,J] dw[t] over one row chunk (FP32 loads, FP64 accumulation);
@@ -230,8 +265,18 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   const int* d_ra = cho_rs_a_dev(c);
   const int* d_rb = cho_rs_b_dev(c);
   const size_t nn = (size_t)n * n, ll = (size_t)ld * ld, lbr = (size_t)ld * block * r;
+  // exchange GEMM on the tensor cores: X^T rows padded to the 128-row tile, K range split so
+  // that the lower-triangle tiles x splits cover the SMs
+  const int ldt = (n + 127) / 128 * 128;
+  const int ntile = (ldt / kTcTile) * (ldt / kTcTile + 1) / 2;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+  const int nsplit = std::max(1, std::min(8, (nsm + ntile - 1) / ntile));
+  const int kq = kTcBK * nsplit;
+  const int kpad = (block * r + kq - 1) / kq * kq;
+  const size_t xt = (size_t)ldt * kpad;
   size_t need = 8 * ((size_t)2 * nrs + block + nn) + 2 * (2 * (size_t)ld * r) + 2 * (2 * (size_t)block * ll) +
-                4 * lbr + 2 * (2 * lbr) + 4 * ll + 16 * 256;
+                4 * lbr + 2 * (2 * xt) + 16 * 256;
   char* ws = (char*)ws_get(h, need, st);
   if (!ws) { h->err = "jk workspace allocation failed"; return MG_ERR_MEMORY; }
   auto take = [&](size_t bytes) { char* p = ws; ws += (bytes + 255) & ~(size_t)255; return (void*)p; };
@@ -244,9 +289,18 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   __nv_bfloat16* Lhi = (__nv_bfloat16*)take(2 * (size_t)block * ll);
   __nv_bfloat16* Llo = (__nv_bfloat16*)take(2 * (size_t)block * ll);
   float* X = (float*)take(4 * lbr);
-  __nv_bfloat16* Xhi = (__nv_bfloat16*)take(2 * lbr);
-  __nv_bfloat16* Xlo = (__nv_bfloat16*)take(2 * lbr);
-  float* Kb = (float*)take(4 * ll);
+  __nv_bfloat16* XThi = (__nv_bfloat16*)take(2 * xt);
+  __nv_bfloat16* XTlo = (__nv_bfloat16*)take(2 * xt);
+  int* d_err = (int*)take(sizeof(int));
+  CUtensorMap map_hi, map_lo;
+  if (!make_operand_map(&map_hi, XThi, ldt, kpad) || !make_operand_map(&map_lo, XTlo, ldt, kpad)) {
+    h->err = "tensor map for the exchange GEMM could not be encoded";
+    return MG_ERR_CUDA;
+  }
+  static std::once_flag smem_once;
+  std::call_once(smem_once,
+                 [] { cudaFuncSetAttribute(tc_syrk3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem); });
+  cudaMemsetAsync(d_err, 0, sizeof(int), st);
   const double one = 1.0, zero = 0.0;
   const float onef = 1.0f, zerof = 0.0f;
   cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, r, &one, d_C, n, d_C, n, &zero, D, n);
@@ -280,20 +334,26 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
       cublasGemmStridedBatchedEx(cb, CUBLAS_OP_N, CUBLAS_OP_N, ld, r, ld, &onef, As[q], CUDA_R_16BF, ld, (long long)ll,
                                  Bs[q], CUDA_R_16BF, ld, 0, q == 0 ? &zerof : &onef, X, CUDA_R_32F, ld,
                                  (long long)ld * r, nb, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
-    // K_b = X X^T over this block (3 split products), then K += K_b in FP64
-    k_split_f32<<<nb256((int64_t)ld * nb * r), 256, 0, st>>>(X, (int64_t)ld * nb * r, Xhi, Xlo);
+    // K += X X^T over this block: split-BF16 X^T (K-major), then the tcgen05 kernel
+    // (3 products into one FP32 accumulator per tile, FP64 atomic add into K)
+    k_split_t<<<dim3(kpad / 32, ldt / 32), dim3(32, 8), 0, st>>>(X, ld, nb * r, ldt, kpad, XThi, XTlo);
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    const __nv_bfloat16* Ps[3] = {Xhi, Xhi, Xlo};
-    const __nv_bfloat16* Qs[3] = {Xhi, Xlo, Xhi};
-    for (int q = 0; q < 3; ++q)
-      cublasGemmEx(cb, CUBLAS_OP_N, CUBLAS_OP_T, ld, ld, nb * r, &onef, Ps[q], CUDA_R_16BF, ld, Qs[q], CUDA_R_16BF, ld,
-                   q == 0 ? &zerof : &onef, Kb, CUDA_R_32F, ld, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
-    k_add_kb<<<nb256((int64_t)nn), 256, 0, st>>>(Kb, ld, d_K, n);
+    tc_syrk3_kernel<<<dim3(ntile, nsplit), 128, kTcSmem, st>>>(map_hi, map_lo, n, kpad, d_K, d_err);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
+  k_symmetrize_lower<<<nb256((int64_t)nn), 256, 0, st>>>(d_K, n);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   k_unpack_sym<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, jrs, n, d_J);
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  return cudaGetLastError() == cudaSuccess ? 0 : MG_ERR_CUDA;
+  if (cudaGetLastError() != cudaSuccess) return MG_ERR_CUDA;
+  int herr = 0;
+  cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return MG_ERR_CUDA;
+  if (herr) {
+    h->err = "exchange GEMM: a pipeline wait ran out (result incomplete)";
+    return MG_ERR_CUDA;
+  }
+  return 0;
 }
 
 }  // namespace mg
