@@ -138,23 +138,46 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bflo
   lo = __float2bfloat16_rn(x - __bfloat162float(hi));
 }
 
-// Lhi/Llo[J][a][b] (= [J][b][a]) from the FP32 rs vectors of a block
-// (squares with leading dimension ld >= n; the padding stays zero)
-__global__ void k_unpack_block_split(const int* __restrict__ rs_a, const int* __restrict__ rs_b, int64_t nrs,
-                                     const float* __restrict__ L, int nb, int ld, __nv_bfloat16* __restrict__ Lhi,
-                                     __nv_bfloat16* __restrict__ Llo) {
-  int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (o >= nrs * nb) return;
-  const int64_t t = o % nrs;
-  const int64_t J = o / nrs;
+// inv[a*n + b] = inv[b*n + a] = t for every rs pair t (entries outside the
+// reduced set stay -1)
+__global__ void k_rs_inverse(const int* __restrict__ rs_a, const int* __restrict__ rs_b, int64_t nrs, int n,
+                             int* __restrict__ inv) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nrs) return;
   const int a = rs_a[t], b = rs_b[t];
-  __nv_bfloat16 hi, lo;
-  split_bf16(L[t + nrs * J], hi, lo);
-  const size_t base = (size_t)J * ld * ld;
-  Lhi[base + (size_t)a * ld + b] = hi;
-  Llo[base + (size_t)a * ld + b] = lo;
-  Lhi[base + (size_t)b * ld + a] = hi;
-  Llo[base + (size_t)b * ld + a] = lo;
+  inv[(size_t)a * n + b] = (int)t;
+  inv[(size_t)b * n + a] = (int)t;
+}
+
+// Dense split squares Lhi/Llo[J][a][b] (leading dimension ld, padding zero)
+// written row by row, two columns per thread (coalesced 4-byte stores); the
+// packed value is gathered through the inverse rs table.
+__global__ void k_unpack_dense_split(const int* __restrict__ inv, int n, int64_t nrs, const float* __restrict__ L,
+                                     int nb, int ld, __nv_bfloat162* __restrict__ Lhi,
+                                     __nv_bfloat162* __restrict__ Llo) {
+  const int64_t half = ld / 2;
+  int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (o >= (int64_t)nb * ld * half) return;
+  const int b2 = (int)(o % half);
+  const int64_t r1 = o / half;
+  const int a = (int)(r1 % ld);
+  const int J = (int)(r1 / ld);
+  float v[2];
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const int b = 2 * b2 + u;
+    float x = 0.0f;
+    if (a < n && b < n) {
+      const int t = inv[(size_t)a * n + b];
+      if (t >= 0) x = L[t + nrs * J];
+    }
+    v[u] = x;
+  }
+  __nv_bfloat16 h0, l0, h1, l1;
+  split_bf16(v[0], h0, l0);
+  split_bf16(v[1], h1, l1);
+  Lhi[o] = __halves2bfloat162(h0, h1);
+  Llo[o] = __halves2bfloat162(l0, l1);
 }
 
 // C (n x r, column-major FP64) -> split BF16 with leading dimension ld (padding zero)
@@ -276,7 +299,7 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   const int kpad = (block * r + kq - 1) / kq * kq;
   const size_t xt = (size_t)ldt * kpad;
   size_t need = 8 * ((size_t)2 * nrs + block + nn) + 2 * (2 * (size_t)ld * r) + 2 * (2 * (size_t)block * ll) +
-                4 * lbr + 2 * (2 * xt) + 16 * 256;
+                4 * lbr + 2 * (2 * xt) + 4 * nn + 16 * 256;
   char* ws = (char*)ws_get(h, need, st);
   if (!ws) { h->err = "jk workspace allocation failed"; return MG_ERR_MEMORY; }
   auto take = [&](size_t bytes) { char* p = ws; ws += (bytes + 255) & ~(size_t)255; return (void*)p; };
@@ -292,6 +315,7 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   __nv_bfloat16* XThi = (__nv_bfloat16*)take(2 * xt);
   __nv_bfloat16* XTlo = (__nv_bfloat16*)take(2 * xt);
   int* d_err = (int*)take(sizeof(int));
+  int* inv = (int*)take(4 * nn);
   CUtensorMap map_hi, map_lo;
   if (!make_operand_map(&map_hi, XThi, ldt, kpad) || !make_operand_map(&map_lo, XTlo, ldt, kpad)) {
     h->err = "tensor map for the exchange GEMM could not be encoded";
@@ -310,10 +334,9 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   g_launches.fetch_add(1, std::memory_order_relaxed);
   cudaMemsetAsync(jrs, 0, 8 * nrs, st);
   cudaMemsetAsync(d_K, 0, 8 * nn, st);
-  if (ld != n) {  // padding rows/columns of the squares stay zero
-    cudaMemsetAsync(Lhi, 0, 2 * (size_t)block * ll, st);
-    cudaMemsetAsync(Llo, 0, 2 * (size_t)block * ll, st);
-  }
+  cudaMemsetAsync(inv, 0xFF, 4 * nn, st);
+  k_rs_inverse<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, n, inv);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   const unsigned jchunks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(64, nrs / 8192));
   for (int J0 = 0; J0 < M; J0 += block) {
     const int nb = std::min(block, M - J0);
@@ -326,7 +349,8 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
     k_jacc<<<nb256(nrs), 256, 0, st>>>(Lb, nrs, nb, V, jrs);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     // Exchange: X_J = L_J C  (3 split products, FP32 accumulation)
-    k_unpack_block_split<<<nb256(nrs * nb), 256, 0, st>>>(d_ra, d_rb, nrs, Lb, nb, ld, Lhi, Llo);
+    k_unpack_dense_split<<<nb256((int64_t)nb * ld * (ld / 2)), 256, 0, st>>>(
+        inv, n, nrs, Lb, nb, ld, (__nv_bfloat162*)Lhi, (__nv_bfloat162*)Llo);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     const __nv_bfloat16* As[3] = {Lhi, Lhi, Llo};
     const __nv_bfloat16* Bs[3] = {Chi, Clo, Chi};
