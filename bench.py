@@ -155,6 +155,25 @@ extern "C" float run_peak(int blocks, int threads, int iters) {
 
 
 # --------------------------------------------------------------- workload
+def max_over_ranks(x, dist, device):
+    """Largest value of x over all ranks (device time of the slowest rank);
+    x itself when not distributed."""
+    if not dist:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def eri_aggregate(eri, world, max_ms):
+    """Whole-job ERI throughput of `world` replicas that each ran the same
+    sample, over the slowest replica's time."""
+    eri["ms"] = float(max_ms)
+    eri["value"] = world * eri["quartets"] / (eri["ms"] / 1e3)
+    return eri
+
+
 def eri_leg(torch, device, reps=2):
     """FP64 ERI throughput over a seeded sample of the screened unique quartets
     (one warm-up call, then `reps` timed calls through MolGpu.eri_quartets;
@@ -267,10 +286,7 @@ def run_gpu(args, rank, world):
         dist.barrier()
     eri = eri_leg(torch, local)
     if dist:  # replicas: every rank runs the same sample; whole-job throughput over the slowest rank
-        t = torch.tensor([eri["ms"]], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        eri["ms"] = float(t.item())
-        eri["value"] = world * eri["quartets"] / (eri["ms"] / 1e3)
+        eri_aggregate(eri, world, max_over_ranks(eri["ms"], dist, f"cuda:{local}"))
     S = setup(torch, local)
     g3, g4, C3, D4 = S["g3"], S["g4"], S["C3"], S["D4"]
     dev = f"cuda:{local}"
@@ -325,11 +341,7 @@ def run_gpu(args, rank, world):
     jk_d, gr_d, _, out_d = timed(MolGpu.PREC_FP64, max(2, min(args.steps, 3)), 1)
     step_m = (jk_m + gr_m) / 1e3
     step_d = (jk_d.mean() + gr_d.mean()) / 1e3
-    ms = float(step_m.mean() * 1e3)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(float(step_m.mean() * 1e3), dist, dev)
     # energies of both paths
     J, K, grad = out_m
     Jd, Kd, gradd = out_d

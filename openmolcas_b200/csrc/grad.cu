@@ -170,7 +170,7 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
     {
       const size_t cta = kCtaLimit / 8 - kGTabD;
       const int nthr = GradThreads<1>::value;
-      for (int tpq = wmax <= 64 ? 64 : wmax <= 512 ? 128 : 256; tpq <= nthr && !c.tpq; tpq *= 2) {
+      for (int tpq = wmax <= 512 ? 128 : 256; tpq <= nthr && !c.tpq; tpq *= 2) {
         const int groups = nthr / tpq;
         const size_t gb = (cta / groups) & ~(size_t)1;
         int pab = std::max(1, std::min(m.npab, 16)), pcd = std::max(1, std::min(m.npcd, 8)), rw = NRc;
