@@ -280,8 +280,10 @@ int setup_pairs(Handle* h) {
   h->prim_kept = kept;
   h->prim_total = total;
   h->tot_np = zeta.size();
+  std::vector<double> izeta(zeta.size());
+  for (size_t i = 0; i < zeta.size(); ++i) izeta[i] = 1.0 / zeta[i];
   std::vector<double> prim;
-  for (auto* v : {&zeta, &kappa, &px, &py, &pz, &al, &be}) prim.insert(prim.end(), v->begin(), v->end());
+  for (auto* v : {&zeta, &kappa, &px, &py, &pz, &al, &be, &izeta}) prim.insert(prim.end(), v->begin(), v->end());
   if (cudaMalloc(&h->d_prim, sizeof(double) * prim.size()) != cudaSuccess ||
       cudaMalloc(&h->d_coef, sizeof(double) * std::max<size_t>(coef.size(), 1)) != cudaSuccess ||
       cudaMalloc(&h->d_hrr, sizeof(double) * std::max<size_t>(hrr.size(), 1)) != cudaSuccess ||

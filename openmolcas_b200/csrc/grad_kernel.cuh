@@ -208,16 +208,29 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
   for (int pcd0 = 0; pcd0 < npcd; pcd0 += PCD) {
     const int npc = min(PCD, npcd - pcd0);
     gsync(g, tpq);
-    // ---- ket half-transform of the 2-PDM: Y[ij][pc][abcd] = sum_kl Ccd[kl][pc] Gam[ij,kl][abcd]
+    // ---- ket half-transform of the 2-PDM: Y[ij][pc][abcd] = sum_kl Ccd[kl][pc] Gam[ij,kl][abcd];
+    //      a thread makes 4 consecutive pc of one (ij, abcd), each Gam load feeds 4 FMAs
     if (multi) {
-      const FDiv f4 = fdiv(ncart4), fpc = fdiv(npc);
-      for (int o = tid; o < nij * npc * ncart4; o += tpq) {
-        const int r1 = fq(o, f4), abcd = o - r1 * ncart4, ij = fq(r1, fpc), pc = r1 - ij * npc;
+      const int npc4 = (npc + 3) >> 2;
+      const FDiv f4 = fdiv(ncart4), fpc = fdiv(npc4);
+      for (int o = tid; o < nij * npc4 * ncart4; o += tpq) {
+        const int r1 = fq(o, f4), abcd = o - r1 * ncart4, ij = fq(r1, fpc), pc0 = 4 * (r1 - ij * npc4);
         const double* gm = Gam + (size_t)ij * ncart4 + abcd;
-        double s = 0.0;
-        for (int klc = 0; klc < nklc; ++klc)
-          s = fma(Ccd[klc * npcd + pcd0 + pc], gm[(size_t)nij * klc * ncart4], s);
-        Y[abcd + ncart4 * (pc + PCD * ij)] = s;
+        const double* cc = Ccd + pcd0 + pc0;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        for (int klc = 0; klc < nklc; ++klc) {
+          const double gv = gm[(size_t)nij * klc * ncart4];
+          const double* ck = cc + klc * npcd;
+          s0 = fma(ck[0], gv, s0);
+          if (pc0 + 1 < npc) s1 = fma(ck[1], gv, s1);
+          if (pc0 + 2 < npc) s2 = fma(ck[2], gv, s2);
+          if (pc0 + 3 < npc) s3 = fma(ck[3], gv, s3);
+        }
+        double* y = Y + abcd + ncart4 * (pc0 + PCD * ij);
+        y[0] = s0;
+        if (pc0 + 1 < npc) y[ncart4] = s1;
+        if (pc0 + 2 < npc) y[2 * ncart4] = s2;
+        if (pc0 + 3 < npc) y[3 * ncart4] = s3;
       }
     }
     for (int pab0 = 0; pab0 < npab; pab0 += PAB) {
@@ -242,8 +255,8 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
         const double U2 = x * zei;
         double* c = cf + t * CFT + r * 10;
         c[0] = 0.5 * U2;
-        c[1] = 0.5 * (1.0 - U2 * eta) / zeta;
-        c[2] = 0.5 * (1.0 - U2 * zeta) / eta;
+        c[1] = 0.5 * (1.0 - U2 * eta) * prim[7 * tot_np + ia];
+        c[2] = 0.5 * (1.0 - U2 * zeta) * prim[7 * tot_np + ic];
         c[3] = px - P.A[0] - eta * U2 * dx;
         c[4] = py - P.A[1] - eta * U2 * dy;
         c[5] = pz - P.A[2] - eta * U2 * dz;
@@ -260,40 +273,60 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
         }
       }
       gsync(g, tpq);
-      // ---- (3) primitive 2-PDM (Tcrtnc): bra half-transform of Y, or the single
+      // ---- (3) primitive 2-PDM (Tcrtnc): bra half-transform of Y (a thread makes 4
+      //      consecutive pa of one (pc, abcd), each Y load feeds 4 FMAs), or the single
       //      contraction coefficient times the contracted 2-PDM
       {
-        const FDiv f4 = fdiv(ncart4);
-        for (int o = tid; o < nt * ncart4; o += tpq) {
-          const int t = fq(o, f4), abcd = o - t * ncart4;
-          double s = 0.0;
+        const int npa4 = (npa + 3) >> 2;
+        const FDiv f4 = fdiv(ncart4), fpa = fdiv(npa4);
+        for (int o = tid; o < npa4 * npc * ncart4; o += tpq) {
+          const int r1 = fq(o, f4), abcd = o - r1 * ncart4, pc = fq(r1, fpa), pa0 = 4 * (r1 - pc * npa4);
+          double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
           if (multi) {
-            const int pc = fq(t, fnpa), pa = t - pc * npa;
             const double* y = Y + abcd + ncart4 * pc;
-            for (int ij = 0; ij < nij; ++ij) s = fma(Cab[ij * npab + pab0 + pa], y[(size_t)ncart4 * PCD * ij], s);
+            const double* ca = Cab + pab0 + pa0;
+            for (int ij = 0; ij < nij; ++ij) {
+              const double yv = y[(size_t)ncart4 * PCD * ij];
+              const double* ci = ca + ij * npab;
+              s0 = fma(ci[0], yv, s0);
+              if (pa0 + 1 < npa) s1 = fma(ci[1], yv, s1);
+              if (pa0 + 2 < npa) s2 = fma(ci[2], yv, s2);
+              if (pa0 + 3 < npa) s3 = fma(ci[3], yv, s3);
+            }
           } else {
-            s = cf[t * CFT + NR * 10 + 3] * Gam[abcd];
+            const double gv = Gam[abcd];
+            const double* e3 = cf + (pa0 + npa * pc) * CFT + NR * 10 + 3;
+            s0 = e3[0] * gv;
+            if (pa0 + 1 < npa) s1 = e3[CFT] * gv;
+            if (pa0 + 2 < npa) s2 = e3[2 * CFT] * gv;
+            if (pa0 + 3 < npa) s3 = e3[3 * CFT] * gv;
           }
-          Gp[t * Gs + abcd] = s;
+          double* gp = Gp + (size_t)(pa0 + npa * pc) * Gs + abcd;
+          gp[0] = s0;
+          if (pa0 + 1 < npa) gp[Gs] = s1;
+          if (pa0 + 2 < npa) gp[2 * Gs] = s2;
+          if (pa0 + 3 < npa) gp[3 * Gs] = s3;
         }
       }
       gsync(g, tpq);
       for (int r0 = 0; r0 < NR; r0 += RW) {
         const int nrw = min(RW, NR - r0);
         const FDiv fnrw = fdiv(nrw);
-        // ---- (2a+2b) 2D recursion and ket 2D-level HRR (HRR2Db): one 8-lane group per
+        // ---- (2a+2b) 2D recursion and ket 2D-level HRR (HRR2Db): one 4- or 8-lane group per
         //      (quartet, root, direction) job; lane e holds the row G[e][0..NJ-1] in registers
         //      and takes G[e-1][j] from its neighbour:
         //        G[e][j+1] = D00 G[e][j] + j B01 G[e][j-1] + e B00 G[e-1][j],
         //        V[e][c][0] = G[e][c],  V[e][c][d+1] = V[e][c+1][d] + CD V[e][c][d]
         {
+          constexpr int LG = NI <= 4 ? 4 : 8;  // lanes per job (power of two >= NI)
+          constexpr int LS = NI <= 4 ? 2 : 3;
           const int njobs = nt * nrw * 3;
           const int lane = tid & 31;
-          for (int ob = tid - lane; ob < njobs * 8; ob += tpq) {  // warp-uniform trip count
+          for (int ob = tid - lane; ob < njobs * LG; ob += tpq) {  // warp-uniform trip count
             const int o = ob + lane;
-            const int e = o & 7;
-            const bool valid = (o >> 3) < njobs && e < NI;
-            const int job = min(o >> 3, njobs - 1);
+            const int e = o & (LG - 1);
+            const bool valid = (o >> LS) < njobs && e < NI;
+            const int job = min(o >> LS, njobs - 1);
             const int d = job % 3, tr = job / 3, t = fq(tr, fnrw), rl = tr - t * nrw, r = r0 + rl;
             const double* c = cf + t * CFT + r * 10;
             const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
@@ -308,7 +341,7 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
             L[0] = g0;
 #pragma unroll
             for (int j = 0; j < NJ - 1; ++j) {
-              const double up = __shfl_up_sync(0xffffffffu, L[j], 1, 8);  // G[e-1][j]
+              const double up = __shfl_up_sync(0xffffffffu, L[j], 1, LG);  // G[e-1][j]
               double v = D00 * L[j];
               if (j > 0) v = fma(j * B01, L[j > 0 ? j - 1 : 0], v);
               if (e > 0) v = fma(e * B00, up, v);

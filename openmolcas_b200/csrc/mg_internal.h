@@ -86,7 +86,7 @@ struct Handle {
   std::vector<double> sph[MG_MAX_L + 3];  // Cartesian->spherical per l (ncart x ncomp, col-major)
   // device memory
   DPair* d_pairs = nullptr;
-  double* d_prim = nullptr;   // SoA: [7][tot_np]: zeta, kappa, Px, Py, Pz, alpha, beta
+  double* d_prim = nullptr;   // SoA: [8][tot_np]: zeta, kappa, Px, Py, Pz, alpha, beta, 1/zeta
   int tot_np = 0;
   long long prim_kept = 0, prim_total = 0;  // primitive pairs after prescreening
   double* d_coef = nullptr;

@@ -3,6 +3,9 @@ the synthetic configurations through the batched ERI entry point (timing and
 profiling driver).
 
     python -m openmolcas_b200.sample_eri c2 20000 [repeats]
+
+The batched calls run inside an NVTX range named "eri" so that a profiler
+can select them (ncu --nvtx --nvtx-include "eri/").
 """
 import sys
 import time
@@ -29,9 +32,11 @@ def main(argv):
     ms = []
     for _ in range(reps):
         e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+        torch.cuda.nvtx.range_push("eri")
         e0.record()
         g.eri_quartets(sel, out)
         e1.record()
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         ms.append(e0.elapsed_time(e1))
     print(f"{cfg}: {len(sel)} of {len(q)} quartets, last {ms[-1]:.2f} ms, {len(sel) / ms[-1] * 1e3:.3e} quartets/s")
