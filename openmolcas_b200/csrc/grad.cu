@@ -50,21 +50,17 @@ static inline size_t ev2(size_t x) { return (x + 1) & ~(size_t)1; }
 // (the layout of grad_kernel, every region rounded to an even count)
 static size_t grad_group_smem(const DPair& P, const DPair& Q, int nijc, int nklc, int pab, int pcd, int rw) {
   const int la = P.la, lb = P.lb, lc = Q.la, ld = Q.lb;
-  const int NI = la + lb + 2, NJ = lc + ld + 2;
   const int NR = (la + lb + lc + ld + 3) / 2;
   const size_t ncart4 = (size_t)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
-  const size_t nsp4 = (size_t)ncomp(la) * ncomp(lb) * ncomp(lc) * ncomp(ld);
   const size_t n1d = (size_t)(la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-  const size_t scr = ((size_t)(NI | 1) * (lc + 2) * (ld + 1)) | 1;
   const size_t nij = nijc, nc = nij * nklc;
   const bool multi = nc > 1;
-  (void)nsp4;
   const size_t fixed = 8 + ev2(nij * P.np) + ev2((size_t)nklc * Q.np) + (multi ? ev2(nij * pcd * ncart4) : 0) +
                        ev2((ncart4 + 1) / 2);
   const size_t nt = (size_t)pab * pcd;
   const size_t w = std::min<size_t>(rw, NR);
   const size_t gs = ncart4 | 1, st = w * 12 * n1d + 2;  // padded strides of Gp and F
-  const size_t tile = ev2(nt * ((size_t)NR * 10 + 5)) + ev2(nt * gs) + nt * st + nt * 3 * w * scr;
+  const size_t tile = ev2(nt * ((size_t)NR * 10 + 5)) + ev2(nt * gs) + nt * st;
   return ev2(fixed + std::max(tile, (size_t)16 * 9));
 }
 

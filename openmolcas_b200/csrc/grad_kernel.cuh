@@ -87,10 +87,6 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
   const bool multi = nc > 1;
   const int npab = P.np, npcd = Q.np;
   const int n1d = (la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-  // per (quartet, root, direction) job: V[d][c][e] with row stride NIp; odd strides
-  // keep the lanes of a warp on distinct banks
-  constexpr int NIp = NI | 1;
-  const int scr = (NIp * (lc + 2) * (ld + 1)) | 1;
   const int PAB = a.PAB, PCD = a.PCD, RW = a.RW;
   const int NT = PAB * PCD;
   const int CFT = NR * 10 + 5;  // per-quartet coefficient record (odd stride)
@@ -106,7 +102,6 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
   double* cf = U0;                                    // NT * CFT
   double* Gp = cf + ev2(NT * CFT);                    // [t][abcd] primitive 2-PDM, row stride Gs
   double* F = Gp + ev2(NT * Gs);                      // [t][rl][dir][e1][4], quartet stride St
-  double* S = F + NT * St;                            // NT * 3 * RW * scr
   double* Gam = Gg;                                   // [il][abcd] (global scratch)
   double* Tmp = Gg + ev2(nc * ncart4);                // stage-0 temp (global scratch)
   if (tid < 3) {
@@ -312,16 +307,22 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
       for (int r0 = 0; r0 < NR; r0 += RW) {
         const int nrw = min(RW, NR - r0);
         const FDiv fnrw = fdiv(nrw);
-        // ---- (2a+2b) 2D recursion and ket 2D-level HRR (HRR2Db): one 4- or 8-lane group per
-        //      (quartet, root, direction) job; lane e holds the row G[e][0..NJ-1] in registers
-        //      and takes G[e-1][j] from its neighbour:
-        //        G[e][j+1] = D00 G[e][j] + j B01 G[e][j-1] + e B00 G[e-1][j],
-        //        V[e][c][0] = G[e][c],  V[e][c][d+1] = V[e][c+1][d] + CD V[e][c][d]
+        // ---- (2) one 4- or 8-lane group per (quartet, root, direction) job, all in registers:
+        //      2D recursion: lane e holds the row G[e][0..NJ-1] and takes G[e-1][j] from its
+        //        neighbour,  G[e][j+1] = D00 G[e][j] + j B01 G[e][j-1] + e B00 G[e-1][j];
+        //      ket 2D-level HRR (HRR2Db) in the lane:  V[e][c][0] = G[e][c],
+        //        V[e][c][d+1] = V[e][c+1][d] + CD V[e][c][d];
+        //      bra 2D-level HRR (HRR2Da) across the lanes of the group (a shift along e):
+        //        U(a,0) = V[a][c][d],  U(a,b+1) = U(a+1,b) + AB U(a,b);
+        //      derivative factors (Rys2Dg): F = U, dA = 2alpha U(a+1,b) - a U(a-1,b),
+        //        dB = 2beta U(a,b+1) - b U(a,b-1), dC = the same transfer of
+        //        W[a] = 2gamma V[a][c+1][d] - c V[a][c-1][d]
         {
           constexpr int LG = NI <= 4 ? 4 : 8;  // lanes per job (power of two >= NI)
           constexpr int LS = NI <= 4 ? 2 : 3;
           const int njobs = nt * nrw * 3;
           const int lane = tid & 31;
+          const int n1d4 = 4 * n1d;
           for (int ob = tid - lane; ob < njobs * LG; ob += tpq) {  // warp-uniform trip count
             const int o = ob + lane;
             const int e = o & (LG - 1);
@@ -347,69 +348,46 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
               if (e > 0) v = fma(e * B00, up, v);
               L[j + 1] = v;
             }
-            double* Vo = S + (size_t)job * scr + e;
-            const double cdv = hdr[3 + d];
+            const double cdv = hdr[3 + d], abv = hdr[d];
+            const double* ex = cf + t * CFT + NR * 10;
+            const double e2a = ex[0], e2b = ex[1], e2c = ex[2];
+            double2* Fo = reinterpret_cast<double2*>(F + (size_t)t * St + (size_t)(job - 3 * nrw * t) * n1d4);
+            const bool wr = valid && e <= la;
 #pragma unroll
-            for (int m = 0; m < NJ; ++m) {
+            for (int m = 0; m < NJ; ++m) {  // ket level: L[c] = V[e][c][m]
               if (m > ld) break;
               if (m > 0) {
 #pragma unroll
                 for (int cc = 0; cc + m < NJ; ++cc) L[cc] = fma(cdv, L[cc], L[cc + 1]);
               }
-              if (valid) {
 #pragma unroll
-                for (int cc = 0; cc + m < NJ; ++cc)
-                  if (cc <= lc + 1) Vo[NIp * (cc + (lc + 2) * m)] = L[cc];
-              }
-            }
-          }
-        }
-        gsync(g, tpq);
-        // ---- (2c) bra 2D-level HRR (HRR2Da) with the derivative factors (Rys2Dg), one thread
-        //      per (job, c, d) column in registers: U(a,0) = V[a][c][d],
-        //      U(a,b+1) = U(a+1,b) + AB U(a,b);  F = U,  dA = 2alpha U(a+1,b) - a U(a-1,b),
-        //      dB = 2beta U(a,b+1) - b U(a,b-1), dC = the same transfer applied to
-        //      W[a] = 2gamma V[a][c+1][d] - c V[a][c-1][d]
-        {
-          const int ncd1 = (lc + 1) * (ld + 1);
-          const FDiv fcd = fdiv(ncd1), fc1 = fdiv(lc + 1), f3rw = fdiv(3 * nrw);
-          for (int o = tid; o < nt * nrw * 3 * ncd1; o += tpq) {
-            const int job = fq(o, fcd), r = o - job * ncd1, dd = fq(r, fc1), cc = r - dd * (lc + 1);
-            const int d = job % 3, t = fq(job, f3rw);
-            const double* V = S + (size_t)job * scr + NIp * ((lc + 2) * dd + cc);
-            const double ab = hdr[d];
-            const double* ex = cf + t * CFT + NR * 10;
-            const double e2a = ex[0], e2b = ex[1], e2c = ex[2];
-            double Lp[NI], Lc[NI], W[NI];
+              for (int cc = 0; cc + m + 1 < NJ; ++cc) {
+                if (cc > lc) break;
+                double u = L[cc];
+                double w = e2c * L[cc + 1] - (cc > 0 ? cc * L[cc > 0 ? cc - 1 : 0] : 0.0);
+                double uprev = 0.0;
+                const int ebase = (la + 1) * (lb + 1) * (cc + (lc + 1) * m);
 #pragma unroll
-            for (int k = 0; k < NI; ++k) {
-              Lc[k] = V[k];
-              W[k] = e2c * V[NIp + k] - (cc ? cc * V[k - NIp] : 0.0);
-              Lp[k] = 0.0;
-            }
-            double2* Fo = reinterpret_cast<double2*>(F + (size_t)t * St) +
-                          2 * ((size_t)(job - 3 * nrw * t) * n1d + (la + 1) * (lb + 1) * (cc + (lc + 1) * dd));
-#pragma unroll
-            for (int b = 0; b < NI - 1; ++b) {
-              if (b > lb) break;
-#pragma unroll
-              for (int aa = 0; aa + b < NI - 1; ++aa) {
-                if (aa <= la) {
-                  double2 v01, v23;
-                  v01.x = Lc[aa];
-                  v01.y = e2a * Lc[aa + 1] - (aa > 0 ? aa * Lc[aa > 0 ? aa - 1 : 0] : 0.0);
-                  v23.x = e2b * fma(ab, Lc[aa], Lc[aa + 1]) - (b > 0 ? b * Lp[aa] : 0.0);
-                  v23.y = W[aa];
-                  Fo[2 * (aa + (la + 1) * b)] = v01;
-                  Fo[2 * (aa + (la + 1) * b) + 1] = v23;
+                for (int b = 0; b < NI - 1; ++b) {
+                  if (b > lb) break;
+                  const double un = __shfl_down_sync(0xffffffffu, u, 1, LG);  // U(e+1, b)
+                  const double ud = __shfl_up_sync(0xffffffffu, u, 1, LG);    // U(e-1, b)
+                  const double wn = __shfl_down_sync(0xffffffffu, w, 1, LG);
+                  const double unext = fma(abv, u, un);                       // U(e, b+1)
+                  if (wr) {
+                    double2 v01, v23;
+                    v01.x = u;
+                    v01.y = e2a * un - (e > 0 ? e * ud : 0.0);
+                    v23.x = e2b * unext - (b > 0 ? b * uprev : 0.0);
+                    v23.y = w;
+                    const int e1 = e + (la + 1) * b + ebase;
+                    Fo[2 * e1] = v01;
+                    Fo[2 * e1 + 1] = v23;
+                  }
+                  uprev = u;
+                  u = unext;
+                  w = fma(abv, w, wn);
                 }
-              }
-              // next transfer level in place: Lp <- Lc, Lc(a) <- Lc(a+1) + AB Lc(a), W likewise
-#pragma unroll
-              for (int k = 0; k + b + 1 < NI; ++k) {
-                Lp[k] = Lc[k];
-                Lc[k] = fma(ab, Lc[k], Lc[k + 1]);
-                W[k] = fma(ab, W[k], W[k + 1]);
               }
             }
           }
