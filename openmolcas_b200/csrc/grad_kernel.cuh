@@ -37,6 +37,79 @@ struct GradArgs {
 using GradFn = void (*)(GradArgs, RysArgs);
 GradFn grad_kernel_m1(int nab1, int ncd1);
 
+// Cartesian exponents of the components of one shell in C3 order (compile-time).
+template <int L>
+struct CartExp {
+  static constexpr int n = (L + 1) * (L + 2) / 2;
+  int e[n > 0 ? n : 1][3];
+  constexpr CartExp() : e() {
+    int k = 0;
+    for (int lx = L; lx >= 0; --lx)
+      for (int ly = L - lx; ly >= 0; --ly) {
+        e[k][0] = lx;
+        e[k][1] = ly;
+        e[k][2] = L - lx - ly;
+        ++k;
+      }
+  }
+};
+
+// Assg1 for one shell quartet class with la = LA, blocked over the Cartesian
+// components of centre A: a thread takes all NCA components that share one
+// (b, c, d) component and one primitive quartet, loads the LA + 1 interleaved
+// 2D records (I, dA, dB, dC) per direction once and reuses them across the NCA
+// components (component 0 is (LA, 0, 0), so the x records start LA before it).
+template <int LA>
+__device__ __forceinline__ void assg1_a_block(const double* __restrict__ F, const double* __restrict__ Gp,
+                                              const int* __restrict__ IX, int nt, int nrest, int St, int Gs, int n1d4,
+                                              int nrw, int tid, int tpq, double* acc) {
+  constexpr int NCA = (LA + 1) * (LA + 2) / 2;
+  constexpr CartExp<LA> ce{};
+  const FDiv fnt = fdiv(nt);
+  for (int w = tid; w < nt * nrest; w += tpq) {
+    const int rest = fq(w, fnt), t = w - rest * nt;
+    const int abcd0 = NCA * rest;
+    double gm[NCA];
+    bool any = false;
+#pragma unroll
+    for (int ca = 0; ca < NCA; ++ca) {
+      gm[ca] = Gp[t * Gs + abcd0 + ca];
+      any |= gm[ca] != 0.0;
+    }
+    if (!any) continue;
+    const int pk = IX[abcd0];
+    const int bx = 4 * ((pk & 255) - LA), by = n1d4 + 4 * ((pk >> 8) & 255), bz = 2 * n1d4 + 4 * (pk >> 16);
+    const double* Fb = F + (size_t)t * St;
+    for (int rl = 0; rl < nrw; ++rl, Fb += 3 * n1d4) {
+      double2 X01[LA + 1], X23[LA + 1], Y01[LA + 1], Y23[LA + 1], Z01[LA + 1], Z23[LA + 1];
+#pragma unroll
+      for (int k = 0; k <= LA; ++k) {
+        X01[k] = *reinterpret_cast<const double2*>(Fb + bx + 4 * k);
+        X23[k] = *reinterpret_cast<const double2*>(Fb + bx + 4 * k + 2);
+        Y01[k] = *reinterpret_cast<const double2*>(Fb + by + 4 * k);
+        Y23[k] = *reinterpret_cast<const double2*>(Fb + by + 4 * k + 2);
+        Z01[k] = *reinterpret_cast<const double2*>(Fb + bz + 4 * k);
+        Z23[k] = *reinterpret_cast<const double2*>(Fb + bz + 4 * k + 2);
+      }
+#pragma unroll
+      for (int ca = 0; ca < NCA; ++ca) {
+        const int ax = ce.e[ca][0], ay = ce.e[ca][1], az = ce.e[ca][2];
+        const double g = gm[ca];
+        const double gyz = g * Y01[ay].x * Z01[az].x, gxz = g * X01[ax].x * Z01[az].x, gxy = g * X01[ax].x * Y01[ay].x;
+        acc[0] = fma(gyz, X01[ax].y, acc[0]);
+        acc[1] = fma(gxz, Y01[ay].y, acc[1]);
+        acc[2] = fma(gxy, Z01[az].y, acc[2]);
+        acc[3] = fma(gyz, X23[ax].x, acc[3]);
+        acc[4] = fma(gxz, Y23[ay].x, acc[4]);
+        acc[5] = fma(gxy, Z23[az].x, acc[5]);
+        acc[6] = fma(gyz, X23[ax].y, acc[6]);
+        acc[7] = fma(gxz, Y23[ay].y, acc[7]);
+        acc[8] = fma(gxy, Z23[az].y, acc[8]);
+      }
+    }
+  }
+}
+
 // Persistent kernel: each group of tpq threads takes work items from a
 // counter until none are left.  The contracted Cartesian 2-PDM of an item
 // (Gam[il][abcd]) and the stage-0 temporaries live in the group's global
@@ -394,8 +467,15 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
         }
         gsync(g, tpq);
         // ---- (4) Assg1: sum over Cartesian components and roots; consecutive threads
-        //      take consecutive primitive quartets of one Cartesian quartet
-        {
+        //      take consecutive primitive quartets of one Cartesian quartet (blocked over
+        //      the components of centre A for la = 1, 2; over those of centre B when
+        //      la = 0, which puts B first in the component order with unit stride)
+        const int lblk = la > 0 ? la : lb;
+        if (lblk == 1) {
+          assg1_a_block<1>(F, Gp, IX, nt, ncart4 / 3, St, Gs, 4 * n1d, nrw, tid, tpq, acc);
+        } else if (lblk == 2) {
+          assg1_a_block<2>(F, Gp, IX, nt, ncart4 / 6, St, Gs, 4 * n1d, nrw, tid, tpq, acc);
+        } else {
           const FDiv fnt = fdiv(nt);
           const int n1d4 = 4 * n1d;
           for (int w = tid; w < nt * ncart4; w += tpq) {
