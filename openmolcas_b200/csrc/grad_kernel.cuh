@@ -380,7 +380,8 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
       for (int r0 = 0; r0 < NR; r0 += RW) {
         const int nrw = min(RW, NR - r0);
         const FDiv fnrw = fdiv(nrw);
-        // ---- (2) one 4- or 8-lane group per (quartet, root, direction) job, all in registers:
+        // ---- (2) one NI-lane segment of a warp per (quartet, root, direction) job (32/NI jobs
+        //      per warp), all in registers:
         //      2D recursion: lane e holds the row G[e][0..NJ-1] and takes G[e-1][j] from its
         //        neighbour,  G[e][j+1] = D00 G[e][j] + j B01 G[e][j-1] + e B00 G[e-1][j];
         //      ket 2D-level HRR (HRR2Db) in the lane:  V[e][c][0] = G[e][c],
@@ -391,16 +392,15 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
         //        dB = 2beta U(a,b+1) - b U(a,b-1), dC = the same transfer of
         //        W[a] = 2gamma V[a][c+1][d] - c V[a][c-1][d]
         {
-          constexpr int LG = NI <= 4 ? 4 : 8;  // lanes per job (power of two >= NI)
-          constexpr int LS = NI <= 4 ? 2 : 3;
+          constexpr int JPW = 32 / NI;  // jobs per warp
           const int njobs = nt * nrw * 3;
           const int lane = tid & 31;
+          const int seg = lane / NI, e = lane - seg * NI;  // seg >= JPW: spare lanes
+          const int lup = (lane + 31) & 31, ldn = (lane + 1) & 31;
           const int n1d4 = 4 * n1d;
-          for (int ob = tid - lane; ob < njobs * LG; ob += tpq) {  // warp-uniform trip count
-            const int o = ob + lane;
-            const int e = o & (LG - 1);
-            const bool valid = (o >> LS) < njobs && e < NI;
-            const int job = min(o >> LS, njobs - 1);
+          for (int jb = (tid >> 5) * JPW; jb < njobs; jb += (tpq >> 5) * JPW) {  // warp-uniform trip count
+            const bool valid = seg < JPW && jb + seg < njobs;
+            const int job = min(jb + seg, njobs - 1);
             const int d = job % 3, tr = job / 3, t = fq(tr, fnrw), rl = tr - t * nrw, r = r0 + rl;
             const double* c = cf + t * CFT + r * 10;
             const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
             L[0] = g0;
 #pragma unroll
             for (int j = 0; j < NJ - 1; ++j) {
-              const double up = __shfl_up_sync(0xffffffffu, L[j], 1, LG);  // G[e-1][j]
+              const double up = __shfl_sync(0xffffffffu, L[j], lup);  // G[e-1][j]
               double v = D00 * L[j];
               if (j > 0) v = fma(j * B01, L[j > 0 ? j - 1 : 0], v);
               if (e > 0) v = fma(e * B00, up, v);
@@ -443,9 +443,9 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
 #pragma unroll
                 for (int b = 0; b < NI - 1; ++b) {
                   if (b > lb) break;
-                  const double un = __shfl_down_sync(0xffffffffu, u, 1, LG);  // U(e+1, b)
-                  const double ud = __shfl_up_sync(0xffffffffu, u, 1, LG);    // U(e-1, b)
-                  const double wn = __shfl_down_sync(0xffffffffu, w, 1, LG);
+                  const double un = __shfl_sync(0xffffffffu, u, ldn);  // U(e+1, b)
+                  const double ud = __shfl_sync(0xffffffffu, u, lup);  // U(e-1, b)
+                  const double wn = __shfl_sync(0xffffffffu, w, ldn);
                   const double unext = fma(abv, u, un);                       // U(e, b+1)
                   if (wr) {
                     double2 v01, v23;
