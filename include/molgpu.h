@@ -143,6 +143,17 @@ int mg_drvg1(mg_handle* h, const double* d_D, double cutint, double* d_grad, voi
  * no reference counterpart).  Negative on error. */
 double mg_drvg1_flops(mg_handle* h, double cutint);
 
+/* ---------------------------------------------------------------------
+ * Rys roots and weights (replaces vRysRW, rys_util/vrysrw.F90:15, and the
+ * RysNN table evaluation, rys22.F90:36-47, at the unit-test level): for the n
+ * arguments T[] (host), x[i*nrys + k] = u^2 (the squared root, as vRysRW
+ * returns it) and w[i*nrys + k] the weight of root k of order nrys (1..9),
+ * evaluated on the device from the handle's table (asymptotic Hermite form
+ * above the table's TMax).  Synchronous.  Returns MG_ERR_ARG for nrys outside
+ * 1..9 or a negative T.
+ */
+int mg_rys_roots(mg_handle* h, int nrys, int64_t n, const double* T, double* x, double* w);
+
 /* Number of kernels of this library launched so far in this process (library
  * calls such as cuBLAS are not counted).  No reference counterpart. */
 long long mg_kernel_launches(void);

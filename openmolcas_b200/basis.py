@@ -97,6 +97,12 @@ class Molecule:
         cf = np.concatenate([s.coef.reshape(-1, order="F") for s in self.shells]).astype(np.float64)
         return xyz, l, npr, nco, at, ex, cf
 
+    def at(self, coords) -> "Molecule":
+        """Copy with every atom at the given coordinates (natom x 3, bohr)."""
+        coords = np.array(coords, dtype=np.float64).reshape(self.natom, 3)
+        shells = [dataclasses.replace(s, center=coords[s.atom].copy()) for s in self.shells]
+        return Molecule(self.name, coords, self.charges, shells, self.seed)
+
     def moved(self, atom: int, axis: int, delta: float) -> "Molecule":
         """Copy with one atom displaced (finite-difference checks)."""
         coords = self.coords.copy()

@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmolgpu.so")
 OBJ = os.path.join(HERE, "_build")
 SOURCES = ["basis_host.cu", "eri.cu", "eri_k_lo.cu", "eri_k_hi.cu", "cholesky.cu", "grad.cu", "grad_k1.cu", "jk.cu",
-           "capi.cu", "eri_noalloc.cu"]
+           "capi.cu", "eri_noalloc.cu", "rys_eval.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

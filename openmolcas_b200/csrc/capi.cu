@@ -370,6 +370,35 @@ int mg_cho_jk(mg_handle* H, const double* d_C, int r, double* d_J, double* d_K, 
 
 long long mg_kernel_launches(void) { return g_launches.load(); }
 
+int mg_rys_roots(mg_handle* H, int nrys, int64_t n, const double* T, double* x, double* w) {
+  if (!H || nrys < 1 || nrys > MG_MAX_RYS || n < 0 || (n && (!T || !x || !w))) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  for (int64_t i = 0; i < n; ++i)
+    if (!(T[i] >= 0.0)) {
+      h->err = "mg_rys_roots: negative or NaN argument";
+      return MG_ERR_ARG;
+    }
+  if (n == 0) return 0;
+  if (cudaSetDevice(h->device) != cudaSuccess) return MG_ERR_CUDA;
+  double* d = nullptr;
+  const size_t bytes = sizeof(double) * (size_t)n * (1 + 2 * nrys);
+  if (cudaMalloc(&d, bytes) != cudaSuccess) {
+    h->err = "mg_rys_roots: device allocation failed";
+    return MG_ERR_MEMORY;
+  }
+  double* dT = d;
+  double* dx = d + n;
+  double* dw = dx + n * nrys;
+  cudaMemcpy(dT, T, sizeof(double) * n, cudaMemcpyHostToDevice);
+  int rc = rys_eval(h, nrys, n, dT, dx, dw);
+  if (!rc && (cudaMemcpy(x, dx, sizeof(double) * n * nrys, cudaMemcpyDeviceToHost) != cudaSuccess ||
+              cudaMemcpy(w, dw, sizeof(double) * n * nrys, cudaMemcpyDeviceToHost) != cudaSuccess))
+    rc = MG_ERR_CUDA;
+  cudaFree(d);
+  if (rc) h->err = "mg_rys_roots: evaluation failed";
+  return rc;
+}
+
 double mg_drvg1_flops(mg_handle* H, double cutint) {
   if (!H) return -1;
   Handle* h = &H->h;

@@ -125,6 +125,7 @@ struct GradPlan {
   double cutint = -1;
 };
 int grad_build(Handle* h, double cutint, GradPlan& plan);
+int rys_eval(Handle* h, int nrys, int64_t n, const double* d_T, double* d_x, double* d_w);
 int grad_run(Handle* h, const GradPlan& plan, const double* d_D, double* d_grad, cudaStream_t st);
 void grad_free(GradPlan* p);
 double grad_plan_flops(const Handle* h, const GradPlan& plan);

@@ -56,6 +56,7 @@ def lib():
     L.mg_cho_diag.argtypes = [vp, C.c_void_p, C.c_void_p]
     L.mg_drvg1.argtypes = [vp, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
     L.mg_cho_jk.argtypes = [vp, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    L.mg_rys_roots.argtypes = [vp, C.c_int, C.c_int64, d, d, d]
     _lib = L
     return L
 
@@ -135,6 +136,14 @@ class MolGpu:
         """One shell quartet (Eval_IJKL), flat Fortran-order AOInt(nijkl, a, b, c, d)."""
         out, _ = self.eri_quartets(np.array([[i, j, k, l]], dtype=np.int32))
         return out
+
+    def rys_roots(self, nrys: int, T) -> tuple[np.ndarray, np.ndarray]:
+        """vRysRW on the device: (u^2, weights), each len(T) x nrys."""
+        T = np.ascontiguousarray(T, dtype=np.float64).reshape(-1)
+        x = np.empty((T.size, nrys))
+        w = np.empty((T.size, nrys))
+        self._check(self.L.mg_rys_roots(self.h, nrys, T.size, _p(T), _p(x), _p(w)), "mg_rys_roots")
+        return x, w
 
     def schwarz(self) -> np.ndarray:
         """Shell_MxSchwz: sqrt(max |(ab|ab)|) per shell pair (nshell x nshell)."""
