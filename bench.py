@@ -201,10 +201,13 @@ def eri_leg(torch, device, reps=2):
         ms.append(e0.elapsed_time(e1))
     launches = (mglib().mg_kernel_launches() - n0) // reps
     ms_mean = float(np.mean(ms))
+    prim_q, flops = g2.eri_work(sel)
     res = {"value": len(sel) / (ms_mean / 1e3), "unit": "quartets/s", "ms": ms_mean, "quartets": int(len(sel)),
            "screened_unique_quartets": int(len(q)), "integrals_gb": float(off[-1]) * 8 / 1e9,
            "workload": f"{ERI_CFG}: 40 atoms, {m2.nbf} bf, Schwarz {CUTINT}, seeded sample of {len(sel)} of "
                        f"{len(q)} unique quartets", "gpu_launches": int(launches), "dtype": "f64",
+           "primitive_quartets_per_s": prim_q / (ms_mean / 1e3), "algorithmic_flops": flops,
+           "achieved_tflops": flops / (ms_mean / 1e3) / 1e12,
            "sample_quartets": sel}
     del out
     torch.cuda.empty_cache()
@@ -389,6 +392,8 @@ def run_gpu(args, rank, world):
     roof["kernel"] = dom
     roof["traffic"] = None
     cpu = cpu_baseline(S)
+    eri["fp64_peak_tflops"] = fp64_peak
+    eri["frac_of_fp64_peak"] = (eri["achieved_tflops"] / fp64_peak) if fp64_peak else None
     eri_sel = eri.pop("sample_quartets")
     if rank == 0 and world == 1:
         eri["cpu_baseline"] = eri_cpu_baseline(eri_sel)

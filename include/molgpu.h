@@ -64,6 +64,12 @@ int mg_schwarz(mg_handle* h, double* tmax);
  * i fastest inside ijkl).  offsets (host int64[nq+1]) is filled by
  * mg_eri_quartets_size. */
 int mg_eri_quartets_size(mg_handle* h, const int32_t* quartets, int64_t nq, int64_t* offsets);
+
+/* Algorithmic work of mg_eri_quartets on the same quartet list: the number of
+ * primitive quartets after primitive-pair prescreening and the FP64 flop
+ * count of the kernel's stages (roofline accounting; no reference
+ * counterpart).  Host only. */
+int mg_eri_work(mg_handle* h, const int32_t* quartets, int64_t nq, double* prim_quartets, double* flops);
 int mg_eri_quartets(mg_handle* h, const int32_t* quartets, int64_t nq, const int64_t* offsets, double* d_out,
                     void* stream);
 

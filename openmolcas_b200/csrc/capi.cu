@@ -220,6 +220,40 @@ int mg_eri_quartets_size(mg_handle* H, const int32_t* q4, int64_t nq, int64_t* o
   return 0;
 }
 
+// Algorithmic work of mg_eri_quartets over a quartet list (FMA = 2 flops), the
+// kernel's own stages: per primitive quartet the roots (2 x 7 FMA per root and
+// weight + 30), the 2D recursion (3 directions x 4 NI NJ per root), [e0|f0]
+// (3 flops per root per (e, f)) and the bra half-transform (2 nij nef); per
+// bra-contracted block the ket half-transform (2 nij nkl nef per ket
+// primitive pair); per contracted quartet the HRR + spherical transforms.
+int mg_eri_work(mg_handle* H, const int32_t* q4, int64_t nq, double* prim_quartets, double* flops) {
+  if (!H || (!q4 && nq) || !prim_quartets || !flops) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  const int ns = h->sh.size();
+  double pq = 0.0, f = 0.0;
+  for (int64_t t = 0; t < nq; ++t) {
+    const int i = q4[4 * t], j = q4[4 * t + 1], k = q4[4 * t + 2], l = q4[4 * t + 3];
+    if (i < 0 || j < 0 || k < 0 || l < 0 || i >= ns || j >= ns || k >= ns || l >= ns || i < j || k < l) {
+      h->err = "mg_eri_work: shell indices out of range or non-canonical pair";
+      return MG_ERR_ARG;
+    }
+    const DPair& P = h->pairs[pair_id(i, j)];
+    const DPair& Q = h->pairs[pair_id(k, l)];
+    const int nab = P.la + P.lb, ncd = Q.la + Q.lb;
+    const int NR = (nab + ncd) / 2 + 1, NI = nab + 1, NJ = ncd + 1;
+    const double nef = (double)P.ne * Q.ne, nij = (double)P.nci * P.ncj, nkl = (double)Q.nci * Q.ncj;
+    const double npq = (double)P.np * Q.np;
+    const double per_prim = NR * 28.0 + 30.0 + 3.0 * NR * 4.0 * NI * NJ + 3.0 * NR * nef + 2.0 * nij * nef;
+    const double ket = 2.0 * nij * nkl * nef * Q.np;
+    const double hrr = 2.0 * nij * nkl * ((double)P.nsa * P.nsb * P.ne * Q.ne + (double)P.nsa * P.nsb * Q.nsa * Q.nsb * Q.ne);
+    pq += npq;
+    f += per_prim * npq + ket + hrr;
+  }
+  *prim_quartets = pq;
+  *flops = f;
+  return 0;
+}
+
 int mg_eri_quartets(mg_handle* H, const int32_t* q4, int64_t nq, const int64_t* offsets, double* d_out, void* stream) {
   if (!H || (!q4 && nq) || !offsets || (!d_out && nq)) return MG_ERR_ARG;
   Handle* h = &H->h;

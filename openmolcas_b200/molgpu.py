@@ -57,6 +57,7 @@ def lib():
     L.mg_drvg1.argtypes = [vp, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
     L.mg_cho_jk.argtypes = [vp, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     L.mg_rys_roots.argtypes = [vp, C.c_int, C.c_int64, d, d, d]
+    L.mg_eri_work.argtypes = [vp, i32, C.c_int64, d, d]
     _lib = L
     return L
 
@@ -136,6 +137,14 @@ class MolGpu:
         """One shell quartet (Eval_IJKL), flat Fortran-order AOInt(nijkl, a, b, c, d)."""
         out, _ = self.eri_quartets(np.array([[i, j, k, l]], dtype=np.int32))
         return out
+
+    def eri_work(self, quartets: np.ndarray) -> tuple[float, float]:
+        """(primitive quartets, algorithmic FP64 flops) of eri_quartets on this list."""
+        q = np.ascontiguousarray(quartets, dtype=np.int32).reshape(-1, 4)
+        pq, fl = C.c_double(), C.c_double()
+        self._check(self.L.mg_eri_work(self.h, _p(q, C.c_int32), q.shape[0], C.byref(pq), C.byref(fl)),
+                    "mg_eri_work")
+        return pq.value, fl.value
 
     def rys_roots(self, nrys: int, T) -> tuple[np.ndarray, np.ndarray]:
         """vRysRW on the device: (u^2, weights), each len(T) x nrys."""
