@@ -203,52 +203,61 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
     const double* Sc = tabs + kGTabSph + d_sph_off(lc);
     const double* Sb = tabs + kGTabSph + d_sph_off(lb);
     const double* Sa = tabs + kGTabSph + d_sph_off(la);
-    {  // d: [il][sa][sb][sc][sd] -> [il][sa][sb][sc][cd]   (Tmp -> Gam)
+    // one-index transforms, ping-ponging between the two scratch buffers; s and p
+    // shells are Cartesian already (identity), so their passes are skipped
+    double* cur = Tmp;
+    double* nxt = Gam;
+    if (ld >= 2) {  // d: [il][sa][sb][sc][sd] -> [il][sa][sb][sc][cd]
       const int inner = nc * nsa * nsb * nsc;
       for (int o = tid; o < inner * ncd; o += tpq) {
         const int in = o % inner, cd = o / inner;
         double s = 0;
-        for (int m = 0; m < nsd; ++m) s = fma(Sd[cd + ncd * m], Tmp[in + inner * m], s);
-        Gam[o] = s;
+        for (int m = 0; m < nsd; ++m) s = fma(Sd[cd + ncd * m], cur[in + inner * m], s);
+        nxt[o] = s;
       }
       gsync(g, tpq);
+      double* t = cur; cur = nxt; nxt = t;
     }
-    {  // c  (Gam -> Tmp)
+    if (lc >= 2) {  // c
       const int inner = nc * nsa * nsb;
       for (int o = tid; o < inner * ncc * ncd; o += tpq) {
         const int in = o % inner, r1 = o / inner, cc = r1 % ncc, cd = r1 / ncc;
         double s = 0;
-        for (int m = 0; m < nsc; ++m) s = fma(Sc[cc + ncc * m], Gam[in + inner * (m + nsc * cd)], s);
-        Tmp[o] = s;
+        for (int m = 0; m < nsc; ++m) s = fma(Sc[cc + ncc * m], cur[in + inner * (m + nsc * cd)], s);
+        nxt[o] = s;
       }
       gsync(g, tpq);
+      double* t = cur; cur = nxt; nxt = t;
     }
-    {  // b  (Tmp -> Gam)
+    if (lb >= 2) {  // b
       const int inner = nc * nsa;
       const int outer = ncc * ncd;
       for (int o = tid; o < inner * ncb * outer; o += tpq) {
         const int in = o % inner, r1 = o / inner, cb = r1 % ncb, ou = r1 / ncb;
         double s = 0;
-        for (int m = 0; m < nsb; ++m) s = fma(Sb[cb + ncb * m], Tmp[in + inner * (m + nsb * ou)], s);
-        Gam[o] = s;
+        for (int m = 0; m < nsb; ++m) s = fma(Sb[cb + ncb * m], cur[in + inner * (m + nsb * ou)], s);
+        nxt[o] = s;
       }
       gsync(g, tpq);
+      double* t = cur; cur = nxt; nxt = t;
     }
-    {  // a  (Gam -> Tmp -> Gam)
+    if (la >= 2) {  // a
       const int outer = ncb * ncc * ncd;
       for (int o = tid; o < nc * nca * outer; o += tpq) {
         const int il = o % nc, r1 = o / nc, ca = r1 % nca, ou = r1 / nca;
         double s = 0;
-        for (int m = 0; m < nsa; ++m) s = fma(Sa[ca + nca * m], Gam[il + nc * (m + nsa * ou)], s);
-        Tmp[o] = s;
+        for (int m = 0; m < nsa; ++m) s = fma(Sa[ca + nca * m], cur[il + nc * (m + nsa * ou)], s);
+        nxt[o] = s;
       }
       gsync(g, tpq);
-      for (int o = tid; o < nc * ncart4; o += tpq) {  // transpose to [il][abcd]
-        const int il = o / ncart4, abcd = o - il * ncart4;
-        Gam[o] = Tmp[il + nc * abcd];
-      }
-      gsync(g, tpq);
+      double* t = cur; cur = nxt; nxt = t;
     }
+    for (int o = tid; o < nc * ncart4; o += tpq) {  // transpose to [il][abcd]
+      const int il = o / ncart4, abcd = o - il * ncart4;
+      nxt[o] = cur[il + nc * abcd];
+    }
+    Gam = nxt;
+    gsync(g, tpq);
   }
   double acc[9];
 #pragma unroll
