@@ -195,8 +195,10 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
       const int ki = ij % P.nci, kj = ij / P.nci, kk = kl % Q.nci, kq = kl / Q.nci;
       const int pa = P.ao_a + sa * P.nci + ki, pb = P.ao_b + sb * P.ncj + kj;
       const int pc = Q.ao_a + sc * Q.nci + kk, pd = Q.ao_b + sd * Q.ncj + kq;
-      Tmp[o] = Dm[pa * nbf + pb] * Dm[pc * nbf + pd] -
-               0.25 * (Dm[pa * nbf + pc] * Dm[pb * nbf + pd] + Dm[pa * nbf + pd] * Dm[pb * nbf + pc]);
+      // D is symmetric: index it with the fastest-varying AO (pa, then pb) as the
+      // column so that neighbouring threads read neighbouring addresses
+      Tmp[o] = Dm[pb * nbf + pa] * Dm[pd * nbf + pc] -
+               0.25 * (Dm[pc * nbf + pa] * Dm[pd * nbf + pb] + Dm[pd * nbf + pa] * Dm[pc * nbf + pb]);
     }
     gsync(g, tpq);
     const double* Sd = tabs + kGTabSph + d_sph_off(ld);
