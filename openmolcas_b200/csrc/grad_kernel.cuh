@@ -348,10 +348,10 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
           e[0] = 2.0 * prim[5 * tot_np + ia];         // 2 alpha
           e[1] = 2.0 * prim[6 * tot_np + ia];         // 2 beta
           e[2] = 2.0 * prim[5 * tot_np + ic];         // 2 gamma
-          e[3] = Cab[pab0 + pa] * Ccd[pcd0 + pc];     // single-contraction coefficient
         }
       }
-      gsync(g, tpq);
+      // (no barrier: the primitive 2-PDM below reads neither the roots' records nor
+      // anything they overwrite, so both stages share one phase)
       // ---- (3) primitive 2-PDM (Tcrtnc): bra half-transform of Y (a thread makes 4
       //      consecutive pa of one (pc, abcd), each Y load feeds 4 FMAs), or the single
       //      contraction coefficient times the contracted 2-PDM
@@ -373,12 +373,12 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
               if (pa0 + 3 < npa) s3 = fma(ci[3], yv, s3);
             }
           } else {
-            const double gv = Gam[abcd];
-            const double* e3 = cf + (pa0 + npa * pc) * CFT + NR * 10 + 3;
-            s0 = e3[0] * gv;
-            if (pa0 + 1 < npa) s1 = e3[CFT] * gv;
-            if (pa0 + 2 < npa) s2 = e3[2 * CFT] * gv;
-            if (pa0 + 3 < npa) s3 = e3[3 * CFT] * gv;
+            const double gv = Gam[abcd] * Ccd[pcd0 + pc];
+            const double* ca = Cab + pab0 + pa0;
+            s0 = ca[0] * gv;
+            if (pa0 + 1 < npa) s1 = ca[1] * gv;
+            if (pa0 + 2 < npa) s2 = ca[2] * gv;
+            if (pa0 + 3 < npa) s3 = ca[3] * gv;
           }
           double* gp = Gp + (size_t)(pa0 + npa * pc) * Gs + abcd;
           gp[0] = s0;
