@@ -516,7 +516,9 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
             }
           }
         }
-        gsync(g, tpq);
+        // the next wave overwrites F; after the last wave the next tile (or chunk, or the
+        // final reduction) starts with its own barrier
+        if (r0 + RW < NR) gsync(g, tpq);
       }  // root waves
     }
   }
