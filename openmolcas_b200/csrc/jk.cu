@@ -7,13 +7,14 @@
 //   K_ab = sum_J sum_k X_J[a,k] X_J[b,k],  X_J = L_J C      (cho_lk_scf.F90:507-830)
 //
 // Mixed path: vectors stored FP32; per block of vectors the rs-packed L_J
-// are unpacked straight into split BF16 pairs (hi + lo, hi = bf16(x),
-// lo = bf16(x - hi)); both GEMMs run as 3 BF16 tensor-core products
-// (hi*hi + hi*lo + lo*hi) with FP32 accumulation.  The exchange product
-// K += X X^T is the hand-written tcgen05 kernel of tc_syrk.cuh (TMA-fed,
-// lower-triangle tiles, FP32 in tensor memory over one block's nb*r terms,
-// FP64 atomic accumulation), so accumulation error does not grow with the
-// number of vectors.  J uses FP32 loads with FP64 accumulation.
+// are unpacked into dense split BF16 squares (hi + lo, hi = bf16(x),
+// lo = bf16(x - hi)); both exchange GEMMs are hand-written tcgen05 kernels
+// with 3 BF16 products (hi*hi + hi*lo + lo*hi) into FP32 tensor memory, fed
+// by TMA: the half-transform X_J = L_J C (tc_xgemm.cuh) writes the split,
+// K-major X^T directly, and K += X X^T (tc_syrk.cuh: lower-triangle tiles,
+// FP32 over one block's nb*r terms, FP64 atomic accumulation) keeps the
+// accumulation error from growing with the number of vectors.  J uses FP32
+// loads with FP64 accumulation.
 //
 // FP64 path ("plain FP64 GPU path"): vectors in FP64, per block of vectors
 // the rs-packed L_J are unpacked to dense symmetric nbf x nbf matrices, the
@@ -31,6 +32,7 @@
 
 #include "mg_internal.h"
 #include "tc_syrk.cuh"
+#include "tc_xgemm.cuh"
 
 namespace mg {
 
@@ -192,29 +194,6 @@ __global__ void k_split_c(const double* __restrict__ C, int n, int r, int ld, __
   lo[o] = l;
 }
 
-// X^T split: XThi/XTlo[a][k] (row a < ldt, k < kpad, K index contiguous) from
-// X (column-major ld x kcols, FP32); zero outside X.  32 x 32 tiles through
-// shared memory so that both the read and the write are coalesced.
-__global__ void k_split_t(const float* __restrict__ X, int ld, int kcols, int ldt, int kpad,
-                          __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
-  __shared__ float tile[32][33];
-  const int k0 = blockIdx.x * 32, a0 = blockIdx.y * 32;
-  for (int i = 0; i < 32; i += 8) {
-    const int a = a0 + threadIdx.x, k = k0 + threadIdx.y + i;
-    tile[threadIdx.y + i][threadIdx.x] = (a < ld && k < kcols) ? X[a + (size_t)ld * k] : 0.0f;
-  }
-  __syncthreads();
-  for (int i = 0; i < 32; i += 8) {
-    const int k = k0 + threadIdx.x, a = a0 + threadIdx.y + i;
-    if (a < ldt && k < kpad) {
-      __nv_bfloat16 h, l;
-      split_bf16(tile[threadIdx.x][threadIdx.y + i], h, l);
-      hi[(size_t)a * kpad + k] = h;
-      lo[(size_t)a * kpad + k] = l;
-    }
-  }
-}
-
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // dependency on the driver library).
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -230,13 +209,13 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// 2D BF16 tensor map over rows x kpad (K contiguous), 64 x 128 boxes, 128-byte swizzle.
-static bool make_operand_map(CUtensorMap* m, const __nv_bfloat16* base, int rows, int kpad) {
+// 2D BF16 tensor map over rows x kpad (K contiguous), 64 x box_rows boxes, 128-byte swizzle.
+static bool make_operand_map(CUtensorMap* m, const __nv_bfloat16* base, int rows, int kpad, int box_rows = kTcTile) {
   auto enc = tensor_map_encoder();
-  if (!enc || ((uintptr_t)base & 15) || (kpad * 2) % 16) return false;
+  if (!enc || ((uintptr_t)base & 15) || (kpad * 2) % 16 || box_rows < 1 || box_rows > 256) return false;
   cuuint64_t gdim[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
   cuuint64_t gstr[1] = {(cuuint64_t)kpad * 2};
-  cuuint32_t box[2] = {(cuuint32_t)kTcBK, (cuuint32_t)kTcTile}, es[2] = {1, 1};
+  cuuint32_t box[2] = {(cuuint32_t)kTcBK, (cuuint32_t)box_rows}, es[2] = {1, 1};
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
@@ -278,7 +257,8 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   const int64_t nrs = cho_nrs(c);
   const int M = cho_nvec(c);
   const int n = h->nbf;
-  const int ld = (n + 63) / 64 * 64;  // padded leading dimension for the tensor-core GEMMs
+  // rows of the squares and of X^T padded to the 128-row tensor-core tile (padding zero)
+  const int ld = (n + 127) / 128 * 128;
   if (!cho_vec_ptr32(c, 0, 1)) {
     int rc = cho_make_fp32(c, st);
     if (rc) { h->err = "FP32 vector copy failed"; return rc; }
@@ -287,19 +267,18 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   cublasSetStream(cb, st);
   const int* d_ra = cho_rs_a_dev(c);
   const int* d_rb = cho_rs_b_dev(c);
-  const size_t nn = (size_t)n * n, ll = (size_t)ld * ld, lbr = (size_t)ld * block * r;
-  // exchange GEMM on the tensor cores: X^T rows padded to the 128-row tile, K range split so
-  // that the lower-triangle tiles x splits cover the SMs
-  const int ldt = (n + 127) / 128 * 128;
-  const int ntile = (ldt / kTcTile) * (ldt / kTcTile + 1) / 2;
+  const size_t nn = (size_t)n * n, ll = (size_t)ld * ld;
+  // exchange product: K range split so that the lower-triangle tiles x splits cover the SMs
+  const int ntile = (ld / kTcTile) * (ld / kTcTile + 1) / 2;
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
   const int nsplit = std::max(1, std::min(8, (nsm + ntile - 1) / ntile));
   const int kq = kTcBK * nsplit;
   const int kpad = (block * r + kq - 1) / kq * kq;
-  const size_t xt = (size_t)ldt * kpad;
+  const size_t xt = (size_t)ld * kpad;
+  const int bbox = r <= kXgMaxN ? (r + 15) / 16 * 16 : kXgMaxN;  // rows of a C box
   size_t need = 8 * ((size_t)2 * nrs + block + nn) + 2 * (2 * (size_t)ld * r) + 2 * (2 * (size_t)block * ll) +
-                4 * lbr + 2 * (2 * xt) + 4 * nn + 16 * 256;
+                2 * (2 * xt) + 4 * nn + 16 * 256;
   char* ws = (char*)ws_get(h, need, st);
   if (!ws) { h->err = "jk workspace allocation failed"; return MG_ERR_MEMORY; }
   auto take = [&](size_t bytes) { char* p = ws; ws += (bytes + 255) & ~(size_t)255; return (void*)p; };
@@ -311,22 +290,24 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   __nv_bfloat16* Clo = (__nv_bfloat16*)take(2 * (size_t)ld * r);
   __nv_bfloat16* Lhi = (__nv_bfloat16*)take(2 * (size_t)block * ll);
   __nv_bfloat16* Llo = (__nv_bfloat16*)take(2 * (size_t)block * ll);
-  float* X = (float*)take(4 * lbr);
   __nv_bfloat16* XThi = (__nv_bfloat16*)take(2 * xt);
   __nv_bfloat16* XTlo = (__nv_bfloat16*)take(2 * xt);
   int* d_err = (int*)take(sizeof(int));
   int* inv = (int*)take(4 * nn);
-  CUtensorMap map_hi, map_lo;
-  if (!make_operand_map(&map_hi, XThi, ldt, kpad) || !make_operand_map(&map_lo, XTlo, ldt, kpad)) {
-    h->err = "tensor map for the exchange GEMM could not be encoded";
+  CUtensorMap map_hi, map_lo, map_lhi, map_llo, map_chi, map_clo;
+  if (!make_operand_map(&map_hi, XThi, ld, kpad) || !make_operand_map(&map_lo, XTlo, ld, kpad) ||
+      !make_operand_map(&map_lhi, Lhi, block * ld, ld) || !make_operand_map(&map_llo, Llo, block * ld, ld) ||
+      !make_operand_map(&map_chi, Chi, r, ld, bbox) || !make_operand_map(&map_clo, Clo, r, ld, bbox)) {
+    h->err = "tensor maps for the exchange GEMMs could not be encoded";
     return MG_ERR_CUDA;
   }
   static std::once_flag smem_once;
-  std::call_once(smem_once,
-                 [] { cudaFuncSetAttribute(tc_syrk3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem); });
+  std::call_once(smem_once, [] {
+    cudaFuncSetAttribute(tc_syrk3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    cudaFuncSetAttribute(tc_xgemm3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kXgSmem);
+  });
   cudaMemsetAsync(d_err, 0, sizeof(int), st);
   const double one = 1.0, zero = 0.0;
-  const float onef = 1.0f, zerof = 0.0f;
   cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, r, &one, d_C, n, d_C, n, &zero, D, n);
   k_pack_density<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, D, n, dw);
   g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -334,6 +315,8 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   g_launches.fetch_add(1, std::memory_order_relaxed);
   cudaMemsetAsync(jrs, 0, 8 * nrs, st);
   cudaMemsetAsync(d_K, 0, 8 * nn, st);
+  cudaMemsetAsync(XThi, 0, 2 * xt, st);  // columns beyond nb*r stay zero
+  cudaMemsetAsync(XTlo, 0, 2 * xt, st);
   cudaMemsetAsync(inv, 0xFF, 4 * nn, st);
   k_rs_inverse<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, n, inv);
   g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -348,19 +331,19 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
     g_launches.fetch_add(1, std::memory_order_relaxed);
     k_jacc<<<nb256(nrs), 256, 0, st>>>(Lb, nrs, nb, V, jrs);
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    // Exchange: X_J = L_J C  (3 split products, FP32 accumulation)
+    // Exchange: split squares of the block, X_J = L_J C written as split X^T (tcgen05),
+    // then K += X X^T (tcgen05; 3 products into one FP32 accumulator per tile, FP64
+    // atomic add into K).  A short last block leaves stale X^T columns of the previous
+    // block beyond nb*r: clear them first.
     k_unpack_dense_split<<<nb256((int64_t)nb * ld * (ld / 2)), 256, 0, st>>>(
         inv, n, nrs, Lb, nb, ld, (__nv_bfloat162*)Lhi, (__nv_bfloat162*)Llo);
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    const __nv_bfloat16* As[3] = {Lhi, Lhi, Llo};
-    const __nv_bfloat16* Bs[3] = {Chi, Clo, Chi};
-    for (int q = 0; q < 3; ++q)
-      cublasGemmStridedBatchedEx(cb, CUBLAS_OP_N, CUBLAS_OP_N, ld, r, ld, &onef, As[q], CUDA_R_16BF, ld, (long long)ll,
-                                 Bs[q], CUDA_R_16BF, ld, 0, q == 0 ? &zerof : &onef, X, CUDA_R_32F, ld,
-                                 (long long)ld * r, nb, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
-    // K += X X^T over this block: split-BF16 X^T (K-major), then the tcgen05 kernel
-    // (3 products into one FP32 accumulator per tile, FP64 atomic add into K)
-    k_split_t<<<dim3(kpad / 32, ldt / 32), dim3(32, 8), 0, st>>>(X, ld, nb * r, ldt, kpad, XThi, XTlo);
+    if (nb < block && J0 > 0) {
+      cudaMemsetAsync(XThi, 0, 2 * xt, st);
+      cudaMemsetAsync(XTlo, 0, 2 * xt, st);
+    }
+    tc_xgemm3_kernel<<<dim3(ld / kTcTile, nb, (r + kXgMaxN - 1) / kXgMaxN), 128, kXgSmem, st>>>(
+        map_lhi, map_llo, map_chi, map_clo, ld, r, bbox, kpad, XThi, XTlo, d_err);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     tc_syrk3_kernel<<<dim3(ntile, nsplit), 128, kTcSmem, st>>>(map_hi, map_lo, n, kpad, d_K, d_err);
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -374,7 +357,7 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return MG_ERR_CUDA;
   if (herr) {
-    h->err = "exchange GEMM: a pipeline wait ran out (result incomplete)";
+    h->err = "exchange GEMMs: a pipeline wait ran out (result incomplete)";
     return MG_ERR_CUDA;
   }
   return 0;
