@@ -65,3 +65,15 @@ def test_jk_mixed_vs_fp64(setup):
     assert relJ < 1e-6
     assert relK < 1e-4
     assert abs(Em - E) < 1e-5 * abs(E)
+
+
+@pytest.mark.parametrize("rank", [1, 17, 300])
+def test_jk_mixed_density_ranks(setup, rank):
+    """Mixed path at density ranks that exercise a single narrow tensor-core N
+    tile, an odd width and two N tiles (rank > 256), against the FP64 path."""
+    mol, g, o, ref, _ = setup
+    C = torch.from_numpy(B.density_factor(g.nbf, rank, 7))
+    J, K = (x.cpu().numpy() for x in g.cho_jk(C, precision=MolGpu.PREC_FP64))
+    Jm, Km = (x.cpu().numpy() for x in g.cho_jk(C, precision=MolGpu.PREC_MIXED))
+    assert np.abs(Jm - J).max() < 1e-6 * np.abs(J).max()
+    assert np.abs(Km - K).max() < 1e-4 * np.abs(K).max()
