@@ -9,8 +9,9 @@
 //   1b  8-lane group per (quartet, root, direction): 2D recursion (vRys2D
 //       vrys2d.F90), lane e holds row I[e][0..NCD] in registers and takes
 //       I[e-1][f] from its neighbour; weight * prefactor folded into z
-//   2a  thread per (quartet, e, f): [e0|f0] = sum_r Ix Iy Iz  (RysEF),
-//       consecutive lanes on consecutive primitive quartets
+//   2a  thread per (quartet, f, Cartesian shell of the bra range):
+//       [e0|f0] = sum_r Ix Iy Iz  (RysEF), each shell's rows loaded once per
+//       root; consecutive lanes on consecutive primitive quartets
 //   2b  half-transforms with the general-contraction coefficients (Cntrct)
 // then HRR + real-spherical transform with the per-pair matrices
 // (HrrMtrx/TnsCtl, hrrmtrx.F90, tnsctl.F90) and the store in the layout of
@@ -42,6 +43,37 @@ struct EriArgs {
 using EriFn = void (*)(EriArgs, RysArgs);
 EriFn eri_kernel_pick(int nab, int ncd);
 constexpr int kEriThreads = 512;
+
+// [e0|f0] of one Cartesian shell L of the bra range for one primitive quartet
+// and one ket component f: the L + 1 values of each direction's row are loaded
+// once per root and reused across the NCL components of the shell.
+// Ib: the quartet's 2D integrals [dir][root][f][e]; fxo/fyo/fzo: f * NI offsets.
+template <int L, int NR, int RS, int DS>
+__device__ __forceinline__ void ef_shell(const double* __restrict__ Ib, int fxo, int fyo, int fzo,
+                                         double* __restrict__ out) {
+  constexpr int NCL = (L + 1) * (L + 2) / 2;
+  constexpr CartExp<L> ce{};
+  double acc[NCL];
+#pragma unroll
+  for (int c = 0; c < NCL; ++c) acc[c] = 0.0;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const double* px = Ib + r * RS + fxo;
+    const double* py = Ib + DS + r * RS + fyo;
+    const double* pz = Ib + 2 * DS + r * RS + fzo;
+    double X[L + 1], Y[L + 1], Z[L + 1];
+#pragma unroll
+    for (int k = 0; k <= L; ++k) {
+      X[k] = px[k];
+      Y[k] = py[k];
+      Z[k] = pz[k];
+    }
+#pragma unroll
+    for (int c = 0; c < NCL; ++c) acc[c] = fma(X[ce.e[c][0]] * Y[ce.e[c][1]], Z[ce.e[c][2]], acc[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < NCL; ++c) out[c] = acc[c];
+}
 
 // Per-group shared layout (doubles, every region even):
 //   hdr[2] | acc | Cab | Ccd | Et, Ft (ints) | union{ HRR temp | X | tile: cf | I | E }
@@ -132,8 +164,8 @@ __global__ void __launch_bounds__(kEriThreads, 1) eri_kernel(const EriArgs a, co
           const double U2 = x * zei;
           double* c = cf + t * CFS + r * 10;
           c[0] = 0.5 * U2;
-          c[1] = 0.5 * (1.0 - U2 * eta) / zeta;
-          c[2] = 0.5 * (1.0 - U2 * zeta) / eta;
+          c[1] = 0.5 * (1.0 - U2 * eta) * prim[7 * tot_np + ia];   // 1/zeta from the table
+          c[2] = 0.5 * (1.0 - U2 * zeta) * prim[7 * tot_np + ic];
           c[3] = px - Ap0 - eta * U2 * dx;
           c[4] = py - Ap1 - eta * U2 * dy;
           c[5] = pz - Ap2 - eta * U2 * dz;
@@ -178,20 +210,28 @@ __global__ void __launch_bounds__(kEriThreads, 1) eri_kernel(const EriArgs a, co
             }
           }
           gsync(g, tpq);
-          // ---- 2a: [e0|f0] = sum_r Ix Iy Iz; consecutive lanes on consecutive quartets
+          // ---- 2a: [e0|f0] = sum_r Ix Iy Iz, one thread per (quartet, f, bra shell L);
+          //      consecutive lanes on consecutive quartets
           {
-            const FDiv fnt = fdiv(nt), fne = fdiv(ne);
-            for (int w = tid; w < nt * nef; w += tpq) {
-              const int ef = fq(w, fnt), t = w - ef * nt;
-              const int jf = fq(ef, fne), ie = ef - jf * ne;
-              const int pk = Et[ie] + Ft[jf];
-              const double* gx = I + (size_t)t * GST + (pk & 255);
-              const double* gy = I + (size_t)t * GST + DS + ((pk >> 8) & 255);
-              const double* gz = I + (size_t)t * GST + 2 * DS + (pk >> 16);
-              double s = 0.0;
-#pragma unroll
-              for (int r = 0; r < NR; ++r) s = fma(gx[r * RS] * gy[r * RS], gz[r * RS], s);
-              E[(size_t)t * Est + ef] = s;
+            const int emin = P.emin, nsh = NAB - emin + 1;
+            const int c0 = d_ccum(emin);
+            const FDiv fnt = fdiv(nt), fnf = fdiv(nf);
+            for (int w = tid; w < nt * nf * nsh; w += tpq) {
+              const int u = fq(w, fnt), t = w - u * nt;
+              const int s = fq(u, fnf), jf = u - s * nf;
+              const int L = emin + s;
+              const int pf = Ft[jf];
+              const double* Ib = I + (size_t)t * GST;
+              double* out = E + (size_t)t * Est + (size_t)ne * jf + (d_ccum(L) - c0);
+              const int fxo = pf & 255, fyo = (pf >> 8) & 255, fzo = pf >> 16;
+              switch (L) {
+#define MG_EF_CASE(LL) \
+  case LL:             \
+    if (LL <= NAB) ef_shell<(LL <= NAB ? LL : 0), NR, RS, DS>(Ib, fxo, fyo, fzo, out); \
+    break;
+                MG_EF_CASE(0) MG_EF_CASE(1) MG_EF_CASE(2) MG_EF_CASE(3) MG_EF_CASE(4) MG_EF_CASE(5) MG_EF_CASE(6)
+#undef MG_EF_CASE
+              }
             }
           }
         } else {

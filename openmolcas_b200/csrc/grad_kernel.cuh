@@ -37,23 +37,6 @@ struct GradArgs {
 using GradFn = void (*)(GradArgs, RysArgs);
 GradFn grad_kernel_m1(int nab1, int ncd1);
 
-// Cartesian exponents of the components of one shell in C3 order (compile-time).
-template <int L>
-struct CartExp {
-  static constexpr int n = (L + 1) * (L + 2) / 2;
-  int e[n > 0 ? n : 1][3];
-  constexpr CartExp() : e() {
-    int k = 0;
-    for (int lx = L; lx >= 0; --lx)
-      for (int ly = L - lx; ly >= 0; --ly) {
-        e[k][0] = lx;
-        e[k][1] = ly;
-        e[k][2] = L - lx - ly;
-        ++k;
-      }
-  }
-};
-
 // Assg1 for one shell quartet class with la = LA, blocked over the Cartesian
 // components of centre A: a thread takes all NCA components that share one
 // (b, c, d) component and one primitive quartet, loads the LA + 1 interleaved

@@ -93,4 +93,21 @@ __device__ __forceinline__ void rys_all(const RysArgs& ra, double T, double* x, 
   }
 }
 
+// Cartesian exponents of the components of one shell in C3 order (compile-time).
+template <int L>
+struct CartExp {
+  static constexpr int n = (L + 1) * (L + 2) / 2;
+  int e[n > 0 ? n : 1][3];
+  constexpr CartExp() : e() {
+    int k = 0;
+    for (int lx = L; lx >= 0; --lx)
+      for (int ly = L - lx; ly >= 0; --ly) {
+        e[k][0] = lx;
+        e[k][1] = ly;
+        e[k][2] = L - lx - ly;
+        ++k;
+      }
+  }
+};
+
 }  // namespace mg
