@@ -239,30 +239,56 @@ __global__ void __launch_bounds__(kEriThreads, 1) eri_kernel(const EriArgs a, co
           for (int t = tid; t < nt; t += tpq) E[(size_t)t * Est] = cf[t * CFS + 9];
         }
         gsync(g, tpq);
-        // ---- 2b1: bra half-transform  X[ij][pc][ef] += sum_pa Cab[ij][pa] E[pa,pc][ef]
+        // ---- 2b1: bra half-transform  X[ij][pc][ef] += sum_pa Cab[ij][pa] E[pa,pc][ef];
+        //      a thread makes 4 consecutive ij of one (pc, ef), each E load feeds 4 FMAs
         {
+          const int nij4 = (nij + 3) >> 2;
           const FDiv fnef = fdiv(nef), fnpc = fdiv(npc);
-          for (int o = tid; o < nij * npc * nef; o += tpq) {
-            const int r1 = fq(o, fnef), ef = o - r1 * nef, ij = fq(r1, fnpc), pc = r1 - ij * npc;
-            const double* ca = Cab + ij * npab + pab0;
+          for (int o = tid; o < nij4 * npc * nef; o += tpq) {
+            const int r1 = fq(o, fnef), ef = o - r1 * nef, q = fq(r1, fnpc), pc = r1 - q * npc;
+            const int ij0 = 4 * q;
+            const double* ca = Cab + ij0 * npab + pab0;
             const double* e = E + (size_t)pc * npa * Est + ef;
-            double s = 0.0;
-            for (int pa = 0; pa < npa; ++pa) s = fma(ca[pa], e[(size_t)pa * Est], s);
-            X[ef + nef * (pc + PCD * ij)] += s;
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            for (int pa = 0; pa < npa; ++pa) {
+              const double ev = e[(size_t)pa * Est];
+              s0 = fma(ca[pa], ev, s0);
+              if (ij0 + 1 < nij) s1 = fma(ca[npab + pa], ev, s1);
+              if (ij0 + 2 < nij) s2 = fma(ca[2 * npab + pa], ev, s2);
+              if (ij0 + 3 < nij) s3 = fma(ca[3 * npab + pa], ev, s3);
+            }
+            double* x = X + ef + nef * (pc + PCD * ij0);
+            x[0] += s0;
+            if (ij0 + 1 < nij) x[nef * PCD] += s1;
+            if (ij0 + 2 < nij) x[2 * nef * PCD] += s2;
+            if (ij0 + 3 < nij) x[3 * nef * PCD] += s3;
           }
         }
       }
       gsync(g, tpq);
-      // ---- 2b2: ket half-transform  acc[kl][ij][ef] += sum_pc Ccd[kl][pc] X[ij][pc][ef]
+      // ---- 2b2: ket half-transform  acc[kl][ij][ef] += sum_pc Ccd[kl][pc] X[ij][pc][ef];
+      //      a thread makes 4 consecutive kl of one (ij, ef), each X load feeds 4 FMAs
       {
+        const int nkl4 = (nklc + 3) >> 2;
         const FDiv fnef = fdiv(nef), fnij = fdiv(nij);
-        for (int o = tid; o < nacc; o += tpq) {
-          const int r1 = fq(o, fnef), ef = o - r1 * nef, klc = fq(r1, fnij), ij = r1 - klc * nij;
-          const double* cc = Ccd + klc * npcd + pcd0;
+        for (int o = tid; o < nkl4 * nij * nef; o += tpq) {
+          const int r1 = fq(o, fnef), ef = o - r1 * nef, q = fq(r1, fnij), ij = r1 - q * nij;
+          const int kl0 = 4 * q;
+          const double* cc = Ccd + kl0 * npcd + pcd0;
           const double* xx = X + ef + nef * PCD * ij;
-          double s = 0.0;
-          for (int pc = 0; pc < npc; ++pc) s = fma(cc[pc], xx[nef * pc], s);
-          acc[o] += s;
+          double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+          for (int pc = 0; pc < npc; ++pc) {
+            const double xv = xx[nef * pc];
+            s0 = fma(cc[pc], xv, s0);
+            if (kl0 + 1 < nklc) s1 = fma(cc[npcd + pc], xv, s1);
+            if (kl0 + 2 < nklc) s2 = fma(cc[2 * npcd + pc], xv, s2);
+            if (kl0 + 3 < nklc) s3 = fma(cc[3 * npcd + pc], xv, s3);
+          }
+          double* ac = acc + (size_t)(kl0 * nij + ij) * nef + ef;
+          ac[0] += s0;
+          if (kl0 + 1 < nklc) ac[(size_t)nij * nef] += s1;
+          if (kl0 + 2 < nklc) ac[(size_t)2 * nij * nef] += s2;
+          if (kl0 + 3 < nklc) ac[(size_t)3 * nij * nef] += s3;
         }
       }
     }
