@@ -107,12 +107,31 @@ int run_eri_items(Handle* h, const std::vector<EriItem>& items, const std::vecto
   if (!d_items) { h->err = "workspace allocation failed"; return MG_ERR_MEMORY; }
   cudaMemcpyAsync(d_items, items.data(), sizeof(EriItem) * items.size(), cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(h->d_eri_counters, 0, sizeof(int) * 64, st);
+  // The class kernels are independent (own counter, own output blocks): spread them over
+  // the handle's side streams so that the tail of one class overlaps the next class.
+  if (!h->eri_streams[0]) {
+    for (int k = 0; k < MG_ERI_STREAMS; ++k) {
+      if (cudaStreamCreateWithFlags(&h->eri_streams[k], cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&h->eri_events[k], cudaEventDisableTiming) != cudaSuccess) {
+        h->err = "ERI side streams could not be created";
+        return MG_ERR_CUDA;
+      }
+    }
+    cudaEventCreateWithFlags(&h->eri_fork, cudaEventDisableTiming);
+  }
+  cudaEventRecord(h->eri_fork, st);
+  for (int k = 0; k < MG_ERI_STREAMS; ++k) cudaStreamWaitEvent(h->eri_streams[k], h->eri_fork, 0);
   for (size_t ci = 0; ci < classes.size(); ++ci) {
     const EriClass& c = classes[ci];
-    if (eri_launch_class(h, d_items + c.begin, c.count, c.nab, c.ncd, c.plan, d_out, h->d_eri_counters + ci, st)) {
+    if (eri_launch_class(h, d_items + c.begin, c.count, c.nab, c.ncd, c.plan, d_out, h->d_eri_counters + ci,
+                         h->eri_streams[ci % MG_ERI_STREAMS])) {
       h->err = std::string("ERI kernel launch failed: ") + cudaGetErrorString(cudaGetLastError());
       return MG_ERR_CUDA;
     }
+  }
+  for (int k = 0; k < MG_ERI_STREAMS; ++k) {
+    cudaEventRecord(h->eri_events[k], h->eri_streams[k]);
+    cudaStreamWaitEvent(st, h->eri_events[k], 0);
   }
   return 0;
 }
@@ -155,6 +174,11 @@ int mg_destroy(mg_handle* H) {
   free_basis(h);
   cudaFree(h->d_rys);
   cudaFree(h->d_eri_counters);
+  for (int k = 0; k < MG_ERI_STREAMS; ++k) {
+    if (h->eri_streams[k]) cudaStreamDestroy(h->eri_streams[k]);
+    if (h->eri_events[k]) cudaEventDestroy(h->eri_events[k]);
+  }
+  if (h->eri_fork) cudaEventDestroy(h->eri_fork);
   if (h->ws.ptr) cudaFree(h->ws.ptr);
   delete H;
   return 0;

@@ -10,6 +10,7 @@
 #include "../../include/molgpu.h"
 
 #define MG_MAX_RYS 9
+#define MG_ERI_STREAMS 4
 #define MG_MAX_L 3
 
 namespace mg {
@@ -101,6 +102,9 @@ struct Handle {
   struct ChoState* cho = nullptr;  // Cholesky vectors of the current basis
   struct GradPlan* grad = nullptr; // gradient work list (per Schwarz threshold)
   int* d_eri_counters = nullptr;   // one work counter per ERI class launch (64)
+  cudaStream_t eri_streams[MG_ERI_STREAMS] = {};  // side streams of the ERI class launches
+  cudaEvent_t eri_events[MG_ERI_STREAMS] = {};
+  cudaEvent_t eri_fork = nullptr;
 };
 
 struct GradItem {
