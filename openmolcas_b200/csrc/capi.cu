@@ -109,18 +109,8 @@ int run_eri_items(Handle* h, const std::vector<EriItem>& items, const std::vecto
   cudaMemsetAsync(h->d_eri_counters, 0, sizeof(int) * 64, st);
   // The class kernels are independent (own counter, own output blocks): spread them over
   // the handle's side streams so that the tail of one class overlaps the next class.
-  if (!h->eri_streams[0]) {
-    for (int k = 0; k < MG_ERI_STREAMS; ++k) {
-      if (cudaStreamCreateWithFlags(&h->eri_streams[k], cudaStreamNonBlocking) != cudaSuccess ||
-          cudaEventCreateWithFlags(&h->eri_events[k], cudaEventDisableTiming) != cudaSuccess) {
-        h->err = "ERI side streams could not be created";
-        return MG_ERR_CUDA;
-      }
-    }
-    cudaEventCreateWithFlags(&h->eri_fork, cudaEventDisableTiming);
-  }
-  cudaEventRecord(h->eri_fork, st);
-  for (int k = 0; k < MG_ERI_STREAMS; ++k) cudaStreamWaitEvent(h->eri_streams[k], h->eri_fork, 0);
+  int rc = side_streams_fork(h, st);
+  if (rc) return rc;
   for (size_t ci = 0; ci < classes.size(); ++ci) {
     const EriClass& c = classes[ci];
     if (eri_launch_class(h, d_items + c.begin, c.count, c.nab, c.ncd, c.plan, d_out, h->d_eri_counters + ci,
@@ -129,11 +119,34 @@ int run_eri_items(Handle* h, const std::vector<EriItem>& items, const std::vecto
       return MG_ERR_CUDA;
     }
   }
+  side_streams_join(h, st);
+  return 0;
+}
+
+int side_streams_fork(Handle* h, cudaStream_t st) {
+  if (!h->eri_streams[0]) {
+    for (int k = 0; k < MG_ERI_STREAMS; ++k) {
+      if (cudaStreamCreateWithFlags(&h->eri_streams[k], cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&h->eri_events[k], cudaEventDisableTiming) != cudaSuccess) {
+        h->err = "side streams could not be created";
+        return MG_ERR_CUDA;
+      }
+    }
+    if (cudaEventCreateWithFlags(&h->eri_fork, cudaEventDisableTiming) != cudaSuccess) {
+      h->err = "side streams could not be created";
+      return MG_ERR_CUDA;
+    }
+  }
+  cudaEventRecord(h->eri_fork, st);
+  for (int k = 0; k < MG_ERI_STREAMS; ++k) cudaStreamWaitEvent(h->eri_streams[k], h->eri_fork, 0);
+  return 0;
+}
+
+void side_streams_join(Handle* h, cudaStream_t st) {
   for (int k = 0; k < MG_ERI_STREAMS; ++k) {
     cudaEventRecord(h->eri_events[k], h->eri_streams[k]);
     cudaStreamWaitEvent(st, h->eri_events[k], 0);
   }
-  return 0;
 }
 
 }  // namespace mg

@@ -226,7 +226,9 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
   cudaFree(plan.d_counters);
   plan.d_scratch = nullptr;
   plan.d_counters = nullptr;
-  if (cudaMalloc(&plan.d_scratch, sizeof(double) * std::max<size_t>(scratch_need, 32)) != cudaSuccess ||
+  // one scratch region per side stream: class kernels on different streams run concurrently
+  plan.scratch_stride = (std::max<size_t>(scratch_need, 32) + 31) & ~(size_t)31;
+  if (cudaMalloc(&plan.d_scratch, sizeof(double) * plan.scratch_stride * MG_ERI_STREAMS) != cudaSuccess ||
       cudaMalloc(&plan.d_counters, sizeof(int) * std::max<size_t>(plan.classes.size(), 1)) != cudaSuccess) {
     h->err = "gradient scratch allocation failed";
     return MG_ERR_MEMORY;
@@ -245,16 +247,25 @@ int grad_run(Handle* h, const GradPlan& plan, const double* d_D, double* d_grad,
   ra.tab = h->d_rys;
   cudaMemsetAsync(d_grad, 0, sizeof(double) * 3 * h->natom, st);
   cudaMemsetAsync(plan.d_counters, 0, sizeof(int) * plan.classes.size(), st);
+  // The class kernels are independent (own counter, own scratch region per stream, atomic
+  // accumulation into the gradient): spread them over the handle's side streams so that the
+  // tail of one class overlaps the next.
+  int rc = side_streams_fork(h, st);
+  if (rc) return rc;
   for (size_t ci = 0; ci < plan.classes.size(); ++ci) {
     const GradClass& c = plan.classes[ci];
     GradFn k = grad_kernel_m1(c.nab1, c.ncd1);
     if (!k) { h->err = "gradient class out of range"; return MG_ERR_ARG; }
+    const int sk = (int)(ci % MG_ERI_STREAMS);
     GradArgs a{plan.d_items + c.begin, c.count, h->d_pairs, h->d_prim, h->tot_np, h->d_coef, d_D, h->nbf,
-               plan.d_tab, d_grad, plan.d_scratch, c.scr, plan.d_counters + ci, c.tpq, c.gsm, c.pab, c.pcd, c.rw};
-    k<<<(unsigned)c.grid, c.tpq * c.groups, sizeof(double) * (kGTabD + (size_t)c.gsm * c.groups), st>>>(a, ra);
+               plan.d_tab, d_grad, plan.d_scratch + plan.scratch_stride * sk, c.scr, plan.d_counters + ci, c.tpq,
+               c.gsm, c.pab, c.pcd, c.rw};
+    k<<<(unsigned)c.grid, c.tpq * c.groups, sizeof(double) * (kGTabD + (size_t)c.gsm * c.groups),
+        h->eri_streams[sk]>>>(a, ra);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (cudaGetLastError() != cudaSuccess) { h->err = "gradient kernel launch failed"; return MG_ERR_CUDA; }
   }
+  side_streams_join(h, st);
   return 0;
 }
 

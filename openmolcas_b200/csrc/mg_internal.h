@@ -102,7 +102,7 @@ struct Handle {
   struct ChoState* cho = nullptr;  // Cholesky vectors of the current basis
   struct GradPlan* grad = nullptr; // gradient work list (per Schwarz threshold)
   int* d_eri_counters = nullptr;   // one work counter per ERI class launch (64)
-  cudaStream_t eri_streams[MG_ERI_STREAMS] = {};  // side streams of the ERI class launches
+  cudaStream_t eri_streams[MG_ERI_STREAMS] = {};  // side streams of the ERI and gradient class launches
   cudaEvent_t eri_events[MG_ERI_STREAMS] = {};
   cudaEvent_t eri_fork = nullptr;
 };
@@ -123,12 +123,16 @@ struct GradPlan {
   std::vector<GradItem> items;
   std::vector<GradClass> classes;
   GradItem* d_items = nullptr;
+  size_t scratch_stride = 0;     // doubles of scratch per side stream
   double* d_tab = nullptr;       // per-CTA tables of the gradient kernel
   double* d_scratch = nullptr;   // per-group 2-PDM slots
   int* d_counters = nullptr;     // one work counter per class
   double cutint = -1;
 };
 int grad_build(Handle* h, double cutint, GradPlan& plan);
+// fork the handle's side streams from `st` (created on first use) / join them back into `st`
+int side_streams_fork(Handle* h, cudaStream_t st);
+void side_streams_join(Handle* h, cudaStream_t st);
 int rys_eval(Handle* h, int nrys, int64_t n, const double* d_T, double* d_x, double* d_w);
 int grad_run(Handle* h, const GradPlan& plan, const double* d_D, double* d_grad, cudaStream_t st);
 void grad_free(GradPlan* p);
