@@ -40,7 +40,7 @@ static inline size_t ev2s(size_t x) { return (x + 1) & ~(size_t)1; }
 // Launch plan of one class: tpq threads per work item (a group), 512/tpq
 // groups per CTA, primitive quartets in tiles of PAB bra x PCD ket pairs.
 // Per-group shared memory (doubles), the kernel's layout:
-//   hdr 2 | acc | Cab | Ccd | Et+Ft | max( X + cf + I + E, HRR temp )
+//   hdr 2 | acc | Cab | Ccd | Ft (bounded by ne + nf ints) | max( X + cf + I + E, HRR temp )
 static size_t eri_group_smem(int nab, int ncd, const ClassStats& cs, int pab, int pcd) {
   const int NR = (nab + ncd) / 2 + 1, NI = nab + 1, NJ = ncd + 1;
   const size_t gst = (size_t)(3 * NR * NI * NJ) | 1, cfs = NR * 10 + 1;

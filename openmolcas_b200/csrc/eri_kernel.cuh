@@ -6,9 +6,9 @@
 //   1a  thread per (primitive quartet, root): T, prefactor, Rys root/weight
 //       (table lookup), recursion coefficients (TERI teri.F90:51-57, ModU2,
 //       vCff2D vcff2d.F90) -> shared memory
-//   1b  8-lane group per (quartet, root, direction): 2D recursion (vRys2D
-//       vrys2d.F90), lane e holds row I[e][0..NCD] in registers and takes
-//       I[e-1][f] from its neighbour; weight * prefactor folded into z
+//   1b  NI-lane warp segment per (quartet, root, direction): 2D recursion
+//       (vRys2D vrys2d.F90), lane e holds row I[e][0..NCD] in registers and
+//       takes I[e-1][f] from its neighbour; weight * prefactor folded into z
 //   2a  thread per (quartet, f, Cartesian shell of the bra range):
 //       [e0|f0] = sum_r Ix Iy Iz  (RysEF), each shell's rows loaded once per
 //       root; consecutive lanes on consecutive primitive quartets
@@ -76,7 +76,7 @@ __device__ __forceinline__ void ef_shell(const double* __restrict__ Ib, int fxo,
 }
 
 // Per-group shared layout (doubles, every region even):
-//   hdr[2] | acc | Cab | Ccd | Et, Ft (ints) | union{ HRR temp | X | tile: cf | I | E }
+//   hdr[2] | acc | Cab | Ccd | Ft (ints) | union{ HRR temp | X | tile: cf | I | E }
 // I holds per primitive quartet [dir][root][f][e] (stride GST, odd); E per
 // quartet [ef] (stride nef | 1).
 template <int NAB, int NCD>
@@ -116,24 +116,19 @@ __global__ void __launch_bounds__(kEriThreads, 1) eri_kernel(const EriArgs a, co
     double* acc = sm + 2;
     double* Cab = acc + ev2(nacc);
     double* Ccd = Cab + ev2(nij * npab);
-    int* Et = reinterpret_cast<int*>(Ccd + ev2(nklc * npcd));
-    int* Ft = Et + ne;
-    double* X = reinterpret_cast<double*>(Et) + ev2((ne + nf + 1) / 2);
+    int* Ft = reinterpret_cast<int*>(Ccd + ev2(nklc * npcd));
+    double* X = reinterpret_cast<double*>(Ft) + ev2((nf + 1) / 2);
     double* cf = X + ev2(nij * PCD * nef);
     double* I = cf + ev2(NT * CFS);
     double* E = I + NT * GST;
     for (int o = tid; o < nacc; o += tpq) acc[o] = 0.0;
     for (int o = tid; o < nij * npab; o += tpq) Cab[o] = a.coef[P.coef_off + o];
     for (int o = tid; o < nklc * npcd; o += tpq) Ccd[o] = a.coef[Q.coef_off + (size_t)it.c0 * npcd + o];
-    {  // packed offsets of the Cartesian e and f components into one root of I
-      const int eoff = d_ccum(P.emin), foff = d_ccum(Q.emin);
-      for (int o = tid; o < ne + nf; o += tpq) {
-        if (o < ne) {
-          Et[o] = cart[eoff + o];
-        } else {
-          const int v = cart[foff + o - ne];
-          Ft[o - ne] = ((v & 255) * NI) | ((((v >> 8) & 255) * NI) << 8) | (((v >> 16) * NI) << 16);
-        }
+    {  // packed offsets of the Cartesian f components (f * NI per direction) into one root of I
+      const int foff = d_ccum(Q.emin);
+      for (int o = tid; o < nf; o += tpq) {
+        const int v = cart[foff + o];
+        Ft[o] = ((v & 255) * NI) | ((((v >> 8) & 255) * NI) << 8) | (((v >> 16) * NI) << 16);
       }
     }
     const double Ap0 = P.Ap[0], Ap1 = P.Ap[1], Ap2 = P.Ap[2];
@@ -176,15 +171,16 @@ __global__ void __launch_bounds__(kEriThreads, 1) eri_kernel(const EriArgs a, co
         }
         gsync(g, tpq);
         if (NI * NJ > 1) {
-          // ---- 1b: 2D recursion, one 8-lane group per (quartet, root, direction):
-          //      I[e][f+1] = D00 I[e][f] + f B01 I[e][f-1] + e B00 I[e-1][f]
+          // ---- 1b: 2D recursion, one NI-lane warp segment per (quartet, root, direction)
+          //      (32/NI jobs per warp): I[e][f+1] = D00 I[e][f] + f B01 I[e][f-1] + e B00 I[e-1][f]
+          constexpr int JPW = 32 / NI;
           const int njobs = nt * NR * 3;
           const int lane = tid & 31;
-          for (int ob = tid - lane; ob < njobs * 8; ob += tpq) {  // warp-uniform trip count
-            const int o = ob + lane;
-            const int e = o & 7;
-            const bool valid = (o >> 3) < njobs && e < NI;
-            const int job = min(o >> 3, njobs - 1);
+          const int seg = lane / NI, e = lane - seg * NI;  // seg >= JPW: spare lanes
+          const int lup = (lane + 31) & 31;
+          for (int jb = (tid >> 5) * JPW; jb < njobs; jb += (tpq >> 5) * JPW) {  // warp-uniform trip count
+            const bool valid = seg < JPW && jb + seg < njobs;
+            const int job = min(jb + seg, njobs - 1);
             const int d = job % 3, tr = job / 3, t = tr / NR, r = tr - t * NR;
             const double* c = cf + t * CFS + r * 10;
             const double B00 = c[0], B10 = c[1], B01 = c[2], C00 = c[3 + d], D00 = c[6 + d];
@@ -200,7 +196,7 @@ __global__ void __launch_bounds__(kEriThreads, 1) eri_kernel(const EriArgs a, co
             if (valid) Io[0] = L;
 #pragma unroll
             for (int j = 0; j < NJ - 1; ++j) {
-              const double up = __shfl_up_sync(0xffffffffu, L, 1, 8);  // I[e-1][j]
+              const double up = __shfl_sync(0xffffffffu, L, lup);  // I[e-1][j]
               double v = D00 * L;
               if (j > 0) v = fma(j * B01, Lm, v);
               if (e > 0) v = fma(e * B00, up, v);
