@@ -77,3 +77,28 @@ def test_jk_mixed_density_ranks(setup, rank):
     Jm, Km = (x.cpu().numpy() for x in g.cho_jk(C, precision=MolGpu.PREC_MIXED))
     assert np.abs(Jm - J).max() < 1e-6 * np.abs(J).max()
     assert np.abs(Km - K).max() < 1e-4 * np.abs(K).max()
+
+
+def test_c1_cluster_jk_energy():
+    """C1 (6 atoms, 84 functions, rank-15 density, ThrCom 1e-6): J, K and
+    E = 1/2 tr(DJ) - 1/4 tr(DK) of the FP64 path against the oracle's J/K
+    from the oracle's own vectors (same pivots), and the mixed path's energy
+    error stated against the FP64 path."""
+    mol = B.config_molecule("c1")
+    g = MolGpu(mol)
+    g.cho_drv(thrcom=1e-6)
+    o = O.Oracle(mol)
+    ref = o.cholesky(thrcom=1e-6)
+    Cm = B.density_factor(g.nbf, B.CONFIGS["c1"]["rank"], B.CONFIGS["c1"]["seed"])
+    J, K = (x.cpu().numpy() for x in g.cho_jk(torch.from_numpy(Cm), precision=MolGpu.PREC_FP64))
+    Jo, Ko = o.cho_jk(ref["L"], Cm)
+    assert np.abs(J - Jo).max() < 1e-10 * np.abs(Jo).max()
+    assert np.abs(K - Ko).max() < 1e-10 * np.abs(Ko).max()
+    D = Cm @ Cm.T
+    E = 0.5 * np.sum(D * J) - 0.25 * np.sum(D * K)
+    Eo = 0.5 * np.sum(D * Jo) - 0.25 * np.sum(D * Ko)
+    assert abs(E - Eo) < 1e-10 * abs(Eo)
+    Jm, Km = (x.cpu().numpy() for x in g.cho_jk(torch.from_numpy(Cm), precision=MolGpu.PREC_MIXED))
+    Em = 0.5 * np.sum(D * Jm) - 0.25 * np.sum(D * Km)
+    print(f"C1: E = {E:.10f}, |E - E_oracle| = {abs(E - Eo):.2e}, mixed dE = {Em - E:.2e}")
+    assert abs(Em - E) < 1e-5 * abs(E)
