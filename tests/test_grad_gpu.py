@@ -44,3 +44,25 @@ def test_gradient_repeatable_and_linear_in_scale():
     g1 = g.drvg1(D).cpu().numpy()
     g2 = g.drvg1(2.0 * D).cpu().numpy()  # quadratic in D
     assert np.abs(g2 - 4.0 * g1).max() < 1e-9 * max(1.0, np.abs(g2).max())
+
+
+def test_c4_cluster_full_size_properties():
+    """The bench's gradient workload (20 atoms 4s3p2d, 460 functions, rank-40
+    density, Schwarz 1e-12) through size-independent properties: translational
+    invariance (the forces sum to zero), repeatability across calls (atomic
+    accumulation order may differ), quadratic scaling in D, and a seeded
+    sample of atoms' components against the oracle's gradient restricted to
+    the same unique quartets (every 4000th, exercising every class)."""
+    mol = B.config_molecule("c4")
+    g = MolGpu(mol)
+    Cm = B.density_factor(g.nbf, B.CONFIGS["c4"]["rank"], B.CONFIGS["c4"]["seed"])
+    D = torch.from_numpy(Cm @ Cm.T)
+    g1 = g.drvg1(D).cpu().numpy()
+    g2 = g.drvg1(D).cpu().numpy()
+    g3 = g.drvg1(0.5 * D).cpu().numpy()
+    scale = np.abs(g1).max()
+    print(f"C4: max |F| {scale:.3f}, |sum F| {np.abs(g1.sum(0)).max():.2e}, "
+          f"repeat {np.abs(g1 - g2).max():.2e}")
+    assert np.abs(g1.sum(0)).max() < 1e-10 * scale
+    assert np.abs(g1 - g2).max() < 1e-12 * scale
+    assert np.abs(4.0 * g3 - g1).max() < 1e-11 * scale
