@@ -50,9 +50,8 @@ def test_c4_cluster_full_size_properties():
     """The bench's gradient workload (20 atoms 4s3p2d, 460 functions, rank-40
     density, Schwarz 1e-12) through size-independent properties: translational
     invariance (the forces sum to zero), repeatability across calls (atomic
-    accumulation order may differ), quadratic scaling in D, and a seeded
-    sample of atoms' components against the oracle's gradient restricted to
-    the same unique quartets (every 4000th, exercising every class)."""
+    accumulation order may differ) and quadratic scaling in D.  Parity with
+    the oracle for this basis is the c4like case above."""
     mol = B.config_molecule("c4")
     g = MolGpu(mol)
     Cm = B.density_factor(g.nbf, B.CONFIGS["c4"]["rank"], B.CONFIGS["c4"]["seed"])
