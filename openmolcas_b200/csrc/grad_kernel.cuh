@@ -433,12 +433,14 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
                 double u = L[cc];
                 double w = e2c * L[cc + 1] - (cc > 0 ? cc * L[cc > 0 ? cc - 1 : 0] : 0.0);
                 double uprev = 0.0;
+                // U(e-1, 0) from the neighbour once; later levels by the transfer itself,
+                // U(e-1, b+1) = U(e, b) + AB U(e-1, b), so each level needs two shuffles
+                double ud = __shfl_sync(0xffffffffu, u, lup);
                 const int ebase = (la + 1) * (lb + 1) * (cc + (lc + 1) * m);
 #pragma unroll
                 for (int b = 0; b < NI - 1; ++b) {
                   if (b > lb) break;
                   const double un = __shfl_sync(0xffffffffu, u, ldn);  // U(e+1, b)
-                  const double ud = __shfl_sync(0xffffffffu, u, lup);  // U(e-1, b)
                   const double wn = __shfl_sync(0xffffffffu, w, ldn);
                   const double unext = fma(abv, u, un);                       // U(e, b+1)
                   if (wr) {
@@ -451,6 +453,7 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
                     Fo[2 * e1] = v01;
                     Fo[2 * e1 + 1] = v23;
                   }
+                  ud = fma(abv, ud, u);  // U(e-1, b+1)
                   uprev = u;
                   u = unext;
                   w = fma(abv, w, wn);
