@@ -145,6 +145,16 @@ int mg_cho_jk(mg_handle* h, const double* d_C, int r, double* d_J, double* d_K, 
  * screening).  Asynchronous on `stream`.
  */
 int mg_drvg1(mg_handle* h, const double* d_D, double cutint, double* d_grad, void* stream);
+/* The same with the full 2-PDM of PGet1 (integral_util/pget1.F90:15-110, as
+ * PGet0 calls it at integral_util/pget0.F90:189 with D0, DS and the module
+ * EtWas factors):
+ *   E = coulfac/2 tr(D J[D]) - exfac/4 (tr(D K[D]) + tr(DS K[DS]))
+ * DS the spin density (DSSO: D_alpha - D_beta for an open shell, D the total
+ * density D_alpha + D_beta) or NULL for a closed shell; coulfac = CoulFac and
+ * exfac = ExFac (the exact-exchange fraction of a hybrid functional, 0 for a
+ * pure one).  mg_drvg1 is (DS = NULL, coulfac = 1, exfac = 1). */
+int mg_drvg1_x(mg_handle* h, const double* d_D, const double* d_DS, double coulfac, double exfac, double cutint,
+               double* d_grad, void* stream);
 /* Algorithmic FP64 flop count of one mg_drvg1 call (roofline accounting;
  * no reference counterpart).  Negative on error. */
 double mg_drvg1_flops(mg_handle* h, double cutint);

@@ -411,6 +411,11 @@ int mg_cho_diag(mg_handle* H, double* d_diag, void* stream) {
 }
 
 int mg_drvg1(mg_handle* H, const double* d_D, double cutint, double* d_grad, void* stream) {
+  return mg_drvg1_x(H, d_D, nullptr, 1.0, 1.0, cutint, d_grad, stream);
+}
+
+int mg_drvg1_x(mg_handle* H, const double* d_D, const double* d_DS, double coulfac, double exfac, double cutint,
+               double* d_grad, void* stream) {
   if (!H || !d_D || !d_grad) return MG_ERR_ARG;
   Handle* h = &H->h;
   if (h->pairs.empty()) { h->err = "mg_drvg1: no basis"; return MG_ERR_ARG; }
@@ -425,7 +430,7 @@ int mg_drvg1(mg_handle* H, const double* d_D, double cutint, double* d_grad, voi
     int rc = grad_build(h, cutint, *h->grad);
     if (rc) return rc;
   }
-  return grad_run(h, *h->grad, d_D, d_grad, (cudaStream_t)stream);
+  return grad_run(h, *h->grad, d_D, d_DS, coulfac, exfac, d_grad, (cudaStream_t)stream);
 }
 
 int mg_cho_jk(mg_handle* H, const double* d_C, int r, double* d_J, double* d_K, int precision, void* stream) {

@@ -241,7 +241,8 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
   return 0;
 }
 
-int grad_run(Handle* h, const GradPlan& plan, const double* d_D, double* d_grad, cudaStream_t st) {
+int grad_run(Handle* h, const GradPlan& plan, const double* d_D, const double* d_DS, double coulfac, double exfac,
+             double* d_grad, cudaStream_t st) {
   RysArgs ra;
   for (int i = 0; i < MG_MAX_RYS; ++i) ra.m[i] = h->rys_meta[i];
   ra.tab = h->d_rys;
@@ -259,7 +260,7 @@ int grad_run(Handle* h, const GradPlan& plan, const double* d_D, double* d_grad,
     const int sk = (int)(ci % MG_ERI_STREAMS);
     GradArgs a{plan.d_items + c.begin, c.count, h->d_pairs, h->d_prim, h->tot_np, h->d_coef, d_D, h->nbf,
                plan.d_tab, d_grad, plan.d_scratch + plan.scratch_stride * sk, c.scr, plan.d_counters + ci, c.tpq,
-               c.gsm, c.pab, c.pcd, c.rw};
+               c.gsm, c.pab, c.pcd, c.rw, d_DS, coulfac, 0.25 * exfac};
     k<<<(unsigned)c.grid, c.tpq * c.groups, sizeof(double) * (kGTabD + (size_t)c.gsm * c.groups),
         h->eri_streams[sk]>>>(a, ra);
     g_launches.fetch_add(1, std::memory_order_relaxed);

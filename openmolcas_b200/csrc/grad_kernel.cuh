@@ -32,6 +32,11 @@ struct GradArgs {
   long long scr_stride;  // doubles per slot
   int* counter;          // work-item counter of this launch (starts at 0)
   int tpq, gsm, PAB, PCD, RW;
+  // 2-PDM of PGet1 (integral_util/pget1.F90:66-106):
+  //   G = cq D(ab) D(cd) - xq [D(ac) D(bd) + D(ad) D(bc) + Ds(ac) Ds(bd) + Ds(ad) Ds(bc)]
+  const double* Ds;  // spin density (open shell) or null
+  double cq;         // CoulFac
+  double xq;         // ExFac / 4
 };
 
 using GradFn = void (*)(GradArgs, RysArgs);
@@ -180,8 +185,9 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
       const int pc = Q.ao_a + sc * Q.nci + kk, pd = Q.ao_b + sd * Q.ncj + kq;
       // D is symmetric: index it with the fastest-varying AO (pa, then pb) as the
       // column so that neighbouring threads read neighbouring addresses
-      Tmp[o] = Dm[pb * nbf + pa] * Dm[pd * nbf + pc] -
-               0.25 * (Dm[pc * nbf + pa] * Dm[pd * nbf + pb] + Dm[pd * nbf + pa] * Dm[pc * nbf + pb]);
+      double x = Dm[pc * nbf + pa] * Dm[pd * nbf + pb] + Dm[pd * nbf + pa] * Dm[pc * nbf + pb];
+      if (a.Ds) x += a.Ds[pc * nbf + pa] * a.Ds[pd * nbf + pb] + a.Ds[pd * nbf + pa] * a.Ds[pc * nbf + pb];
+      Tmp[o] = a.cq * Dm[pb * nbf + pa] * Dm[pd * nbf + pc] - a.xq * x;
     }
     gsync(g, tpq);
     const double* Sd = tabs + kGTabSph + d_sph_off(ld);

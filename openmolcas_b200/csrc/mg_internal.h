@@ -134,7 +134,8 @@ int grad_build(Handle* h, double cutint, GradPlan& plan);
 int side_streams_fork(Handle* h, cudaStream_t st);
 void side_streams_join(Handle* h, cudaStream_t st);
 int rys_eval(Handle* h, int nrys, int64_t n, const double* d_T, double* d_x, double* d_w);
-int grad_run(Handle* h, const GradPlan& plan, const double* d_D, double* d_grad, cudaStream_t st);
+int grad_run(Handle* h, const GradPlan& plan, const double* d_D, const double* d_DS, double coulfac, double exfac,
+             double* d_grad, cudaStream_t st);
 void grad_free(GradPlan* p);
 double grad_plan_flops(const Handle* h, const GradPlan& plan);
 

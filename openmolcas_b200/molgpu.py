@@ -55,6 +55,8 @@ def lib():
     L.mg_cho_copy_vectors.argtypes = [vp, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
     L.mg_cho_diag.argtypes = [vp, C.c_void_p, C.c_void_p]
     L.mg_drvg1.argtypes = [vp, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
+    L.mg_drvg1_x.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p,
+                             C.c_void_p]
     L.mg_cho_jk.argtypes = [vp, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     L.mg_rys_roots.argtypes = [vp, C.c_int, C.c_int64, d, d, d]
     L.mg_eri_work.argtypes = [vp, i32, C.c_int64, d, d]
@@ -230,15 +232,28 @@ class MolGpu:
         return J, K
 
     # -------------------------------------------------------- gradient
-    def drvg1(self, D: torch.Tensor, cutint: float = 1e-12, out: torch.Tensor | None = None) -> torch.Tensor:
-        """Drvg1: two-electron gradient dE/dR (natom x 3) of E = 1/2 tr(DJ) - 1/4 tr(DK)."""
+    def drvg1(self, D: torch.Tensor, cutint: float = 1e-12, out: torch.Tensor | None = None,
+              exfac: float = 1.0, coulfac: float = 1.0, DS: torch.Tensor | None = None) -> torch.Tensor:
+        """Drvg1: two-electron gradient dE/dR (natom x 3) of
+        E = coulfac/2 tr(D J[D]) - exfac/4 (tr(D K[D]) + tr(DS K[DS])).
+
+        The 2-PDM is PGet1's (integral_util/pget1.F90:66-110): exfac = ExFac
+        (1 for Hartree-Fock, the exact-exchange fraction of a hybrid functional,
+        0 for a pure one), coulfac = CoulFac, DS the spin density of an open
+        shell (D_alpha - D_beta, with D = D_alpha + D_beta) or None."""
         D = D.to(device=f"cuda:{self.device}", dtype=torch.float64).contiguous()
         if D.shape != (self.nbf, self.nbf):
             raise MolGpuError(f"density must be {self.nbf}x{self.nbf}")
+        ds_ptr = None
+        if DS is not None:
+            DS = DS.to(device=f"cuda:{self.device}", dtype=torch.float64).contiguous()
+            if DS.shape != (self.nbf, self.nbf):
+                raise MolGpuError(f"spin density must be {self.nbf}x{self.nbf}")
+            ds_ptr = DS.data_ptr()
         if out is None:
             out = torch.empty((self.natom, 3), dtype=torch.float64, device=f"cuda:{self.device}")
-        self._check(self.L.mg_drvg1(self.h, C.c_void_p(D.data_ptr()), cutint, C.c_void_p(out.data_ptr()),
-                                    _stream(self.device)), "mg_drvg1")
+        self._check(self.L.mg_drvg1_x(self.h, C.c_void_p(D.data_ptr()), C.c_void_p(ds_ptr), coulfac, exfac, cutint,
+                                      C.c_void_p(out.data_ptr()), _stream(self.device)), "mg_drvg1_x")
         return out
 
 

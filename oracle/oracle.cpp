@@ -812,7 +812,8 @@ std::vector<double> eri_diag(const Basis& bs, const RSList& R) {
 // --------------------------------------------------------------- gradient
 // Cartesian 2-PDM for one shell quartet, primitive quartet loop with the
 // derivative 2D integrals (Rysg1 + Rys2Dg + Assg1 + Distg1 restated).
-void grad_quartet(const Basis& bs, int iS, int jS, int kS, int lS, const double* Dm, double scale, double* grad) {
+void grad_quartet(const Basis& bs, int iS, int jS, int kS, int lS, const double* Dm, double scale, double* grad,
+                  const double* Ds = nullptr, double coulfac = 1.0, double exfac = 1.0) {
   const Shell* S[4] = {&bs.sh[iS], &bs.sh[jS], &bs.sh[kS], &bs.sh[lS]};
   int l[4], ns[4], ncr[4], nc[4];
   for (int t = 0; t < 4; ++t) { l[t] = S[t]->l; ns[t] = nsph(l[t]); ncr[t] = ncart(l[t]); nc[t] = S[t]->nc; }
@@ -824,7 +825,10 @@ void grad_quartet(const Basis& bs, int iS, int jS, int kS, int lS, const double*
   for (int md = 0; md < ns[3]; ++md) for (int mc = 0; mc < ns[2]; ++mc) for (int mb = 0; mb < ns[1]; ++mb) for (int ma = 0; ma < ns[0]; ++ma)
     for (int k4 = 0; k4 < nc[3]; ++k4) for (int k3 = 0; k3 < nc[2]; ++k3) for (int k2 = 0; k2 < nc[1]; ++k2) for (int k1 = 0; k1 < nc[0]; ++k1) {
       size_t p = ao_index(*S[0], k1, ma), q = ao_index(*S[1], k2, mb), r = ao_index(*S[2], k3, mc), s = ao_index(*S[3], k4, md);
-      double g = Dm[p * n + q] * Dm[r * n + s] - 0.25 * (Dm[p * n + r] * Dm[q * n + s] + Dm[p * n + s] * Dm[q * n + r]);
+      // CoulFac, ExFac and the spin density DSSO as in integral_util/pget1.F90:66-106
+      double x = Dm[p * n + r] * Dm[q * n + s] + Dm[p * n + s] * Dm[q * n + r];
+      if (Ds) x += Ds[p * n + r] * Ds[q * n + s] + Ds[p * n + s] * Ds[q * n + r];
+      double g = coulfac * Dm[p * n + q] * Dm[r * n + s] - 0.25 * exfac * x;
       int ijkl = k1 + nc[0] * (k2 + nc[1] * (k3 + nc[2] * k4));
       Gs[ijkl + (size_t)nijkl * (ma + ns[0] * (mb + (size_t)ns[1] * (mc + (size_t)ns[2] * md)))] = g;
     }
@@ -1126,12 +1130,23 @@ int or_cho_jk(void* h, const double* L, int M, const double* C, int r, double* J
 // D full nbf x nbf symmetric; grad[3*natom].  Quartets screened by
 // tmax(ij) tmax(kl) < cutint.
 int or_grad_sampled(void* h, const double* D, double cutint, int stride, double* grad, int64_t* nquartets);
+static int grad_sampled_x(void* h, const double* D, const double* Ds, double coulfac, double exfac, double cutint,
+                          int stride, double* grad, int64_t* nquartets);
 int or_grad(void* h, const double* D, double cutint, double* grad) {
-  return or_grad_sampled(h, D, cutint, 1, grad, nullptr);
+  return grad_sampled_x(h, D, nullptr, 1.0, 1.0, cutint, 1, grad, nullptr);
+}
+// the same with PGet1's full 2-PDM (integral_util/pget1.F90:66-106): spin
+// density Ds (or null), CoulFac and ExFac
+int or_grad_x(void* h, const double* D, const double* Ds, double coulfac, double exfac, double cutint, double* grad) {
+  return grad_sampled_x(h, D, Ds, coulfac, exfac, cutint, 1, grad, nullptr);
 }
 // every stride-th unique quartet only (timing samples of the CPU baseline);
 // *nquartets receives the total number of unique quartets after screening
 int or_grad_sampled(void* h, const double* D, double cutint, int stride, double* grad, int64_t* nquartets) {
+  return grad_sampled_x(h, D, nullptr, 1.0, 1.0, cutint, stride, grad, nquartets);
+}
+static int grad_sampled_x(void* h, const double* D, const double* Ds, double coulfac, double exfac, double cutint,
+                          int stride, double* grad, int64_t* nquartets) {
   Basis& bs = ((Handle*)h)->bs;
   if (bs.tmax.empty()) compute_tmax(bs);
   int ns = bs.sh.size();
@@ -1158,7 +1173,7 @@ int or_grad_sampled(void* h, const double* D, double cutint, int stride, double*
 #pragma omp for schedule(dynamic)
     for (size_t t = 0; t < qs.size(); ++t) {
       auto q = qs[t];
-      grad_quartet(bs, q[0], q[1], q[2], q[3], D, 0.5 * q[4], gl.data());
+      grad_quartet(bs, q[0], q[1], q[2], q[3], D, 0.5 * q[4], gl.data(), Ds, coulfac, exfac);
     }
 #pragma omp critical
     for (int t = 0; t < 3 * na; ++t) grad[t] += gl[t];

@@ -49,6 +49,7 @@ def lib():
         L.or_cholesky.argtypes = [vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, i, i, i, d, i]
         L.or_cho_jk.argtypes = [vp, d, C.c_int, d, C.c_int, d, d]
         L.or_grad.argtypes = [vp, d, C.c_double, d]
+        L.or_grad_x.argtypes = [vp, d, C.c_void_p, C.c_double, C.c_double, C.c_double, d]
         L.or_grad_sampled.argtypes = [vp, d, C.c_double, C.c_int, d, C.POINTER(C.c_int64)]
         L.or_num_threads.restype = C.c_int
         rc = L.or_load_rys(TABLE.encode())
@@ -167,10 +168,11 @@ class Oracle:
         lib().or_cho_jk(self.h, _p(Lf), M, _p(Cf), Cf.shape[1], _p(J), _p(K))
         return J.reshape(n, n, order="F"), K.reshape(n, n, order="F")
 
-    def grad(self, D, cutint=0.0):
+    def grad(self, D, cutint=0.0, exfac=1.0, coulfac=1.0, DS=None):
         Dc = np.ascontiguousarray(D, dtype=np.float64)
+        Ds = None if DS is None else np.ascontiguousarray(DS, dtype=np.float64)
         g = np.empty(3 * self.mol.natom)
-        lib().or_grad(self.h, _p(Dc), cutint, _p(g))
+        lib().or_grad_x(self.h, _p(Dc), None if Ds is None else Ds.ctypes.data, coulfac, exfac, cutint, _p(g))
         return g.reshape(-1, 3)
 
 

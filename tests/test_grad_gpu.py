@@ -36,6 +36,44 @@ def test_gradient_matches_oracle(mol, rel, absbar):
     assert np.abs(got.sum(0)).max() < 1e-9 * scale
 
 
+@pytest.mark.parametrize("cf,xf,open_shell", [(1.0, 0.0, False), (1.0, 0.25, False), (0.9, 0.2, True)])
+def test_gradient_2pdm_factors_match_oracle(cf, xf, open_shell):
+    """mg_drvg1_x: CoulFac, ExFac and the open-shell spin density of PGet1
+    (integral_util/pget1.F90:66-106) against the oracle, on the 4s3p2d cluster
+    at its 1e-9 relative bar."""
+    mol = B.make_molecule("c4like", 3, [("4s3p2d", 3)], 4)
+    g = MolGpu(mol)
+    o = O.Oracle(mol)
+    Ca = B.density_factor(g.nbf, 6, 3)
+    Da = Ca @ Ca.T
+    if open_shell:
+        Cb = B.density_factor(g.nbf, 4, 9)
+        Db = Cb @ Cb.T
+        D, DS = Da + Db, Da - Db
+    else:
+        D, DS = Da, None
+    ref = o.grad(D, exfac=xf, coulfac=cf, DS=DS)
+    got = g.drvg1(torch.from_numpy(D), exfac=xf, coulfac=cf,
+                  DS=None if DS is None else torch.from_numpy(DS)).cpu().numpy()
+    scale = max(1.0, np.abs(ref).max())
+    err = np.abs(got - ref).max()
+    print(f"coulfac {cf} exfac {xf} open {open_shell}: max |gpu - oracle| = {err:.2e} (scale {scale:.2f})")
+    assert err < 1e-9 * scale, (got, ref)
+    assert np.abs(got.sum(0)).max() < 1e-9 * scale
+
+
+def test_gradient_spin_density_limit():
+    """One spin only (D_beta = 0, so DS = D): the exchange part doubles, i.e.
+    drvg1(D, DS=D, exfac=1) equals drvg1(D, exfac=2) on the device."""
+    mol = B.small_molecule(3, seed=8)
+    g = MolGpu(mol)
+    Cm = B.density_factor(g.nbf, 5, 1)
+    D = torch.from_numpy(Cm @ Cm.T)
+    a = g.drvg1(D, DS=D).cpu().numpy()
+    b = g.drvg1(D, exfac=2.0).cpu().numpy()
+    assert np.abs(a - b).max() < 1e-11 * max(1.0, np.abs(b).max())
+
+
 def test_gradient_repeatable_and_linear_in_scale():
     mol = B.small_molecule(3, seed=8)
     g = MolGpu(mol)

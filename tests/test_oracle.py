@@ -173,3 +173,33 @@ def test_gradient_vs_central_fd():
         Ep = O.energy_from_full(O.Oracle(mol.moved(at, ax, h)).eri_full(), D)[0]
         Em = O.energy_from_full(O.Oracle(mol.moved(at, ax, -h)).eri_full(), D)[0]
         assert abs((Ep - Em) / (2 * h) - g[at, ax]) < 1e-6
+
+
+def test_gradient_open_shell_hybrid_vs_central_fd():
+    """PGet1's full 2-PDM (integral_util/pget1.F90:66-106): CoulFac, ExFac and
+    the spin density.  The oracle gradient is the derivative of
+    E = coulfac/2 tr(D J[D]) - exfac/4 (tr(D K[D]) + tr(DS K[DS]))."""
+    mol = B.small_molecule(3, seed=7)
+    o = O.Oracle(mol)
+    Ca = B.density_factor(o.nbf, 4, 3)
+    Cb = B.density_factor(o.nbf, 3, 5)
+    Da, Db = Ca @ Ca.T, Cb @ Cb.T
+    D, DS = Da + Db, Da - Db
+    cf, xf = 0.9, 0.25
+    g = o.grad(D, exfac=xf, coulfac=cf, DS=DS)
+    assert np.abs(g.sum(0)).max() < 1e-10
+
+    def energy(eri):
+        _, J, K = O.energy_from_full(eri, D)
+        KS = np.einsum("acbd,cd->ab", eri, DS)
+        return 0.5 * cf * np.sum(D * J) - 0.25 * xf * (np.sum(D * K) + np.sum(DS * KS))
+
+    h = 1e-4
+    for at, ax in [(0, 0), (1, 2), (2, 1)]:
+        Ep = energy(O.Oracle(mol.moved(at, ax, h)).eri_full())
+        Em = energy(O.Oracle(mol.moved(at, ax, -h)).eri_full())
+        assert abs((Ep - Em) / (2 * h) - g[at, ax]) < 1e-6
+    # linear in the factors
+    gJ = o.grad(D, exfac=0.0)
+    gK = o.grad(D, exfac=1.0, coulfac=0.0, DS=DS)
+    assert np.abs(g - (cf * gJ + xf * gK)).max() < 1e-11 * max(1.0, np.abs(g).max())
