@@ -187,6 +187,25 @@ def small_molecule(natom=3, mix=None, seed=11, name="small") -> Molecule:
     return make_molecule(name, natom, mix, seed)
 
 
+def molecule_from_arrays(name, coords, charges, shell_atom, shell_l, shell_nprim, shell_ncontr, exps,
+                         coefs) -> Molecule:
+    """A molecule from basis-library data: per shell its atom, l, nprim and
+    ncontr; exponents concatenated; raw contraction coefficients concatenated
+    per shell as [nprim, ncontr] row-major, the layout of the reference's
+    basis library entries.  Coefficients are normalised with Nrmlz."""
+    coords = np.asarray(coords, dtype=np.float64).reshape(-1, 3)
+    shells = []
+    pe = pc = 0
+    for a, l, npr, nco in zip(shell_atom, shell_l, shell_nprim, shell_ncontr):
+        a, l, npr, nco = int(a), int(l), int(npr), int(nco)
+        e = np.array(exps[pe:pe + npr], dtype=np.float64)
+        c = np.array(coefs[pc:pc + npr * nco], dtype=np.float64).reshape(npr, nco)
+        pe += npr
+        pc += npr * nco
+        shells.append(Shell(a, l, coords[a].copy(), e, nrmlz(e, c, l)))
+    return Molecule(name, coords, np.asarray(charges, dtype=np.float64), shells, 0)
+
+
 def density_factor(nbf: int, rank: int, seed: int) -> np.ndarray:
     """C (nbf x rank, column-major contiguous as F-order) with D = C C^T."""
     rng = np.random.default_rng(1000 + seed)

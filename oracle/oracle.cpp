@@ -579,8 +579,8 @@ inline double blk_elem(const Basis& bs, const double* blk, int i, int j, int k, 
 
 // columns (rs_row | ab_q) for all rows and the listed columns (all in one
 // shell pair AB), restating CHO_MCA_CALCINT_1 + PLF_Cho
-void cho_columns(const Basis& bs, const RSList& R, const std::vector<char>& inred, const std::vector<int>& cols,
-                 std::vector<double>& xint /* nrs x ncol */) {
+void cho_columns_sp(const Basis& bs, const RSList& R, const std::vector<char>& inred, const std::vector<int>& cols,
+                    std::vector<double>& xint /* nrs x ncol */) {
   size_t nrs = R.a.size();
   int ncol = cols.size();
   xint.assign(nrs * ncol, 0.0);
@@ -606,9 +606,30 @@ void cho_columns(const Basis& bs, const RSList& R, const std::vector<char>& inre
   }
 }
 
+// columns of qualified diagonals taken from several shell pairs (one
+// Cho_MCA_CalcInt per shell pair, cho_getint.F90:118), in list order
+void cho_columns(const Basis& bs, const RSList& R, const std::vector<char>& inred, const std::vector<int>& cols,
+                 std::vector<double>& xint /* nrs x ncol */) {
+  size_t nrs = R.a.size();
+  xint.assign(nrs * cols.size(), 0.0);
+  std::vector<char> done(cols.size(), 0);
+  for (size_t c0 = 0; c0 < cols.size(); ++c0) {
+    if (done[c0]) continue;
+    std::vector<int> sub, pos;
+    for (size_t c = c0; c < cols.size(); ++c)
+      if (!done[c] && R.sp[cols[c]] == R.sp[cols[c0]]) { sub.push_back(cols[c]); pos.push_back((int)c); done[c] = 1; }
+    std::vector<double> x;
+    cho_columns_sp(bs, R, inred, sub, x);
+    for (size_t q = 0; q < sub.size(); ++q)
+      std::copy(x.begin() + nrs * q, x.begin() + nrs * (q + 1), xint.begin() + nrs * pos[q]);
+  }
+}
+
 struct ChoCfg {
   double thrcom, span, damp1, damp2, thrneg, warneg, tooneg;
   int minqual, maxqual;
+  int mxshpr = 1;  // max. shell pairs qualified per pass; 0 = no limit (the serial default, cho_setmxshpr_def.F90)
+  int ialqua = 1;  // qualification: 1 = Cho_Qualify_1 (in order up to MaxQual), 2 = Cho_Qualify_2 (the default)
 };
 double cho_default_damp(double thrcom) {  // cho_setdamp.F90
   if (thrcom > 9.99e-3) return 1e7;
@@ -691,20 +712,67 @@ ChoResult cho_decompose(const Basis& bs, const ChoCfg& cfg, const std::vector<do
     double diamin = std::max(dgmax * cfg.span, cfg.thrcom);
     std::vector<double> diash(nsp, 0.0);
     for (size_t t = 0; t < nrs; ++t) if (inred[t]) diash[R.sp[t]] = std::max(diash[R.sp[t]], diag[t]);
-    for (int sp = 0; sp < nsp; ++sp) if (!(diash[sp] > cfg.thrcom)) diash[sp] = 0.0;
-    // Cho_GetMaxShl (MXSHPR=1: one shell pair per pass)
-    double smax = -1e9;
-    int spab = -1;
-    for (int sp = 0; sp < nsp; ++sp) if (diash[sp] > smax) { smax = diash[sp]; spab = sp; }
-    if (smax == 0.0 || std::fabs(smax) < diamin) { res.irc = 104; break; }
-    // Cho_Qualify_1
-    std::vector<int> qual;
-    for (int t = 0; t < R.sp_count[spab] && (int)qual.size() < cfg.maxqual; ++t) {
-      int rs = R.sp_first[spab] + t;
-      if (inred[rs] && diag[rs] >= diamin) qual.push_back(rs);
+    int npotsh = 0;
+    for (int sp = 0; sp < nsp; ++sp) {
+      if (!(diash[sp] > cfg.thrcom)) diash[sp] = 0.0; else ++npotsh;
     }
+    // Cho_GetInt (cho_getint.F90:38-140): take shell pairs in order of their
+    // largest diagonal (Cho_GetMaxShl zeroes the one it returns) and qualify
+    // their columns (Cho_Qualify, IALQUA = 2: cho_qualify_2.F90) until
+    // MinQual columns, MaxQual (FULL) or MXSHPR shell pairs
+    const int mcount = cfg.mxshpr > 0 ? std::min(npotsh, cfg.mxshpr) : npotsh;
+    std::vector<int> qual;
+    bool dodeco = false, fail = false;
+    for (int icount = 0; !dodeco && icount < mcount;) {
+      ++icount;
+      double smax = -1e9;
+      int spab = -1;
+      for (int sp = 0; sp < nsp; ++sp) if (diash[sp] > smax) { smax = diash[sp]; spab = sp; }
+      diash[spab] = 0.0;
+      if (smax == 0.0 || std::fabs(smax) < diamin) {
+        if (icount == 1) { fail = true; break; }
+        dodeco = !qual.empty();
+        break;
+      }
+      const int maxq = cfg.maxqual - (int)qual.size();
+      const size_t ioffq = qual.size();
+      if (cfg.ialqua == 1) {  // cho_qualify_1.F90:26-40: in order, up to MAXQ
+        for (int t = 0; t < R.sp_count[spab] && (int)(qual.size() - ioffq) < maxq; ++t) {
+          int rs = R.sp_first[spab] + t;
+          if (inred[rs] && diag[rs] >= diamin) qual.push_back(rs);
+        }
+      } else if (maxq == 1) {  // the largest >= DIAMIN (last one on ties)
+        double xmax = diamin;
+        int imax = -1;
+        for (int t = 0; t < R.sp_count[spab]; ++t) {
+          int rs = R.sp_first[spab] + t;
+          if (inred[rs] && diag[rs] >= xmax) { xmax = diag[rs]; imax = rs; }
+        }
+        if (imax >= 0) qual.push_back(imax);
+      } else if (maxq > 1) {  // in order; once MAXQ are taken, a larger one replaces the smallest
+        for (int t = 0; t < R.sp_count[spab]; ++t) {
+          int rs = R.sp_first[spab] + t;
+          if (!inred[rs] || !(diag[rs] >= diamin)) continue;
+          if ((int)(qual.size() - ioffq) < maxq) {
+            qual.push_back(rs);
+          } else {
+            size_t kmin = ioffq;
+            for (size_t k = ioffq + 1; k < qual.size(); ++k) if (diag[qual[k]] < diag[qual[kmin]]) kmin = k;
+            if (diag[rs] > diag[qual[kmin]]) qual[kmin] = rs;
+          }
+        }
+      }
+      const int ncolab = (int)(qual.size() - ioffq);
+      const bool full = (int)qual.size() == cfg.maxqual;
+      if (ncolab > 0) {
+        dodeco = full || (int)qual.size() >= cfg.minqual;
+      } else {
+        if (qual.empty()) { fail = true; break; }
+        dodeco = true;
+      }
+    }
+    if (fail || qual.empty()) { res.irc = 104; break; }
     int nq = qual.size();
-    if (nq == 0) { res.irc = 104; break; }
     std::vector<double> xint;
     cho_columns(bs, R, inred, qual, xint);
     // Cho_Dec_Qual: Q = MQ - LQ LQ^T, pivoted CD of Q
@@ -1048,11 +1116,20 @@ int or_eri_diag(void* h, double* d) {
 }
 
 // Cholesky alg 4. Output: M, pivots[M] (rs index), pass[M], L (nrs x maxvec)
+int or_cholesky_x(void* h, double thrcom, double span, int minqual, int maxqual, int mxshpr, int ialqua, int maxvec,
+                  int* M_out, int* piv, int* pass_of, double* L, int* npass);
 int or_cholesky(void* h, double thrcom, double span, int minqual, int maxqual, int maxvec, int* M_out, int* piv,
                 int* pass_of, double* L, int* npass) {
+  return or_cholesky_x(h, thrcom, span, minqual, maxqual, 1, 1, maxvec, M_out, piv, pass_of, L, npass);
+}
+// mxshpr: shell pairs qualified per pass (MXSHPR; 0 = the serial default);
+// ialqua: qualification algorithm (IALQUA; 2 = the default, cho_inp.F90:156)
+int or_cholesky_x(void* h, double thrcom, double span, int minqual, int maxqual, int mxshpr, int ialqua, int maxvec,
+                  int* M_out, int* piv, int* pass_of, double* L, int* npass) {
   Basis& bs = ((Handle*)h)->bs;
   ChoCfg cfg;
-  cfg.thrcom = thrcom; cfg.span = span; cfg.minqual = minqual; cfg.maxqual = maxqual;
+  cfg.thrcom = thrcom; cfg.span = span; cfg.minqual = minqual; cfg.maxqual = maxqual; cfg.mxshpr = mxshpr;
+  cfg.ialqua = ialqua;
   cfg.damp1 = cfg.damp2 = cho_default_damp(thrcom);
   cfg.thrneg = -1e-40; cfg.warneg = -1e-10; cfg.tooneg = -1e-8;
   RSList R = make_rs(bs);

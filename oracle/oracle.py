@@ -47,6 +47,8 @@ def lib():
         L.or_rs_list.argtypes = [vp, i, i, i]
         L.or_eri_diag.argtypes = [vp, d]
         L.or_cholesky.argtypes = [vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, i, i, i, d, i]
+        L.or_cholesky_x.argtypes = [vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, i, i, i,
+                                    d, i]
         L.or_cho_jk.argtypes = [vp, d, C.c_int, d, C.c_int, d, d]
         L.or_grad.argtypes = [vp, d, C.c_double, d]
         L.or_grad_x.argtypes = [vp, d, C.c_void_p, C.c_double, C.c_double, C.c_double, d]
@@ -141,7 +143,10 @@ class Oracle:
         lib().or_eri_diag(self.h, _p(d))
         return d
 
-    def cholesky(self, thrcom=1e-6, span=1e-2, minqual=50, maxqual=100, maxvec=None):
+    def cholesky(self, thrcom=1e-6, span=1e-2, minqual=50, maxqual=100, maxvec=None, mxshpr=1, ialqua=1):
+        """Pivoted Cholesky decomposition (alg 4).  mxshpr/ialqua: shell pairs
+        per pass and qualification algorithm; (1, 1) is the mode the device
+        decomposition implements, (0, 2) the reference's serial defaults."""
         nrs = lib().or_rs_count(self.h)
         if maxvec is None:
             maxvec = min(nrs, 20 * self.nbf)
@@ -150,8 +155,8 @@ class Oracle:
         pas = np.zeros(maxvec, np.int32)
         M = C.c_int(0)
         npass = C.c_int(0)
-        rc = lib().or_cholesky(self.h, thrcom, span, minqual, maxqual, maxvec, C.byref(M), _p(piv, C.c_int),
-                               _p(pas, C.c_int), _p(L), C.byref(npass))
+        rc = lib().or_cholesky_x(self.h, thrcom, span, minqual, maxqual, mxshpr, ialqua, maxvec, C.byref(M),
+                                 _p(piv, C.c_int), _p(pas, C.c_int), _p(L), C.byref(npass))
         if rc != 0:
             raise RuntimeError(f"oracle cholesky failed rc={rc}")
         m = M.value

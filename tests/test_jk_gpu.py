@@ -102,3 +102,30 @@ def test_c1_cluster_jk_energy():
     Em = 0.5 * np.sum(D * Jm) - 0.25 * np.sum(D * Km)
     print(f"C1: E = {E:.10f}, |E - E_oracle| = {abs(E - Eo):.2e}, mixed dE = {Em - E:.2e}")
     assert abs(Em - E) < 1e-5 * abs(E)
+
+
+def test_scf065_energy_through_device_cholesky(scf065):
+    """The reference's test 065 (CO, cc-pVDZ) through the device path: Cho_Drv
+    at ThrCom 1e-4 (mg_cho_drv) and FP64 J/K (mg_cho_jk) for the embedded
+    orbitals, with the oracle's one-electron matrices.  The energy equals the
+    oracle's from its own vectors (same pivots) to 1e-9 and E_SCF within the
+    reference harness's own tolerance for it (10^-4, the checkfile's digits)."""
+    from conftest import rhf_energy
+    from oracle import oneint
+    mol, z, Cocc = scf065["mol"], scf065["z"], scf065["Cocc"]
+    S, T, V = oneint.one_electron(mol)
+    D = 2.0 * Cocc @ Cocc.T
+    Cm = np.sqrt(2.0) * Cocc
+    g = MolGpu(mol)
+    g.cho_drv(thrcom=1e-4)
+    piv, _ = g.cho_pivots()
+    J, K = (x.cpu().numpy() for x in g.cho_jk(torch.from_numpy(Cm), precision=MolGpu.PREC_FP64))
+    E = rhf_energy(T + V, J, K, D, float(z["POTNUC"]))
+    o = O.Oracle(mol)
+    ref = o.cholesky(thrcom=1e-4)
+    Jo, Ko = o.cho_jk(ref["L"], Cm)
+    Eo = rhf_energy(T + V, Jo, Ko, D, float(z["POTNUC"]))
+    print(f"065 device: E = {E:.12f}  oracle {Eo:.12f}  E_SCF {float(z['E_SCF']):.12f}")
+    assert np.array_equal(piv, ref["piv"])
+    assert abs(E - Eo) < 1e-9
+    assert abs(E - float(z["E_SCF"])) <= 10.0 ** -int(z["E_SCF_digits"])

@@ -203,3 +203,49 @@ def test_gradient_open_shell_hybrid_vs_central_fd():
     gJ = o.grad(D, exfac=0.0)
     gK = o.grad(D, exfac=1.0, coulfac=0.0, DS=DS)
     assert np.abs(g - (cf * gJ + xf * gK)).max() < 1e-11 * max(1.0, np.abs(g).max())
+
+
+def test_scf065_one_electron_pins(scf065):
+    """The one-electron oracle against the reference's test 065 checkfile:
+    SEWARD_KINETIC / SEWARD_ATTRACT are the first packed element of the
+    kinetic and nuclear-attraction matrices (integral_util/oneel.F90:302-303),
+    POTNUC the nuclear repulsion; the embedded orbitals are orthonormal."""
+    from oracle import oneint
+    mol, z, Cocc = scf065["mol"], scf065["z"], scf065["Cocc"]
+    S, T, V = oneint.one_electron(mol)
+    assert abs(T[0, 0] - z["SEWARD_KINETIC"]) < 1e-10
+    assert abs(V[0, 0] - z["SEWARD_ATTRACT"]) < 1e-10
+    assert abs(oneint.nuclear_repulsion(mol) - z["POTNUC"]) < 1e-12
+    assert np.abs(np.diag(S) - 1.0).max() < 1e-13
+    assert np.abs(Cocc.T @ S @ Cocc - np.eye(Cocc.shape[1])).max() < 1e-10
+
+
+def test_scf065_energy_from_oracle_cholesky(scf065):
+    """E_SCF of the reference's test 065 from the oracle's Cholesky vectors
+    (ThrCom 1e-4, as Seward's Cholesky keyword sets it).  The reference's own
+    harness accepts |dE| <= 1e-4 for this value (tolerance digits 4,
+    Tools/pymolcas/check_test.py:137-151); the Cholesky error itself is of
+    that order (the exact-ERI energy is 9.4e-5 below E_SCF), so matching the
+    printed digits would need the reference's decomposition bit for bit.
+    The mode the device decomposition implements (one shell pair per pass,
+    Cho_Qualify_1) lands 2.1e-5 from E_SCF; the reference's serial defaults
+    (MxShPr 0, IALQUA 2) restated here give a valid decomposition with a
+    different pass structure, checked through its residual diagonal."""
+    from conftest import rhf_energy
+    from oracle import oneint
+    mol, z, Cocc = scf065["mol"], scf065["z"], scf065["Cocc"]
+    S, T, V = oneint.one_electron(mol)
+    D = 2.0 * Cocc @ Cocc.T
+    o = O.Oracle(mol)
+    res = o.cholesky(thrcom=1e-4)
+    J, K = o.cho_jk(res["L"], math.sqrt(2.0) * Cocc)
+    E = rhf_energy(T + V, J, K, D, float(z["POTNUC"]))
+    print(f"065: E = {E:.12f}  E_SCF = {float(z['E_SCF']):.12f}  dE = {E - float(z['E_SCF']):.2e}")
+    assert abs(E - float(z["E_SCF"])) <= 10.0 ** -int(z["E_SCF_digits"])
+    diag = o.eri_diag()
+    for mx, ia in ((1, 1), (0, 2)):
+        r = o.cholesky(thrcom=1e-4, mxshpr=mx, ialqua=ia)
+        resid = diag - np.einsum("tj,tj->t", r["L"], r["L"])
+        assert resid.max() <= 1e-4 and resid.min() > -1e-10, (mx, ia)
+        assert len(set(r["piv"].tolist())) == r["M"]
+    assert r["npass"] < res["npass"]  # several shell pairs per pass
