@@ -138,6 +138,9 @@ BASIS_TYPES = {
     "4s3p2d1f": [(4, 8), (3, 5), (2, 3), (1, 1)],
     "2s1p_r": [(2, None), (1, None)],
     "4s3p2d1f_r": [(4, None), (3, None), (2, None), (1, None)],
+    # large general contractions: shell pairs hold up to 450 AO pairs, above
+    # the Cholesky MaxQual of 100
+    "7s6p5d": [(7, 9), (6, 8), (5, 7)],
 }
 
 

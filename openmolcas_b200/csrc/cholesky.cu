@@ -3,8 +3,8 @@
 //
 //   pass loop  CHO_DECDRV          cho_decdrv.F90:98-260
 //   SetPass    max diag, DiaMin    cho_setpass.F90:29-47
-//   GetMaxShl  one shell pair      cho_getmaxshl.F90, MXSHPR=1 (cho_inp.F90:710-715)
-//   Qualify_1  diag >= DiaMin      cho_qualify_1.F90:26-40, MaxQual = 100
+//   GetMaxShl  one shell pair      cho_getmaxshl.F90, MXSHPR=1 (cho_inp.F90:709-715)
+//   Qualify_2  diag >= DiaMin      cho_qualify_2.F90 (IALQUA = 2, cho_inp.F90:156), MaxQual = 100
 //   columns    (CD|AB) all CD      cho_mca_calcint_1.F90 + PLF_Cho
 //   Dec_Qual   Q = MQ - LQ LQ^T    cho_dec_qual.F90:57-83 (Thr = max(ThrCom, Dmax Span))
 //   CD_InCore_1p pivot rule        cd_incore_1p.F90:33-85 (Acc tie rule, host FP64)
@@ -438,7 +438,10 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
       if (v > smax) { smax = v; spab = sp; }
     }
     if (smax == 0.0 || std::fabs(smax) < diamin) { rc = MG_ERR_DECOMP; err = "no qualifying diagonal (Cho_GetInt 104)"; break; }
-    // ---- Cho_Qualify_1 within shell pair spab
+    // ---- Cho_Qualify_2 within shell pair spab: the reduced-set diagonals
+    // >= DiaMin in order; once MaxQual are taken, a larger one replaces the
+    // smallest taken (the first of equal smallest); MaxQual = 1 takes the
+    // largest (the last of equal largest)
     const int64_t f = c->sp_first[spab];
     const int cnt = c->sp_count[spab];
     std::vector<double> dpair(cnt);
@@ -446,9 +449,27 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
     cudaMemcpyAsync(dpair.data(), c->d_diag + f, sizeof(double) * cnt, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(rpair.data(), c->d_inred + f, cnt, cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
-    std::vector<int> qual;
-    for (int t = 0; t < cnt && (int)qual.size() < cfg.maxqual; ++t)
-      if (rpair[t] && dpair[t] >= diamin) qual.push_back((int)(f + t));
+    std::vector<int> qual;  // positions t inside the pair, then rs indices
+    if (cfg.maxqual == 1) {
+      double xmax = diamin;
+      int imax = -1;
+      for (int t = 0; t < cnt; ++t)
+        if (rpair[t] && dpair[t] >= xmax) { xmax = dpair[t]; imax = t; }
+      if (imax >= 0) qual.push_back(imax);
+    } else {
+      for (int t = 0; t < cnt; ++t) {
+        if (!rpair[t] || !(dpair[t] >= diamin)) continue;
+        if ((int)qual.size() < cfg.maxqual) {
+          qual.push_back(t);
+        } else {
+          size_t kmin = 0;
+          for (size_t k = 1; k < qual.size(); ++k)
+            if (dpair[qual[k]] < dpair[qual[kmin]]) kmin = k;
+          if (dpair[t] > dpair[qual[kmin]]) qual[kmin] = t;
+        }
+      }
+    }
+    for (int& t : qual) t = (int)(f + t);
     const int nq = qual.size();
     if (nq == 0) { rc = MG_ERR_DECOMP; err = "empty qualification (Cho_GetInt 104)"; break; }
     // ---- integral columns (CD|AB) for every CD pair touching the reduced set

@@ -26,8 +26,10 @@
 //    AOInt(nijkl, iCmp1, iCmp2, iCmp3, iCmp4), contracted index fastest,
 //    i fastest inside ijkl.
 //  * Cholesky alg 4 (cholesky_util): Cho_SetPass (cho_setpass.F90:29-47),
-//    Cho_GetMaxShl (cho_getmaxshl.F90), Cho_Qualify_1 (cho_qualify_1.F90:
-//    26-40), Cho_Dec_Qual (cho_dec_qual.F90:57-83), CD_InCore_1p
+//    Cho_GetInt (cho_getint.F90:38-140, MXSHPR), Cho_GetMaxShl
+//    (cho_getmaxshl.F90), Cho_Qualify_2 (cho_qualify_2.F90; IALQUA = 2, the
+//    default) and Cho_Qualify_1 (cho_qualify_1.F90:26-40), Cho_Dec_Qual
+//    (cho_dec_qual.F90:57-83), CD_InCore_1p
 //    (cd_incore_1p.F90:33-85), Cho_CompVec (cho_compvec.F90:40-120),
 //    Cho_ChkDia_A4 (cho_chkdia_a4.F90:31-62), Cho_SetRed mode 1
 //    (cho_setred.F90:72-100), Cho_SetDamp (cho_setdamp.F90).
@@ -628,8 +630,8 @@ void cho_columns(const Basis& bs, const RSList& R, const std::vector<char>& inre
 struct ChoCfg {
   double thrcom, span, damp1, damp2, thrneg, warneg, tooneg;
   int minqual, maxqual;
-  int mxshpr = 1;  // max. shell pairs qualified per pass; 0 = no limit (the serial default, cho_setmxshpr_def.F90)
-  int ialqua = 1;  // qualification: 1 = Cho_Qualify_1 (in order up to MaxQual), 2 = Cho_Qualify_2 (the default)
+  int mxshpr = 1;  // max. shell pairs qualified per pass (1 for algorithm 4); 0 = no limit (algorithms 1-3)
+  int ialqua = 2;  // qualification: 1 = Cho_Qualify_1 (in order up to MaxQual), 2 = Cho_Qualify_2 (the default)
 };
 double cho_default_damp(double thrcom) {  // cho_setdamp.F90
   if (thrcom > 9.99e-3) return 1e7;
@@ -1120,10 +1122,11 @@ int or_cholesky_x(void* h, double thrcom, double span, int minqual, int maxqual,
                   int* M_out, int* piv, int* pass_of, double* L, int* npass);
 int or_cholesky(void* h, double thrcom, double span, int minqual, int maxqual, int maxvec, int* M_out, int* piv,
                 int* pass_of, double* L, int* npass) {
-  return or_cholesky_x(h, thrcom, span, minqual, maxqual, 1, 1, maxvec, M_out, piv, pass_of, L, npass);
+  return or_cholesky_x(h, thrcom, span, minqual, maxqual, 1, 2, maxvec, M_out, piv, pass_of, L, npass);
 }
-// mxshpr: shell pairs qualified per pass (MXSHPR; 0 = the serial default);
-// ialqua: qualification algorithm (IALQUA; 2 = the default, cho_inp.F90:156)
+// mxshpr: shell pairs qualified per pass (MXSHPR: 1 for algorithm 4,
+// cho_inp.F90:709-715; 0 = no limit, algorithms 1-3); ialqua: qualification
+// algorithm (IALQUA; 2 = the default, cho_inp.F90:156).  or_cholesky is (1, 2).
 int or_cholesky_x(void* h, double thrcom, double span, int minqual, int maxqual, int mxshpr, int ialqua, int maxvec,
                   int* M_out, int* piv, int* pass_of, double* L, int* npass) {
   Basis& bs = ((Handle*)h)->bs;

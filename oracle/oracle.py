@@ -143,10 +143,10 @@ class Oracle:
         lib().or_eri_diag(self.h, _p(d))
         return d
 
-    def cholesky(self, thrcom=1e-6, span=1e-2, minqual=50, maxqual=100, maxvec=None, mxshpr=1, ialqua=1):
-        """Pivoted Cholesky decomposition (alg 4).  mxshpr/ialqua: shell pairs
-        per pass and qualification algorithm; (1, 1) is the mode the device
-        decomposition implements, (0, 2) the reference's serial defaults."""
+    def cholesky(self, thrcom=1e-6, span=1e-2, minqual=50, maxqual=100, maxvec=None, mxshpr=1, ialqua=2):
+        """Pivoted Cholesky decomposition.  mxshpr/ialqua: shell pairs per pass
+        and qualification algorithm; (1, 2) is the reference's default for
+        algorithm 4 and what the device decomposition implements."""
         nrs = lib().or_rs_count(self.h)
         if maxvec is None:
             maxvec = min(nrs, 20 * self.nbf)

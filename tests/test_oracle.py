@@ -227,10 +227,10 @@ def test_scf065_energy_from_oracle_cholesky(scf065):
     Tools/pymolcas/check_test.py:137-151); the Cholesky error itself is of
     that order (the exact-ERI energy is 9.4e-5 below E_SCF), so matching the
     printed digits would need the reference's decomposition bit for bit.
-    The mode the device decomposition implements (one shell pair per pass,
-    Cho_Qualify_1) lands 2.1e-5 from E_SCF; the reference's serial defaults
-    (MxShPr 0, IALQUA 2) restated here give a valid decomposition with a
-    different pass structure, checked through its residual diagonal."""
+    The algorithm-4 defaults (one shell pair per pass, cho_inp.F90:709-715;
+    Cho_Qualify_2) land 2.1e-5 from E_SCF.  MXSHPR 0 (algorithms 1-3: shell
+    pairs are qualified until MinQual) gives a valid decomposition with fewer
+    passes, checked through its residual diagonal."""
     from conftest import rhf_energy
     from oracle import oneint
     mol, z, Cocc = scf065["mol"], scf065["z"], scf065["Cocc"]
@@ -249,3 +249,20 @@ def test_scf065_energy_from_oracle_cholesky(scf065):
         assert resid.max() <= 1e-4 and resid.min() > -1e-10, (mx, ia)
         assert len(set(r["piv"].tolist())) == r["M"]
     assert r["npass"] < res["npass"]  # several shell pairs per pass
+
+
+def test_cholesky_qualify_2_replaces_when_a_shell_pair_exceeds_maxqual():
+    """Cho_Qualify_2 (IALQUA 2, the default; cho_qualify_2.F90): once MaxQual
+    diagonals of a shell pair are taken, a larger one replaces the smallest.
+    With shell pairs of up to 450 AO pairs this changes the pivots relative
+    to in-order qualification (Cho_Qualify_1); both are valid decompositions."""
+    mol = B.make_molecule("bigpair", 2, [("7s6p5d", 2)], 3)
+    o = O.Oracle(mol)
+    diag = o.eri_diag()
+    a = o.cholesky(thrcom=1e-6, ialqua=1)
+    b = o.cholesky(thrcom=1e-6)  # ialqua 2
+    assert not (a["M"] == b["M"] and np.array_equal(a["piv"], b["piv"]))
+    for r in (a, b):
+        resid = diag - np.einsum("tj,tj->t", r["L"], r["L"])
+        assert resid.max() <= 1e-6 and resid.min() > -1e-10
+        assert len(set(r["piv"].tolist())) == r["M"]
