@@ -1,0 +1,95 @@
+"""Closed-shell SCF iteration over the Cholesky J/K build.
+
+The caller loop around ``CHO_LK_SCF``: the reference's SCF program builds the
+two-electron Fock matrix from Cholesky vectors in ``ChoSCF_Drv``
+(``scf/choscf_drv.F90:15``, ``CHO_LK_SCF`` at :208) for the density of the
+occupied orbitals, and iterates Roothaan steps with DIIS until the energy and
+the density converge.  The energy is the one the reference prints as E_SCF
+(``scf/prfin0.F90:147``): one-electron energy tr(D h) + two-electron energy
+1/2 tr(D J) - 1/4 tr(D K) + nuclear repulsion, D = 2 C_occ C_occ^T.
+
+Here the two-electron part is ``jk(C)``: J and K of D = C C^T, by default the
+device build ``MolGpu.cho_jk`` (FP64) over vectors from ``MolGpu.cho_drv``.
+The one-electron matrices h and S come from the caller (the reference reads
+them from Seward's one-electron file).  Every matrix lives on one torch
+device; the iteration is O(nbf^3) dense algebra per step (eigendecomposition,
+DIIS extrapolation) next to the J/K build.
+
+Restated with our own choices: core-Hamiltonian guess unless orbitals are
+given, canonical orthogonalisation dropping overlap eigenvalues below
+``lindep``, Pulay DIIS on the orthogonalised commutator FDS - SDF.
+"""
+from __future__ import annotations
+
+from typing import Callable, Optional
+
+import torch
+
+
+def _orthogonaliser(S: torch.Tensor, lindep: float) -> torch.Tensor:
+    s, U = torch.linalg.eigh(S)
+    keep = s > lindep
+    return U[:, keep] / torch.sqrt(s[keep])[None, :]
+
+
+def rhf(jk: Callable[[torch.Tensor], tuple], h: torch.Tensor, S: torch.Tensor, nocc: int, enuc: float,
+        C0: Optional[torch.Tensor] = None, e_conv: float = 1e-10, d_conv: float = 1e-8, maxiter: int = 100,
+        ndiis: int = 8, lindep: float = 1e-9) -> dict:
+    """Closed-shell SCF.  jk(C) returns (J, K) of D = C C^T (nbf x nbf).
+
+    Returns dict(energy, C (nbf x nmo), eps (nmo), niter, converged, history):
+    ``energy`` is E_SCF of the last density, ``history`` the energy per
+    iteration.  Converged when the energy change is below ``e_conv`` and the
+    largest element of the orthogonalised commutator below ``d_conv``."""
+    dev, dt = h.device, torch.float64
+    h = h.to(dev, dt)
+    S = S.to(dev, dt)
+    X = _orthogonaliser(S, lindep)
+
+    def diag(F):
+        eps, Ct = torch.linalg.eigh(X.T @ F @ X)
+        return eps, X @ Ct
+
+    if C0 is None:
+        eps, C = diag(h)
+        Cocc = C[:, :nocc]
+    else:
+        Cocc = C0.to(dev, dt)[:, :nocc]
+    fock_hist, err_hist, energies = [], [], []
+    e_old = None
+    converged = False
+    eps = C = None
+    for it in range(1, maxiter + 1):
+        D = 2.0 * Cocc @ Cocc.T
+        J, K = jk(Cocc * (2.0 ** 0.5))
+        J = J.to(dev, dt)
+        K = K.to(dev, dt)
+        F = h + J - 0.5 * K
+        E = float(torch.sum(D * h) + 0.5 * torch.sum(D * J) - 0.25 * torch.sum(D * K)) + enuc
+        energies.append(E)
+        err = X.T @ (F @ D @ S - S @ D @ F) @ X
+        emax = float(err.abs().max())
+        if e_old is not None and abs(E - e_old) < e_conv and emax < d_conv:
+            converged = True
+            eps, C = diag(F)
+            break
+        e_old = E
+        fock_hist.append(F)
+        err_hist.append(err)
+        del fock_hist[:-ndiis], err_hist[:-ndiis]
+        n = len(fock_hist)
+        if n > 1:
+            Bm = torch.empty((n + 1, n + 1), dtype=dt, device=dev)
+            for i in range(n):
+                for j in range(n):
+                    Bm[i, j] = torch.sum(err_hist[i] * err_hist[j])
+            Bm[n, :n] = -1.0
+            Bm[:n, n] = -1.0
+            Bm[n, n] = 0.0
+            rhs = torch.zeros(n + 1, dtype=dt, device=dev)
+            rhs[n] = -1.0
+            c = torch.linalg.solve(Bm, rhs)[:n]
+            F = sum(ci * Fi for ci, Fi in zip(c, fock_hist))
+        eps, C = diag(F)
+        Cocc = C[:, :nocc]
+    return dict(energy=energies[-1], C=C, eps=eps, niter=len(energies), converged=converged, history=energies)
