@@ -200,3 +200,136 @@ def nuclear_repulsion(mol):
         for j in range(i):
             e += mol.charges[i] * mol.charges[j] / float(np.linalg.norm(mol.coords[i] - mol.coords[j]))
     return e
+
+
+def _prim_tables(sa, sb, ka, kb, nuclei, extra):
+    """1D tables of one primitive pair with angular momenta raised by
+    ``extra`` (1 for first derivatives): S and T per direction, the Hermite
+    expansion per direction and R_tuv per nucleus."""
+    a, b = sa.exps[ka], sb.exps[kb]
+    A, B = sa.center, sb.center
+    p = a + b
+    P = (a * A + b * B) / p
+    mu = a * b / p
+    AB = A - B
+    la, lb = sa.l + extra, sb.l + extra
+    Sx = [_os_1d(la, lb + 2, P[d] - A[d], P[d] - B[d], p, math.sqrt(math.pi / p) * math.exp(-mu * AB[d] ** 2))
+          for d in range(3)]
+    Tx = []
+    for d in range(3):
+        S = Sx[d]
+        T = np.zeros((la + 1, lb + 1))
+        for i in range(la + 1):
+            for j in range(lb + 1):
+                v = -2.0 * b * b * S[i, j + 2] + b * (2 * j + 1) * S[i, j]
+                if j > 1:
+                    v -= 0.5 * j * (j - 1) * S[i, j - 2]
+                T[i, j] = v
+        Tx.append(T)
+    Ex = [_hermite_1d(la, lb, P[d] - A[d], P[d] - B[d], p, math.exp(-mu * AB[d] ** 2)) for d in range(3)]
+    Rs = [_hermite_r(la + lb, p, P - C) for _, C in nuclei]
+    return a, b, p, Sx, Tx, Ex, Rs
+
+
+def _ints(tab, u, v, nuclei):
+    """S, T and V_C (per nucleus, without -Z) of Cartesian exponent triples u, v."""
+    a, b, p, Sx, Tx, Ex, Rs = tab
+    if min(u) < 0 or min(v) < 0:
+        return 0.0, 0.0, np.zeros(len(nuclei))
+    sx, sy, sz = Sx[0][u[0], v[0]], Sx[1][u[1], v[1]], Sx[2][u[2], v[2]]
+    s = sx * sy * sz
+    t = Tx[0][u[0], v[0]] * sy * sz + sx * Tx[1][u[1], v[1]] * sz + sx * sy * Tx[2][u[2], v[2]]
+    ex, ey, ez = Ex[0][u[0], v[0]], Ex[1][u[1], v[1]], Ex[2][u[2], v[2]]
+    vc = np.empty(len(nuclei))
+    for c, R in enumerate(Rs):
+        acc = 0.0
+        for tt in range(u[0] + v[0] + 1):
+            for w in range(u[1] + v[1] + 1):
+                acc += ex[tt] * ey[w] * float(ez[: u[2] + v[2] + 1] @ R[tt, w, : u[2] + v[2] + 1])
+        vc[c] = 2.0 * math.pi / p * acc
+    return s, t, vc
+
+
+def one_electron_gradient(mol, D, W):
+    """sum_mn D_mn dh_mn/dR - W_mn dS_mn/dR (natom x 3), h = T + V.
+
+    The derivative of a primitive with respect to its centre is
+    2 alpha |u + e_d> - u_d |u - e_d>; the operator (Hellmann-Feynman) part of
+    the attraction of nucleus C follows from translational invariance:
+    d<a|V_C|b>/dC = -(d/dA + d/dB)<a|V_C|b>.  D, W: full symmetric AO
+    matrices (density and energy-weighted density)."""
+    nuclei = [(float(mol.charges[i]), np.asarray(mol.coords[i], dtype=np.float64)) for i in range(mol.natom)]
+    offs = np.cumsum([0] + [s.nbf for s in mol.shells])
+    G = np.zeros((mol.natom, 3))
+    sph = {}
+
+    def tr(l):
+        if l < 2:
+            return np.eye((l + 1) * (l + 2) // 2)
+        if l not in sph:
+            sph[l] = O.sph_matrix(l)
+        return sph[l]
+
+    for i, sa in enumerate(mol.shells):
+        for j, sb in enumerate(mol.shells):
+            ca, cb = _carts(sa.l), _carts(sb.l)
+            # accumulators [type][d] with type: dS/dA, dS/dB, dT/dA, dT/dB, dV_C/dA, dV_C/dB (per C)
+            nC = len(nuclei)
+            acc = np.zeros((6 + 2 * nC, 3, len(ca), sa.ncontr, len(cb), sb.ncontr))
+            for ka in range(sa.nprim):
+                for kb in range(sb.nprim):
+                    tab = _prim_tables(sa, sb, ka, kb, nuclei, 1)
+                    a, b = tab[0], tab[1]
+                    cc = np.outer(sa.coef[ka], sb.coef[kb])
+                    for u, ue in enumerate(ca):
+                        for v, ve in enumerate(cb):
+                            for d in range(3):
+                                up = list(ue); up[d] += 1
+                                um = list(ue); um[d] -= 1
+                                vp = list(ve); vp[d] += 1
+                                vm = list(ve); vm[d] -= 1
+                                sp, tp, vpc = _ints(tab, up, ve, nuclei)
+                                sm, tm, vmc = _ints(tab, um, ve, nuclei)
+                                dA = (2 * a * sp - ue[d] * sm, 2 * a * tp - ue[d] * tm, 2 * a * vpc - ue[d] * vmc)
+                                sp, tp, vpc = _ints(tab, ue, vp, nuclei)
+                                sm, tm, vmc = _ints(tab, ue, vm, nuclei)
+                                dB = (2 * b * sp - ve[d] * sm, 2 * b * tp - ve[d] * tm, 2 * b * vpc - ve[d] * vmc)
+                                vals = [dA[0], dB[0], dA[1], dB[1]]
+                                acc[0, d, u, :, v, :] += dA[0] * cc
+                                acc[1, d, u, :, v, :] += dB[0] * cc
+                                acc[2, d, u, :, v, :] += dA[1] * cc
+                                acc[3, d, u, :, v, :] += dB[1] * cc
+                                for c in range(nC):
+                                    acc[6 + c, d, u, :, v, :] += dA[2][c] * cc
+                                    acc[6 + nC + c, d, u, :, v, :] += dB[2][c] * cc
+                                del vals
+            Ua, Ub = tr(sa.l), tr(sb.l)
+            blkD = D[offs[i]:offs[i + 1], offs[j]:offs[j + 1]]
+            blkW = W[offs[i]:offs[i + 1], offs[j]:offs[j + 1]]
+
+            def contract(m, d):
+                x = np.einsum("ucvd,um,vn->mcnd", acc[m, d], Ua, Ub).reshape(sa.nbf, sb.nbf)
+                return x
+
+            for d in range(3):
+                dSA, dSB = contract(0, d), contract(1, d)
+                dTA, dTB = contract(2, d), contract(3, d)
+                G[sa.atom, d] += np.sum(blkD * dTA) - np.sum(blkW * dSA)
+                G[sb.atom, d] += np.sum(blkD * dTB) - np.sum(blkW * dSB)
+                for c, (Z, _) in enumerate(nuclei):
+                    dVA, dVB = contract(6 + c, d), contract(6 + nC + c, d)
+                    eA, eB = -Z * np.sum(blkD * dVA), -Z * np.sum(blkD * dVB)
+                    G[sa.atom, d] += eA
+                    G[sb.atom, d] += eB
+                    G[c, d] -= eA + eB
+    return G
+
+
+def nuclear_repulsion_gradient(mol):
+    G = np.zeros((mol.natom, 3))
+    for i in range(mol.natom):
+        for j in range(mol.natom):
+            if i != j:
+                r = mol.coords[i] - mol.coords[j]
+                G[i] -= mol.charges[i] * mol.charges[j] * r / float(np.linalg.norm(r)) ** 3
+    return G

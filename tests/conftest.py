@@ -40,3 +40,56 @@ def rhf_energy(h, J, K, D, enuc):
     """Closed-shell energy tr(D h) + 1/2 tr(D J) - 1/4 tr(D K) + E_nuc, D = 2 C_occ C_occ^T."""
     import numpy as np
     return float(np.sum(D * h) + 0.5 * np.sum(D * J) - 0.25 * np.sum(D * K) + enuc)
+
+
+@pytest.fixture(scope="session")
+def grad862():
+    """The reference's test 862 (water, 6-31G, no symmetry, conventional
+    integrals, SCF + Alaska), first geometry, from
+    tests/golden/grad862_h2o_631g.npz (made by make_grad862_golden.py)."""
+    import numpy as np
+
+    from openmolcas_b200 import basis as B
+
+    z = dict(np.load(os.path.join(ROOT, "tests", "golden", "grad862_h2o_631g.npz")))
+    mol = B.molecule_from_arrays("h2o_631g", z["coords"], z["charges"], z["shell_atom"], z["shell_l"],
+                                 z["shell_nprim"], z["shell_ncontr"], z["exps"], z["coefs"])
+    return dict(mol=mol, z=z, nocc=int(round(float(z["charges"].sum()) / 2)))
+
+
+def full_eri_from_blocks(mol, quartets, flat, off):
+    """Full (ab|cd) tensor from Eval_IJKL-layout blocks of unique quartets
+    (i>=j, k>=l, ij>=kl): block = AOInt(nijkl, a, b, c, d) in Fortran order,
+    contracted index fastest, AO = shell offset + component * ncontr + k."""
+    import numpy as np
+
+    sh = mol.shells
+    offs = np.cumsum([0] + [s.nbf for s in sh])
+    n = int(offs[-1])
+    eri = np.zeros((n, n, n, n))
+    for t, (i, j, k, l) in enumerate(np.asarray(quartets)):
+        S = [sh[i], sh[j], sh[k], sh[l]]
+        nc = [s.ncontr for s in S]
+        nm = [s.ncomp for s in S]
+        blk = np.asarray(flat[off[t]:off[t + 1]]).reshape(nc + nm, order="F")
+        blk = blk.transpose(4, 0, 5, 1, 6, 2, 7, 3).reshape([s.nbf for s in S])
+        si = [slice(offs[x], offs[x + 1]) for x in (i, j, k, l)]
+        for a, b, c, d, perm in (
+            (0, 1, 2, 3, (0, 1, 2, 3)), (1, 0, 2, 3, (1, 0, 2, 3)), (0, 1, 3, 2, (0, 1, 3, 2)),
+            (1, 0, 3, 2, (1, 0, 3, 2)), (2, 3, 0, 1, (2, 3, 0, 1)), (3, 2, 0, 1, (3, 2, 0, 1)),
+            (2, 3, 1, 0, (2, 3, 1, 0)), (3, 2, 1, 0, (3, 2, 1, 0))):
+            eri[si[a], si[b], si[c], si[d]] = blk.transpose(perm)
+    return eri
+
+
+def exact_jk(eri):
+    """jk(C) for scf.rhf from a full ERI tensor: J, K of D = C C^T."""
+    import numpy as np
+    import torch
+
+    def jk(Cf):
+        Cn = Cf.detach().cpu().numpy()
+        D = Cn @ Cn.T
+        return (torch.from_numpy(np.einsum("abcd,cd->ab", eri, D)),
+                torch.from_numpy(np.einsum("acbd,cd->ab", eri, D)))
+    return jk
