@@ -105,7 +105,7 @@ typedef struct mg_cho_cfg {
   double span;   /* Span (cho_inp.F90:151, 1e-2)                            */
   int minqual;   /* MinQual (50)                                             */
   int maxqual;   /* MaxQual (100)                                            */
-  int maxvec;    /* capacity of the vector store (0 = 8 x nbf)               */
+  int maxvec;    /* max. vectors (0 = nbf(nbf+1)/2, the most there can be)  */
 } mg_cho_cfg;
 
 int mg_cho_default(mg_cho_cfg* cfg);

@@ -93,3 +93,18 @@ def exact_jk(eri):
         return (torch.from_numpy(np.einsum("abcd,cd->ab", eri, D)),
                 torch.from_numpy(np.einsum("acbd,cd->ab", eri, D)))
     return jk
+
+
+@pytest.fixture(scope="session")
+def scf071():
+    """The reference's test 071 (water, cc-pVTZ: s to f shells, no symmetry,
+    conventional integrals, closed-shell SCF), from
+    tests/golden/scf071_h2o_ccpvtz.npz (made by make_scf071_golden.py)."""
+    import numpy as np
+
+    from openmolcas_b200 import basis as B
+
+    z = dict(np.load(os.path.join(ROOT, "tests", "golden", "scf071_h2o_ccpvtz.npz")))
+    mol = B.molecule_from_arrays("h2o_ccpvtz", z["coords"], z["charges"], z["shell_atom"], z["shell_l"],
+                                 z["shell_nprim"], z["shell_ncontr"], z["exps"], z["coefs"])
+    return dict(mol=mol, z=z, nocc=int(round(float(z["charges"].sum()) / 2)))
