@@ -108,3 +108,19 @@ def scf071():
     mol = B.molecule_from_arrays("h2o_ccpvtz", z["coords"], z["charges"], z["shell_atom"], z["shell_l"],
                                  z["shell_nprim"], z["shell_ncontr"], z["exps"], z["coefs"])
     return dict(mol=mol, z=z, nocc=int(round(float(z["charges"].sum()) / 2)))
+
+
+@pytest.fixture(scope="session")
+def grad020():
+    """The reference's test 020 (CH4, cc-pVDZ, generators x z, conventional
+    integrals, SCF + Alaska), first geometry, expanded to all atoms, from
+    tests/golden/grad020_ch4_ccpvdz.npz (made by make_grad020_golden.py).
+    GRAD[i] is the component grad_comp[i] of atom grad_atom[i]."""
+    import numpy as np
+
+    from openmolcas_b200 import basis as B
+
+    z = dict(np.load(os.path.join(ROOT, "tests", "golden", "grad020_ch4_ccpvdz.npz")))
+    mol = B.molecule_from_arrays("ch4_ccpvdz", z["coords"], z["charges"], z["shell_atom"], z["shell_l"],
+                                 z["shell_nprim"], z["shell_ncontr"], z["exps"], z["coefs"])
+    return dict(mol=mol, z=z, nocc=int(round(float(z["charges"].sum()) / 2)))

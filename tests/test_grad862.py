@@ -65,3 +65,20 @@ def test_one_electron_gradient_vs_central_fd(grad862):
             return np.sum(D * (T + V)) - np.sum(W * S)
         fd = (e1(mol.moved(at, ax, h)) - e1(mol.moved(at, ax, -h))) / (2 * h)
         assert abs(fd - G[at, ax]) < 1e-6 * max(1.0, abs(fd))
+
+
+def test_grad020_ch4_ccpvdz_energy_and_symmetry_unique_gradient(grad020):
+    """The reference's test 020 (CH4, cc-pVDZ: d shells on C; C2v in the
+    reference, all atoms here): E_SCF to its 8 digits and the GRAD entries
+    (symmetry-allowed components of the unique centres) to their 6 digits."""
+    mol, z, nocc = grad020["mol"], grad020["z"], grad020["nocc"]
+    assert abs(oneint.nuclear_repulsion(mol) - float(z["POTNUC"])) <= 10.0 ** -int(z["POTNUC_digits"])
+    o = O.Oracle(mol)
+    res, D, W = _scf(mol, o.eri_full(), nocc)
+    assert res["converged"]
+    assert abs(res["energy"] - float(z["E_SCF"])) <= 10.0 ** -int(z["E_SCF_digits"])
+    G = oneint.one_electron_gradient(mol, D, W) + o.grad(D) + oneint.nuclear_repulsion_gradient(mol)
+    g = G[z["grad_atom"], z["grad_comp"]]
+    err = np.abs(g - z["GRAD"]).max()
+    print(f"020: E - E_SCF = {res['energy'] - float(z['E_SCF']):.1e}, max |grad - GRAD| = {err:.1e}")
+    assert err <= 10.0 ** -int(z["GRAD_digits"])
