@@ -273,7 +273,7 @@ def one_electron_gradient(mol, D, W):
     for i, sa in enumerate(mol.shells):
         for j, sb in enumerate(mol.shells):
             ca, cb = _carts(sa.l), _carts(sb.l)
-            # accumulators [type][d] with type: dS/dA, dS/dB, dT/dA, dT/dB, dV_C/dA, dV_C/dB (per C)
+            # accumulators [type][d]: dS/dA, dS/dB, dT/dA, dT/dB, (unused 4, 5), dV_C/dA per C, dV_C/dB per C
             nC = len(nuclei)
             acc = np.zeros((6 + 2 * nC, 3, len(ca), sa.ncontr, len(cb), sb.ncontr))
             for ka in range(sa.nprim):
@@ -294,7 +294,6 @@ def one_electron_gradient(mol, D, W):
                                 sp, tp, vpc = _ints(tab, ue, vp, nuclei)
                                 sm, tm, vmc = _ints(tab, ue, vm, nuclei)
                                 dB = (2 * b * sp - ve[d] * sm, 2 * b * tp - ve[d] * tm, 2 * b * vpc - ve[d] * vmc)
-                                vals = [dA[0], dB[0], dA[1], dB[1]]
                                 acc[0, d, u, :, v, :] += dA[0] * cc
                                 acc[1, d, u, :, v, :] += dB[0] * cc
                                 acc[2, d, u, :, v, :] += dA[1] * cc
@@ -302,14 +301,12 @@ def one_electron_gradient(mol, D, W):
                                 for c in range(nC):
                                     acc[6 + c, d, u, :, v, :] += dA[2][c] * cc
                                     acc[6 + nC + c, d, u, :, v, :] += dB[2][c] * cc
-                                del vals
             Ua, Ub = tr(sa.l), tr(sb.l)
             blkD = D[offs[i]:offs[i + 1], offs[j]:offs[j + 1]]
             blkW = W[offs[i]:offs[i + 1], offs[j]:offs[j + 1]]
 
             def contract(m, d):
-                x = np.einsum("ucvd,um,vn->mcnd", acc[m, d], Ua, Ub).reshape(sa.nbf, sb.nbf)
-                return x
+                return np.einsum("ucvd,um,vn->mcnd", acc[m, d], Ua, Ub).reshape(sa.nbf, sb.nbf)
 
             for d in range(3):
                 dSA, dSB = contract(0, d), contract(1, d)
