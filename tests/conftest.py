@@ -110,17 +110,22 @@ def scf071():
     return dict(mol=mol, z=z, nocc=int(round(float(z["charges"].sum()) / 2)))
 
 
-@pytest.fixture(scope="session")
-def grad020():
-    """The reference's test 020 (CH4, cc-pVDZ, generators x z, conventional
-    integrals, SCF + Alaska), first geometry, expanded to all atoms, from
-    tests/golden/grad020_ch4_ccpvdz.npz (made by make_grad020_golden.py).
-    GRAD[i] is the component grad_comp[i] of atom grad_atom[i]."""
+def _symgrad_case(name):
     import numpy as np
 
     from openmolcas_b200 import basis as B
 
-    z = dict(np.load(os.path.join(ROOT, "tests", "golden", "grad020_ch4_ccpvdz.npz")))
-    mol = B.molecule_from_arrays("ch4_ccpvdz", z["coords"], z["charges"], z["shell_atom"], z["shell_l"],
+    z = dict(np.load(os.path.join(ROOT, "tests", "golden", name + ".npz")))
+    mol = B.molecule_from_arrays(name, z["coords"], z["charges"], z["shell_atom"], z["shell_l"],
                                  z["shell_nprim"], z["shell_ncontr"], z["exps"], z["coefs"])
     return dict(mol=mol, z=z, nocc=int(round(float(z["charges"].sum()) / 2)))
+
+
+@pytest.fixture(scope="session", params=["grad020_ch4_ccpvdz", "grad023_ch2o2_ccpvdz"])
+def symgrad(request):
+    """The reference's tests 020 (CH4, cc-pVDZ, generators x z) and 023
+    (CH2O2, cc-pVDZ, generator Y): conventional integrals, SCF + Alaska, first
+    geometry, expanded to all atoms, from tests/golden/<name>.npz (made by
+    make_symgrad_golden.py).  GRAD[i] is the component grad_comp[i] of atom
+    grad_atom[i] (the symmetry-allowed components of the unique centres)."""
+    return _symgrad_case(request.param)

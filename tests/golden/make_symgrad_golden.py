@@ -1,9 +1,12 @@
-"""Generate tests/golden/grad020_ch4_ccpvdz.npz from the reference's test 020.
+"""Generate a gradient fixture from one of the reference's SCF + Alaska tests
+that use point-group symmetry (tests/golden/grad020_ch4_ccpvdz.npz from test
+020, tests/golden/grad023_ch2o2_ccpvdz.npz from test 023).
 
-The reference's ``test/standard/020.input`` optimises CH4 in cc-pVDZ with the
-symmetry generators ``x z`` (C2v) and conventional integrals (``NoCD``):
-``&SEWARD``, ``&SCF``, ``&ALASKA``.  Its checkfile holds, for the first
-geometry, POTNUC, E_SCF (8 digits) and GRAD (6 digits).  With symmetry, GRAD
+Test 020 optimises CH4 in cc-pVDZ with the symmetry generators ``x z`` (C2v),
+test 023 a CH2O2 transition state in cc-pVDZ with the generator ``Y`` (Cs);
+both use conventional integrals (``NoCD``): ``&SEWARD``, ``&SCF``,
+``&ALASKA``.  Their checkfiles hold, for the first geometry, POTNUC, E_SCF
+(8 digits) and GRAD (6 digits).  With symmetry, GRAD
 lists the symmetry-allowed Cartesian components of the symmetry-unique
 centres: centre by centre in input order, x, y, z, keeping a component when
 no operation that leaves the centre in place changes its sign.
@@ -11,15 +14,16 @@ no operation that leaves the centre in place changes its sign.
 This script reads, from a reference tree:
   * the generators after ``Symmetry`` and the ``Basis Set`` blocks of
     ``&SEWARD`` (label line, then ``name x y z`` in bohr; lines starting with
-    ``*`` are comments) from ``test/standard/020.input``, and the first POTNUC,
-    E_SCF and GRAD entries of its checkfile;
-  * the C and H entries of ``basis_library/CC-PVDZ`` (the reader of
+    ``*`` are comments) from ``test/standard/<id>.input``, and the first
+    POTNUC, E_SCF and GRAD entries of its checkfile;
+  * the entries of ``basis_library/CC-PVDZ`` for its elements (the reader of
     make_grad862_golden.py);
 expands every unique centre by the group the generators span (a generator
 names the coordinates whose sign it changes), and writes the molecule, the
 index of each atom's unique centre, and for every GRAD entry the atom and
 component it belongs to.  Run in a container that has the reference tree:
-    python tests/golden/make_grad020_golden.py /path/to/OpenMolcas
+    python tests/golden/make_symgrad_golden.py /path/to/OpenMolcas 020 grad020_ch4_ccpvdz
+    python tests/golden/make_symgrad_golden.py /path/to/OpenMolcas 023 grad023_ch2o2_ccpvdz
 """
 from __future__ import annotations
 
@@ -83,8 +87,8 @@ def group_ops(gens):
     return sorted(ops, reverse=True)
 
 
-def main(ref):
-    gens, centres, chk = read_input(os.path.join(ref, "test", "standard", "020.input"))
+def main(ref, test_id, name):
+    gens, centres, chk = read_input(os.path.join(ref, "test", "standard", test_id + ".input"))
     ops = group_ops(gens)
     xyz, unique_of, elems, labels = [], [], [], []
     comps = []  # (atom index, component) per GRAD entry
@@ -127,10 +131,10 @@ def main(ref):
     out["GRAD"] = np.array([chk[f"GRAD[{i}]"][0] for i in range(len(comps))])
     out["GRAD_digits"] = np.array(chk["GRAD[0]"][1])
     assert f"GRAD[{len(comps)}]" not in chk
-    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "grad020_ch4_ccpvdz.npz")
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), name + ".npz")
     np.savez(dst, **out)
     print(dst, len(xyz), "atoms", comps, float(out["E_SCF"]), out["GRAD"].tolist())
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1], sys.argv[2], sys.argv[3])

@@ -67,11 +67,12 @@ def test_one_electron_gradient_vs_central_fd(grad862):
         assert abs(fd - G[at, ax]) < 1e-6 * max(1.0, abs(fd))
 
 
-def test_grad020_ch4_ccpvdz_energy_and_symmetry_unique_gradient(grad020):
-    """The reference's test 020 (CH4, cc-pVDZ: d shells on C; C2v in the
-    reference, all atoms here): E_SCF to its 8 digits and the GRAD entries
-    (symmetry-allowed components of the unique centres) to their 6 digits."""
-    mol, z, nocc = grad020["mol"], grad020["z"], grad020["nocc"]
+def test_symmetric_case_energy_and_symmetry_unique_gradient(symgrad):
+    """The reference's tests 020 (CH4) and 023 (CH2O2), cc-pVDZ with d shells
+    on the heavy atoms, point-group symmetry in the reference and all atoms
+    here: E_SCF to its 8 digits and the GRAD entries (symmetry-allowed
+    components of the unique centres) to their 6 digits."""
+    mol, z, nocc = symgrad["mol"], symgrad["z"], symgrad["nocc"]
     assert abs(oneint.nuclear_repulsion(mol) - float(z["POTNUC"])) <= 10.0 ** -int(z["POTNUC_digits"])
     o = O.Oracle(mol)
     res, D, W = _scf(mol, o.eri_full(), nocc)
@@ -80,5 +81,5 @@ def test_grad020_ch4_ccpvdz_energy_and_symmetry_unique_gradient(grad020):
     G = oneint.one_electron_gradient(mol, D, W) + o.grad(D) + oneint.nuclear_repulsion_gradient(mol)
     g = G[z["grad_atom"], z["grad_comp"]]
     err = np.abs(g - z["GRAD"]).max()
-    print(f"020: E - E_SCF = {res['energy'] - float(z['E_SCF']):.1e}, max |grad - GRAD| = {err:.1e}")
+    print(f"{mol.name}: E - E_SCF = {res['energy'] - float(z['E_SCF']):.1e}, max |grad - GRAD| = {err:.1e}")
     assert err <= 10.0 ** -int(z["GRAD_digits"])

@@ -141,17 +141,17 @@ def test_grad862_device_eris_and_drvg1_against_reference(grad862):
     assert err <= 10.0 ** -int(z["GRAD_digits"])
 
 
-def test_grad020_device_drvg1_with_d_shells_against_reference(grad020):
-    """The reference's test 020 (CH4, cc-pVDZ, d shells on C): the SCF over
-    the device ERIs meets E_SCF (8 digits) and mg_drvg1 gives the
-    two-electron gradient, which with the oracle's one-electron and nuclear
-    terms meets the checkfile's symmetry-reduced GRAD (6 digits)."""
+def test_symmetric_case_device_drvg1_with_d_shells_against_reference(symgrad):
+    """The reference's tests 020 (CH4) and 023 (CH2O2), cc-pVDZ with d
+    shells: the SCF over the device ERIs meets E_SCF (8 digits) and mg_drvg1
+    gives the two-electron gradient, which with the oracle's one-electron and
+    nuclear terms meets the checkfile's symmetry-reduced GRAD (6 digits)."""
     from conftest import exact_jk, full_eri_from_blocks
     from oracle import oneint
     from openmolcas_b200 import scf
     from openmolcas_b200.molgpu import unique_quartets
 
-    mol, z, nocc = grad020["mol"], grad020["z"], grad020["nocc"]
+    mol, z, nocc = symgrad["mol"], symgrad["z"], symgrad["nocc"]
     g = MolGpu(mol)
     o = O.Oracle(mol)
     q = unique_quartets(len(mol.shells))
@@ -170,5 +170,5 @@ def test_grad020_device_drvg1_with_d_shells_against_reference(grad020):
     assert np.abs(g2 - ref2).max() < 1e-9 * max(1.0, np.abs(ref2).max())
     G = oneint.one_electron_gradient(mol, D, W) + g2 + oneint.nuclear_repulsion_gradient(mol)
     err = np.abs(G[z["grad_atom"], z["grad_comp"]] - z["GRAD"]).max()
-    print(f"020 device: max |grad - GRAD| = {err:.1e}")
+    print(f"{mol.name} device: max |grad - GRAD| = {err:.1e}")
     assert err <= 10.0 ** -int(z["GRAD_digits"])
