@@ -121,7 +121,9 @@ def _symgrad_case(name):
     return dict(mol=mol, z=z, nocc=int(round(float(z["charges"].sum()) / 2)))
 
 
-@pytest.fixture(scope="session", params=["grad020_ch4_ccpvdz", "grad023_ch2o2_ccpvdz"])
+# function scope: a parametrised fixture of wider scope makes pytest regroup
+# the tests that use it across files, out of collection order
+@pytest.fixture(params=["grad020_ch4_ccpvdz", "grad023_ch2o2_ccpvdz"])
 def symgrad(request):
     """The reference's tests 020 (CH4, cc-pVDZ, generators x z) and 023
     (CH2O2, cc-pVDZ, generator Y): conventional integrals, SCF + Alaska, first

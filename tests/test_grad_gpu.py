@@ -104,71 +104,3 @@ def test_c4_cluster_full_size_properties():
     assert np.abs(g1 - g2).max() < 1e-12 * scale
     assert np.abs(4.0 * g3 - g1).max() < 1e-11 * scale
 
-
-def test_grad862_device_eris_and_drvg1_against_reference(grad862):
-    """The reference's test 862 (water, 6-31G, conventional integrals), first
-    geometry, through the device: every unique shell quartet from
-    mg_eri_quartets feeds the SCF (E_SCF to the checkfile's 8 digits), and
-    mg_drvg1 gives the two-electron gradient, which with the oracle's
-    one-electron and nuclear terms meets GRAD to its 6 digits; the device
-    parts also equal the oracle's (1e-11 ERIs, 1e-9 relative gradient)."""
-    from conftest import exact_jk, full_eri_from_blocks
-    from oracle import oneint
-    from openmolcas_b200 import scf
-    from openmolcas_b200.molgpu import unique_quartets
-
-    mol, z, nocc = grad862["mol"], grad862["z"], grad862["nocc"]
-    g = MolGpu(mol)
-    o = O.Oracle(mol)
-    q = unique_quartets(len(mol.shells))
-    flat, off = g.eri_quartets(q)
-    eri = full_eri_from_blocks(mol, q, flat.cpu().numpy(), off)
-    assert np.abs(eri - o.eri_full()).max() < 1e-11
-    S, T, V = oneint.one_electron(mol)
-    res = scf.rhf(exact_jk(eri), torch.from_numpy(T + V), torch.from_numpy(S), nocc, oneint.nuclear_repulsion(mol),
-                  e_conv=1e-12, d_conv=1e-10)
-    assert res["converged"]
-    assert abs(res["energy"] - float(z["E_SCF"])) <= 10.0 ** -int(z["E_SCF_digits"])
-    C, eps = res["C"].numpy(), res["eps"].numpy()
-    Co = C[:, :nocc]
-    D, W = 2.0 * Co @ Co.T, 2.0 * (Co * eps[:nocc]) @ Co.T
-    g2 = g.drvg1(torch.from_numpy(D)).cpu().numpy()
-    ref2 = o.grad(D)
-    assert np.abs(g2 - ref2).max() < 1e-9 * max(1.0, np.abs(ref2).max())
-    G = oneint.one_electron_gradient(mol, D, W) + g2 + oneint.nuclear_repulsion_gradient(mol)
-    err = np.abs(G - z["GRAD"]).max()
-    print(f"862 device: E = {res['energy']:.12f} (E_SCF {float(z['E_SCF']):.12f}), max |grad - GRAD| = {err:.1e}")
-    assert err <= 10.0 ** -int(z["GRAD_digits"])
-
-
-def test_symmetric_case_device_drvg1_with_d_shells_against_reference(symgrad):
-    """The reference's tests 020 (CH4) and 023 (CH2O2), cc-pVDZ with d
-    shells: the SCF over the device ERIs meets E_SCF (8 digits) and mg_drvg1
-    gives the two-electron gradient, which with the oracle's one-electron and
-    nuclear terms meets the checkfile's symmetry-reduced GRAD (6 digits)."""
-    from conftest import exact_jk, full_eri_from_blocks
-    from oracle import oneint
-    from openmolcas_b200 import scf
-    from openmolcas_b200.molgpu import unique_quartets
-
-    mol, z, nocc = symgrad["mol"], symgrad["z"], symgrad["nocc"]
-    g = MolGpu(mol)
-    o = O.Oracle(mol)
-    q = unique_quartets(len(mol.shells))
-    flat, off = g.eri_quartets(q)
-    eri = full_eri_from_blocks(mol, q, flat.cpu().numpy(), off)
-    S, T, V = oneint.one_electron(mol)
-    res = scf.rhf(exact_jk(eri), torch.from_numpy(T + V), torch.from_numpy(S), nocc, oneint.nuclear_repulsion(mol),
-                  e_conv=1e-12, d_conv=1e-10)
-    assert res["converged"]
-    assert abs(res["energy"] - float(z["E_SCF"])) <= 10.0 ** -int(z["E_SCF_digits"])
-    C, eps = res["C"].numpy(), res["eps"].numpy()
-    Co = C[:, :nocc]
-    D, W = 2.0 * Co @ Co.T, 2.0 * (Co * eps[:nocc]) @ Co.T
-    g2 = g.drvg1(torch.from_numpy(D)).cpu().numpy()
-    ref2 = o.grad(D)
-    assert np.abs(g2 - ref2).max() < 1e-9 * max(1.0, np.abs(ref2).max())
-    G = oneint.one_electron_gradient(mol, D, W) + g2 + oneint.nuclear_repulsion_gradient(mol)
-    err = np.abs(G[z["grad_atom"], z["grad_comp"]] - z["GRAD"]).max()
-    print(f"{mol.name} device: max |grad - GRAD| = {err:.1e}")
-    assert err <= 10.0 ** -int(z["GRAD_digits"])
