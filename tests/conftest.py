@@ -95,19 +95,14 @@ def exact_jk(eri):
     return jk
 
 
-@pytest.fixture(scope="session")
-def scf071():
-    """The reference's test 071 (water, cc-pVTZ: s to f shells, no symmetry,
-    conventional integrals, closed-shell SCF), from
-    tests/golden/scf071_h2o_ccpvtz.npz (made by make_scf071_golden.py)."""
-    import numpy as np
-
-    from openmolcas_b200 import basis as B
-
-    z = dict(np.load(os.path.join(ROOT, "tests", "golden", "scf071_h2o_ccpvtz.npz")))
-    mol = B.molecule_from_arrays("h2o_ccpvtz", z["coords"], z["charges"], z["shell_atom"], z["shell_l"],
-                                 z["shell_nprim"], z["shell_ncontr"], z["exps"], z["coefs"])
-    return dict(mol=mol, z=z, nocc=int(round(float(z["charges"].sum()) / 2)))
+@pytest.fixture(params=["scf071_h2o_ccpvtz", "scf004_h2o_anos"])
+def refscf(request):
+    """Conventional closed-shell SCF cases of the reference: test 071 (water,
+    cc-pVTZ, s to f shells, no symmetry) and test 004 (water, ANO-S 3s2p1d /
+    2s1p general contractions, C2v in the reference, all atoms here), from
+    tests/golden/<name>.npz (made by make_scf071_golden.py and
+    make_scf004_golden.py)."""
+    return _symgrad_case(request.param)
 
 
 def _symgrad_case(name):

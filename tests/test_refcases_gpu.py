@@ -44,13 +44,14 @@ def test_rhf_over_device_jk_scf065(scf065):
     assert np.isfinite(res["eps"].cpu().numpy()).all()
 
 
-def test_scf071_ccpvtz_device_eris_and_cholesky(scf071):
-    """The reference's test 071 (water, cc-pVTZ: d and f shells, conventional
-    integrals) through the device: the SCF over every unique shell quartet
-    from mg_eri_quartets, and over mg_cho_drv (ThrCom 1e-9) + mg_cho_jk FP64,
-    both meet E_SCF to the checkfile's 8 digits; the Cholesky SCF equals the
-    same loop over the oracle's vectors to 1e-9."""
-    mol, z, nocc = scf071["mol"], scf071["z"], scf071["nocc"]
+def test_reference_scf_device_eris_and_cholesky(refscf):
+    """The reference's tests 071 (water, cc-pVTZ: d and f shells) and 004
+    (water, ANO-S general contractions), conventional integrals, through the
+    device: the SCF over every unique shell quartet from mg_eri_quartets, and
+    over mg_cho_drv (ThrCom 1e-9) + mg_cho_jk FP64, both meet E_SCF to the
+    checkfile's 8 digits; the Cholesky SCF equals the same loop over the
+    oracle's vectors to 1e-9."""
+    mol, z, nocc = refscf["mol"], refscf["z"], refscf["nocc"]
     S, T, V = oneint.one_electron(mol)
     enuc = oneint.nuclear_repulsion(mol)
     bar = 10.0 ** -int(z["E_SCF_digits"])
@@ -74,7 +75,7 @@ def test_scf071_ccpvtz_device_eris_and_cholesky(scf071):
         return torch.from_numpy(J), torch.from_numpy(K)
 
     r3 = scf.rhf(jk, h, Sm, nocc, enuc, e_conv=1e-12, d_conv=1e-10)
-    print(f"071 device: ERIs {r1['energy']:.12f}, Cholesky {r2['energy']:.12f}, E_SCF {float(z['E_SCF']):.12f}")
+    print(f"{mol.name} device: ERIs {r1['energy']:.12f}, Cholesky {r2['energy']:.12f}, E_SCF {float(z['E_SCF']):.12f}")
     assert r2["converged"] and abs(r2["energy"] - float(z["E_SCF"])) <= bar
     assert abs(r2["energy"] - r3["energy"]) < 1e-9
 

@@ -52,18 +52,19 @@ def _rhf_071(mol, nocc, jk):
                    e_conv=1e-12, d_conv=1e-10)
 
 
-def test_scf071_ccpvtz_energy_exact_and_cholesky(scf071):
-    """The reference's test 071 (water, cc-pVTZ with d and f shells,
-    conventional integrals): the SCF over the oracle's exact ERIs meets E_SCF
-    (checked to 8 digits by the reference harness) and POTNUC (12 digits);
-    over Cholesky vectors at ThrCom 1e-9 it stays within the same 1e-8."""
+def test_reference_scf_energy_exact_and_cholesky(refscf):
+    """The reference's tests 071 (water, cc-pVTZ with d and f shells) and 004
+    (water, ANO-S general contractions), conventional integrals: the SCF over
+    the oracle's exact ERIs meets E_SCF (checked to 8 digits by the reference
+    harness) and POTNUC (12 digits); over Cholesky vectors at ThrCom 1e-9 it
+    stays within the same 1e-8."""
     from conftest import exact_jk
-    mol, z, nocc = scf071["mol"], scf071["z"], scf071["nocc"]
+    mol, z, nocc = refscf["mol"], refscf["z"], refscf["nocc"]
     assert abs(oneint.nuclear_repulsion(mol) - float(z["POTNUC"])) <= 10.0 ** -int(z["POTNUC_digits"])
     o = O.Oracle(mol)
     bar = 10.0 ** -int(z["E_SCF_digits"])
     res = _rhf_071(mol, nocc, exact_jk(o.eri_full()))
-    print(f"071: E = {res['energy']:.12f}  E_SCF = {float(z['E_SCF']):.12f}")
+    print(f"{mol.name}: E = {res['energy']:.12f}  E_SCF = {float(z['E_SCF']):.12f}")
     assert res["converged"] and abs(res["energy"] - float(z["E_SCF"])) <= bar
     L = o.cholesky(thrcom=1e-9)["L"]
 
