@@ -50,7 +50,7 @@ def test_reference_scf_device_eris_and_cholesky(refscf):
     device: the SCF over every unique shell quartet from mg_eri_quartets, and
     over mg_cho_drv (ThrCom 1e-9) + mg_cho_jk FP64, both meet E_SCF to the
     checkfile's 8 digits; the Cholesky SCF equals the same loop over the
-    oracle's vectors to 1e-9."""
+    oracle's vectors to 1e-8 (1e-10 relative: the FP64 J/K parity bar)."""
     mol, z, nocc = refscf["mol"], refscf["z"], refscf["nocc"]
     S, T, V = oneint.one_electron(mol)
     enuc = oneint.nuclear_repulsion(mol)
@@ -77,7 +77,7 @@ def test_reference_scf_device_eris_and_cholesky(refscf):
     r3 = scf.rhf(jk, h, Sm, nocc, enuc, e_conv=1e-12, d_conv=1e-10)
     print(f"{mol.name} device: ERIs {r1['energy']:.12f}, Cholesky {r2['energy']:.12f}, E_SCF {float(z['E_SCF']):.12f}")
     assert r2["converged"] and abs(r2["energy"] - float(z["E_SCF"])) <= bar
-    assert abs(r2["energy"] - r3["energy"]) < 1e-9
+    assert abs(r2["energy"] - r3["energy"]) < 1e-8
 
 
 def test_grad862_device_eris_and_drvg1_against_reference(grad862):
