@@ -26,6 +26,7 @@
 #include <cstdio>
 #include <vector>
 
+#include "cho_qualify.h"
 #include "mg_internal.h"
 
 namespace mg {
@@ -438,10 +439,7 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
       if (v > smax) { smax = v; spab = sp; }
     }
     if (smax == 0.0 || std::fabs(smax) < diamin) { rc = MG_ERR_DECOMP; err = "no qualifying diagonal (Cho_GetInt 104)"; break; }
-    // ---- Cho_Qualify_2 within shell pair spab: the reduced-set diagonals
-    // >= DiaMin in order; once MaxQual are taken, a larger one replaces the
-    // smallest taken (the first of equal smallest); MaxQual = 1 takes the
-    // largest (the last of equal largest)
+    // ---- Cho_Qualify_2 within shell pair spab (cho_qualify.h)
     const int64_t f = c->sp_first[spab];
     const int cnt = c->sp_count[spab];
     std::vector<double> dpair(cnt);
@@ -449,26 +447,8 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
     cudaMemcpyAsync(dpair.data(), c->d_diag + f, sizeof(double) * cnt, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(rpair.data(), c->d_inred + f, cnt, cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
-    std::vector<int> qual;  // positions t inside the pair, then rs indices
-    if (cfg.maxqual == 1) {
-      double xmax = diamin;
-      int imax = -1;
-      for (int t = 0; t < cnt; ++t)
-        if (rpair[t] && dpair[t] >= xmax) { xmax = dpair[t]; imax = t; }
-      if (imax >= 0) qual.push_back(imax);
-    } else {
-      for (int t = 0; t < cnt; ++t) {
-        if (!rpair[t] || !(dpair[t] >= diamin)) continue;
-        if ((int)qual.size() < cfg.maxqual) {
-          qual.push_back(t);
-        } else {
-          size_t kmin = 0;
-          for (size_t k = 1; k < qual.size(); ++k)
-            if (dpair[qual[k]] < dpair[qual[kmin]]) kmin = k;
-          if (dpair[t] > dpair[qual[kmin]]) qual[kmin] = t;
-        }
-      }
-    }
+    // positions t inside the pair, then rs indices
+    std::vector<int> qual = cho_qualify_2(dpair.data(), rpair.data(), cnt, diamin, cfg.maxqual);
     for (int& t : qual) t = (int)(f + t);
     const int nq = qual.size();
     if (nq == 0) { rc = MG_ERR_DECOMP; err = "empty qualification (Cho_GetInt 104)"; break; }
