@@ -19,6 +19,7 @@
 #include <mutex>
 #include <vector>
 
+#include "../../include/molgpu.h"  // the definition below is checked against its declaration
 #include "mg_internal.h"
 
 namespace mg {
