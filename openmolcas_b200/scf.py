@@ -40,11 +40,17 @@ def rhf(jk: Callable[[torch.Tensor], tuple], h: torch.Tensor, S: torch.Tensor, n
     Returns dict(energy, C (nbf x nmo), eps (nmo), niter, converged, history):
     ``energy`` is E_SCF of the last density, ``history`` the energy per
     iteration.  Converged when the energy change is below ``e_conv`` and the
-    largest element of the orthogonalised commutator below ``d_conv``."""
+    largest element of the orthogonalised commutator below ``d_conv``.
+    Raises ValueError when nocc exceeds the orbitals left after dropping
+    near-linear dependencies or maxiter < 1."""
+    if maxiter < 1:
+        raise ValueError("rhf: maxiter must be >= 1")
     dev, dt = h.device, torch.float64
     h = h.to(dev, dt)
     S = S.to(dev, dt)
     X = _orthogonaliser(S, lindep)
+    if not 0 < nocc <= X.shape[1]:
+        raise ValueError(f"rhf: {nocc} occupied orbitals, {X.shape[1]} linearly independent functions")
 
     def diag(F):
         eps, Ct = torch.linalg.eigh(X.T @ F @ X)
@@ -88,8 +94,11 @@ def rhf(jk: Callable[[torch.Tensor], tuple], h: torch.Tensor, S: torch.Tensor, n
             Bm[n, n] = 0.0
             rhs = torch.zeros(n + 1, dtype=dt, device=dev)
             rhs[n] = -1.0
-            c = torch.linalg.solve(Bm, rhs)[:n]
-            F = sum(ci * Fi for ci, Fi in zip(c, fock_hist))
+            try:
+                c = torch.linalg.solve(Bm, rhs)[:n]
+                F = sum(ci * Fi for ci, Fi in zip(c, fock_hist))
+            except RuntimeError:  # singular subspace: restart it from the newest Fock matrix
+                del fock_hist[:-1], err_hist[:-1]
         eps, C = diag(F)
         Cocc = C[:, :nocc]
     return dict(energy=energies[-1], C=C, eps=eps, niter=len(energies), converged=converged, history=energies)

@@ -74,3 +74,19 @@ def test_reference_scf_energy_exact_and_cholesky(refscf):
 
     rc = _rhf_071(mol, nocc, jk)
     assert rc["converged"] and abs(rc["energy"] - float(z["E_SCF"])) <= bar
+
+
+def test_rhf_rejects_bad_arguments():
+    import pytest
+    h = torch.eye(3, dtype=torch.float64)
+    S = torch.eye(3, dtype=torch.float64)
+
+    def jk(Cf):
+        return torch.zeros(3, 3, dtype=torch.float64), torch.zeros(3, 3, dtype=torch.float64)
+
+    with pytest.raises(ValueError):
+        scf.rhf(jk, h, S, 4, 0.0)
+    with pytest.raises(ValueError):
+        scf.rhf(jk, h, S, 1, 0.0, maxiter=0)
+    res = scf.rhf(jk, h, S, 2, 1.0)  # no two-electron term: E = 2 * 2 * 1 + 1
+    assert res["converged"] and abs(res["energy"] - 5.0) < 1e-12
