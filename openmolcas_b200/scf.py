@@ -102,3 +102,89 @@ def rhf(jk: Callable[[torch.Tensor], tuple], h: torch.Tensor, S: torch.Tensor, n
         eps, C = diag(F)
         Cocc = C[:, :nocc]
     return dict(energy=energies[-1], C=C, eps=eps, niter=len(energies), converged=converged, history=energies)
+
+
+def uhf(jk: Callable[[torch.Tensor], tuple], h: torch.Tensor, S: torch.Tensor, nalpha: int, nbeta: int,
+        enuc: float, C0: Optional[tuple] = None, e_conv: float = 1e-10, d_conv: float = 1e-8, maxiter: int = 200,
+        ndiis: int = 8, lindep: float = 1e-9) -> dict:
+    """Unrestricted SCF (the reference's ``UHF`` keyword of &SCF): separate
+    alpha and beta orbitals, F_s = h + J[D_a + D_b] - K[D_s], two jk calls per
+    iteration, one DIIS over both spin commutators.
+
+    E = 1/2 tr((D_a + D_b) h) + 1/2 tr(D_a F_a) + 1/2 tr(D_b F_b) + enuc; its
+    two-electron part equals 1/2 tr(D J[D]) - 1/4 (tr(D K[D]) + tr(DS K[DS]))
+    with D = D_a + D_b and DS = D_a - D_b, the 2-PDM of PGet1 with the spin
+    density, i.e. what ``mg_drvg1_x(h, D, DS, 1, 1, ...)`` differentiates.
+    Returns dict(energy, C=(C_a, C_b), eps=(eps_a, eps_b), niter, converged,
+    history)."""
+    if maxiter < 1:
+        raise ValueError("uhf: maxiter must be >= 1")
+    dev, dt = h.device, torch.float64
+    h = h.to(dev, dt)
+    S = S.to(dev, dt)
+    X = _orthogonaliser(S, lindep)
+    if not (0 <= nbeta <= nalpha <= X.shape[1] and nalpha > 0):
+        raise ValueError(f"uhf: {nalpha} alpha / {nbeta} beta electrons, {X.shape[1]} linearly independent functions")
+    nocc = (nalpha, nbeta)
+
+    def diag(F):
+        eps, Ct = torch.linalg.eigh(X.T @ F @ X)
+        return eps, X @ Ct
+
+    if C0 is None:
+        eps0, C = diag(h)
+        Cs = [C, C]
+        eps = [eps0, eps0]
+    else:
+        Cs = [c.to(dev, dt) for c in C0]
+        eps = [None, None]
+    fock_hist, err_hist, energies = [], [], []
+    e_old = None
+    converged = False
+    for it in range(1, maxiter + 1):
+        Ds, Ks = [], []
+        J = torch.zeros_like(h)
+        for s in range(2):
+            Co = Cs[s][:, :nocc[s]]
+            Ds.append(Co @ Co.T)
+            if nocc[s] > 0:
+                Js, Kk = jk(Co)
+                J = J + Js.to(dev, dt)
+                Ks.append(Kk.to(dev, dt))
+            else:
+                Ks.append(torch.zeros_like(h))
+        Fs = [h + J - Ks[s] for s in range(2)]
+        E = float(0.5 * torch.sum((Ds[0] + Ds[1]) * h) + 0.5 * torch.sum(Ds[0] * Fs[0])
+                  + 0.5 * torch.sum(Ds[1] * Fs[1])) + enuc
+        energies.append(E)
+        errs = [X.T @ (Fs[s] @ Ds[s] @ S - S @ Ds[s] @ Fs[s]) @ X for s in range(2)]
+        emax = max(float(e.abs().max()) for e in errs)
+        if e_old is not None and abs(E - e_old) < e_conv and emax < d_conv:
+            converged = True
+            for s in range(2):
+                eps[s], Cs[s] = diag(Fs[s])
+            break
+        e_old = E
+        fock_hist.append(Fs)
+        err_hist.append(errs)
+        del fock_hist[:-ndiis], err_hist[:-ndiis]
+        n = len(fock_hist)
+        if n > 1:
+            Bm = torch.empty((n + 1, n + 1), dtype=dt, device=dev)
+            for i in range(n):
+                for j in range(n):
+                    Bm[i, j] = torch.sum(err_hist[i][0] * err_hist[j][0]) + torch.sum(err_hist[i][1] * err_hist[j][1])
+            Bm[n, :n] = -1.0
+            Bm[:n, n] = -1.0
+            Bm[n, n] = 0.0
+            rhs = torch.zeros(n + 1, dtype=dt, device=dev)
+            rhs[n] = -1.0
+            try:
+                c = torch.linalg.solve(Bm, rhs)[:n]
+                Fs = [sum(ci * Fi[s] for ci, Fi in zip(c, fock_hist)) for s in range(2)]
+            except RuntimeError:  # singular subspace: restart it from the newest Fock matrices
+                del fock_hist[:-1], err_hist[:-1]
+        for s in range(2):
+            eps[s], Cs[s] = diag(Fs[s])
+    return dict(energy=energies[-1], C=tuple(Cs), eps=tuple(eps), niter=len(energies), converged=converged,
+                history=energies)

@@ -90,3 +90,40 @@ def test_rhf_rejects_bad_arguments():
         scf.rhf(jk, h, S, 1, 0.0, maxiter=0)
     res = scf.rhf(jk, h, S, 2, 1.0)  # no two-electron term: E = 2 * 2 * 1 + 1
     assert res["converged"] and abs(res["energy"] - 5.0) < 1e-12
+
+
+def _uhf(mol, na, nb):
+    from conftest import exact_jk
+    S, T, V = oneint.one_electron(mol)
+    o = O.Oracle(mol)
+    return scf.uhf(exact_jk(o.eri_full()), torch.from_numpy(T + V), torch.from_numpy(S), na, nb,
+                   oneint.nuclear_repulsion(mol), e_conv=1e-12, d_conv=1e-10), o
+
+
+def test_uhf_closed_shell_limit_is_scf862(grad862):
+    """With equal alpha and beta occupations UHF is RHF: test 862's E_SCF."""
+    mol, z = grad862["mol"], grad862["z"]
+    res, _ = _uhf(mol, 5, 5)
+    assert res["converged"] and abs(res["energy"] - float(z["E_SCF"])) <= 10.0 ** -int(z["E_SCF_digits"])
+
+
+def test_uhf_gradient_with_spin_density_vs_central_fd(grad862):
+    """H2O+ doublet (5 alpha, 4 beta) in 6-31G: the nuclear gradient from
+    the spin-density 2-PDM (oracle Drvg1 with DS = D_a - D_b, the input of
+    mg_drvg1_x), the one-electron terms with W = sum_s C_s eps_s C_s^T and
+    the nuclear repulsion equals central differences of converged UHF
+    energies."""
+    mol = grad862["mol"]
+    res, o = _uhf(mol, 5, 4)
+    assert res["converged"]
+    (Ca, Cb), (ea, eb) = [c.numpy() for c in res["C"]], [e.numpy() for e in res["eps"]]
+    Da, Db = Ca[:, :5] @ Ca[:, :5].T, Cb[:, :4] @ Cb[:, :4].T
+    W = (Ca[:, :5] * ea[:5]) @ Ca[:, :5].T + (Cb[:, :4] * eb[:4]) @ Cb[:, :4].T
+    G = (oneint.one_electron_gradient(mol, Da + Db, W) + o.grad(Da + Db, DS=Da - Db)
+         + oneint.nuclear_repulsion_gradient(mol))
+    assert np.abs(G.sum(0)).max() < 1e-10
+    h = 1e-4
+    for at, ax in [(0, 2), (1, 0), (2, 2)]:
+        ep = _uhf(mol.moved(at, ax, h), 5, 4)[0]["energy"]
+        em = _uhf(mol.moved(at, ax, -h), 5, 4)[0]["energy"]
+        assert abs((ep - em) / (2 * h) - G[at, ax]) < 1e-7
