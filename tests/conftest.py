@@ -126,3 +126,11 @@ def symgrad(request):
     make_symgrad_golden.py).  GRAD[i] is the component grad_comp[i] of atom
     grad_atom[i] (the symmetry-allowed components of the unique centres)."""
     return _symgrad_case(request.param)
+
+
+@pytest.fixture(params=["grad020_ch4_ccpvdz", "grad023_ch2o2_ccpvdz", "grad019_c4h8_sto3g",
+                        "grad021_c6h6_sto3g"])
+def symgrad_all(request):
+    """symgrad plus the reference's tests 019 (C4H8, STO-3G, generators z y x)
+    and 021 (benzene, STO-3G, generators x y z), same layout."""
+    return _symgrad_case(request.param)

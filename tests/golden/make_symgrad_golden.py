@@ -1,6 +1,7 @@
 """Generate a gradient fixture from one of the reference's SCF + Alaska tests
 that use point-group symmetry (tests/golden/grad020_ch4_ccpvdz.npz from test
-020, tests/golden/grad023_ch2o2_ccpvdz.npz from test 023).
+020, tests/golden/grad023_ch2o2_ccpvdz.npz from test 023, and tests 019, 021
+and 049 likewise).
 
 Test 020 optimises CH4 in cc-pVDZ with the symmetry generators ``x z`` (C2v),
 test 023 a CH2O2 transition state in cc-pVDZ with the generator ``Y`` (Cs);
@@ -24,6 +25,9 @@ index of each atom's unique centre, and for every GRAD entry the atom and
 component it belongs to.  Run in a container that has the reference tree:
     python tests/golden/make_symgrad_golden.py /path/to/OpenMolcas 020 grad020_ch4_ccpvdz
     python tests/golden/make_symgrad_golden.py /path/to/OpenMolcas 023 grad023_ch2o2_ccpvdz
+    python tests/golden/make_symgrad_golden.py /path/to/OpenMolcas 019 grad019_c4h8_sto3g
+    python tests/golden/make_symgrad_golden.py /path/to/OpenMolcas 021 grad021_c6h6_sto3g
+    python tests/golden/make_symgrad_golden.py /path/to/OpenMolcas 049 grad049_ch2o2_ccpvdz
 """
 from __future__ import annotations
 
