@@ -105,6 +105,13 @@ def refscf(request):
     return _symgrad_case(request.param)
 
 
+@pytest.fixture(params=["scf071_h2o_ccpvtz", "scf004_h2o_anos", "scf007_ch2_inline"])
+def refscf_all(request):
+    """refscf plus the reference's test 007 (singlet CH2 with an inline
+    cc-pVTZ-type basis without f, C2v in the reference; make_scf007_golden.py)."""
+    return _symgrad_case(request.param)
+
+
 def _symgrad_case(name):
     import numpy as np
 

@@ -52,14 +52,15 @@ def _rhf_071(mol, nocc, jk):
                    e_conv=1e-12, d_conv=1e-10)
 
 
-def test_reference_scf_energy_exact_and_cholesky(refscf):
-    """The reference's tests 071 (water, cc-pVTZ with d and f shells) and 004
-    (water, ANO-S general contractions), conventional integrals: the SCF over
+def test_reference_scf_energy_exact_and_cholesky(refscf_all):
+    """The reference's tests 071 (water, cc-pVTZ with d and f shells), 004
+    (water, ANO-S general contractions) and 007 (CH2, inline basis),
+    conventional integrals: the SCF over
     the oracle's exact ERIs meets E_SCF (checked to 8 digits by the reference
     harness) and POTNUC (12 digits); over Cholesky vectors at ThrCom 1e-9 it
     stays within the same 1e-8."""
     from conftest import exact_jk
-    mol, z, nocc = refscf["mol"], refscf["z"], refscf["nocc"]
+    mol, z, nocc = refscf_all["mol"], refscf_all["z"], refscf_all["nocc"]
     assert abs(oneint.nuclear_repulsion(mol) - float(z["POTNUC"])) <= 10.0 ** -int(z["POTNUC_digits"])
     o = O.Oracle(mol)
     bar = 10.0 ** -int(z["E_SCF_digits"])
