@@ -99,3 +99,18 @@ def test_scf049_ch2o2_energy():
     res, _, _ = _scf(mol, O.Oracle(mol).eri_full(), nocc)
     assert res["converged"]
     assert abs(res["energy"] - float(z["E_SCF"])) <= 10.0 ** -int(z["E_SCF_digits"])
+
+
+def test_grad094_hcn_sto3g_energy_and_gradient():
+    """The reference's test 094 (HCN/CNH, STO-3G, no symmetry; &SCF then
+    &SLAPAF, which has Alaska compute the SCF gradient): E_SCF to its 8 digits
+    and the first GRAD to its 6 digits."""
+    from conftest import _symgrad_case
+    c = _symgrad_case("scf094_hcn_sto3g")
+    mol, z, nocc = c["mol"], c["z"], c["nocc"]
+    o = O.Oracle(mol)
+    res, D, W = _scf(mol, o.eri_full(), nocc)
+    assert res["converged"]
+    assert abs(res["energy"] - float(z["E_SCF"])) <= 10.0 ** -int(z["E_SCF_digits"])
+    G = oneint.one_electron_gradient(mol, D, W) + o.grad(D) + oneint.nuclear_repulsion_gradient(mol)
+    assert np.abs(G - z["GRAD"]).max() <= 10.0 ** -int(z["GRAD_digits"])
