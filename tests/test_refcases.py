@@ -1,8 +1,8 @@
-"""The reference's test 862 (water, 6-31G, no symmetry, conventional
-integrals): SCF energy and nuclear gradient of the first geometry against its
-checkfile, with the oracle's ERIs, one-electron matrices and Drvg1
-restatement, and the SCF loop of openmolcas_b200/scf.py.  The bars are the
-reference harness's own (E_SCF 8 digits, GRAD 6 digits;
+"""SCF energies and nuclear gradients against the reference's regression
+tests (the checkfile values of tests 862, 020, 023, 019, 021, 049 and 094; the
+energy-only cases are in test_scf.py), with the oracle's ERIs, one-electron
+matrices and Drvg1 restatement, and the SCF loop of openmolcas_b200/scf.py.
+The bars are the reference harness's own (E_SCF 8 digits, GRAD 6 digits;
 Tools/pymolcas/check_test.py:137-151)."""
 import numpy as np
 import torch
