@@ -106,12 +106,13 @@ def refscf(request):
 
 
 @pytest.fixture(params=["scf071_h2o_ccpvtz", "scf004_h2o_anos", "scf007_ch2_inline", "scf078_h2o2_631g",
-                        "scf090_sto3g", "scf094_hcn_sto3g", "scf095_hcn_sto3g"])
+                        "scf090_sto3g", "scf094_hcn_sto3g", "scf095_hcn_sto3g", "scf099_c2h2o3_631g"])
 def refscf_all(request):
     """refscf plus the reference's tests 007 (singlet CH2 with an inline
     cc-pVTZ-type basis without f, C2v in the reference; make_scf007_golden.py),
-    078 (water dimer, 6-31G), 090 (STO-3G), 094 and 095 (HCN/CNH, STO-3G), the
-    last four from XYZ geometries (make_xyz_golden.py)."""
+    078 (water dimer, 6-31G), 090 (STO-3G), 094 and 095 (HCN/CNH, STO-3G) and
+    099 (1,2-dioxetanone, 6-31G, from its embedded orbitals), the last five
+    from XYZ geometries (make_xyz_golden.py)."""
     return _symgrad_case(request.param)
 
 

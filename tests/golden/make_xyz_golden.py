@@ -1,7 +1,10 @@
 """Generate a fixture from one of the reference's no-symmetry tests whose
 &GATEWAY gives the geometry as an XYZ block in angstrom and one basis label
 for every atom: tests 078 (water dimer, 6-31G), 090 (STO-3G), 094 and 095
-(HCN/CNH, STO-3G).  GRAD, when the checkfile has one, is its first gradient:
+(HCN/CNH, STO-3G), and 099 (1,2-dioxetanone, 6-31G), whose &SCF starts from
+an orbital file the input embeds (``FILE = name``: INPORB, ``#ORB`` vectors
+and ``#OCC`` occupations, stored as ``orbitals`` and ``occupation``).  GRAD,
+when the checkfile has one and the test checks it, is its first gradient:
 the SCF gradient of the first geometry for 094 (&SCF then &SLAPAF), an MP2
 gradient for 078 and 090 (&MBPT2 before &SLAPAF).
 
@@ -15,7 +18,8 @@ reproduces POTNUC (make_scf071_golden.py), and the first POTNUC, E_SCF and,
 when present, GRAD of the checkfile.  Run in a container that has the
 reference tree:
     python tests/golden/make_xyz_golden.py /path/to/OpenMolcas 094 scf094_hcn_sto3g
-(and 078 scf078_h2o2_631g, 090 scf090_sto3g, 095 scf095_hcn_sto3g).
+(and 078 scf078_h2o2_631g, 090 scf090_sto3g, 095 scf095_hcn_sto3g,
+099 scf099_c2h2o3_631g).
 """
 from __future__ import annotations
 
@@ -69,16 +73,38 @@ def read_input(path):
             geo = atom_lines(body[2:], n)
         break
     basis = next(re.split(r"=", ln, 1)[1].strip() for ln in lines if re.match(r"\s*basis\s*=", ln, re.I))
+    orbs = None
+    for ln in lines:
+        m = re.match(r"\s*file\s*=\s*(\S+)", ln, re.I)
+        if m and m.group(1) in files and files[m.group(1)][0].startswith("#INPORB"):
+            orbs = read_inporb(files[m.group(1)])
     chk = {}
     for ln in lines:
         m = re.match(r'#> ([\w\[\]]+)="([-0-9.eE+]+)"/(\d+)', ln)
         if m and m.group(1) not in chk:
             chk[m.group(1)] = (float(m.group(2)), int(m.group(3)))
-    return geo, basis, chk
+    nocheck = any(re.search(r"MOLCAS_NOCHECK=.*GRAD", ln) for ln in lines)
+    return geo, basis, chk, orbs, nocheck
+
+
+def read_inporb(body):
+    """(orbitals [norb, nbf], occupations) of an INPORB 2.x file, one symmetry."""
+    i0 = body.index("#ORB")
+    i1 = next(i for i, ln in enumerate(body) if ln.startswith("#OCC"))
+    i2 = next(i for i, ln in enumerate(body) if i > i1 and ln.startswith("#") and not ln.startswith("#OCC"))
+    orbs, cur = [], None
+    for ln in body[i0 + 1:i1]:
+        if ln.startswith("* ORBITAL"):
+            cur = []
+            orbs.append(cur)
+        elif not ln.startswith("*"):
+            cur.extend(float(v) for v in ln.split())
+    occ = [float(v) for ln in body[i1 + 1:i2] if not ln.startswith("*") for v in ln.split()]
+    return np.array(orbs), np.array(occ)
 
 
 def main(ref, test_id, name):
-    (els, xyz), basis, chk = read_input(os.path.join(ref, "test", "standard", test_id + ".input"))
+    (els, xyz), basis, chk, orbs, nocheck = read_input(os.path.join(ref, "test", "standard", test_id + ".input"))
     xyz = np.array(xyz)
     q = np.array([CHARGE[e.upper()] for e in els])
     best = None
@@ -109,7 +135,9 @@ def main(ref, test_id, name):
     for key in ("POTNUC", "E_SCF"):
         out[key] = np.array(chk[key][0])
         out[key + "_digits"] = np.array(chk[key][1])
-    if "GRAD[0]" in chk:
+    if orbs is not None:
+        out["orbitals"], out["occupation"] = orbs
+    if "GRAD[0]" in chk and not nocheck:
         out["GRAD"] = np.array([chk[f"GRAD[{i}]"][0] for i in range(3 * len(els))]).reshape(-1, 3)
         out["GRAD_digits"] = np.array(chk["GRAD[0]"][1])
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), name + ".npz")

@@ -46,10 +46,13 @@ def test_rhf_converges_to_scf065_energy(scf065):
     assert abs(res2["energy"] - res["energy"]) < 1e-9
 
 
-def _rhf_071(mol, nocc, jk):
+def _rhf_ref(mol, nocc, jk, z):
+    """SCF from a core guess, or from the orbitals the reference test embeds
+    (``orbitals`` in the fixture), as that test's &SCF starts."""
     S, T, V = oneint.one_electron(mol)
+    C0 = torch.from_numpy(z["orbitals"].T.copy()) if "orbitals" in z else None
     return scf.rhf(jk, torch.from_numpy(T + V), torch.from_numpy(S), nocc, oneint.nuclear_repulsion(mol),
-                   e_conv=1e-12, d_conv=1e-10)
+                   C0=C0, e_conv=1e-12, d_conv=1e-10)
 
 
 def test_reference_scf_energy_exact_and_cholesky(refscf_all):
@@ -64,7 +67,7 @@ def test_reference_scf_energy_exact_and_cholesky(refscf_all):
     assert abs(oneint.nuclear_repulsion(mol) - float(z["POTNUC"])) <= 10.0 ** -int(z["POTNUC_digits"])
     o = O.Oracle(mol)
     bar = 10.0 ** -int(z["E_SCF_digits"])
-    res = _rhf_071(mol, nocc, exact_jk(o.eri_full()))
+    res = _rhf_ref(mol, nocc, exact_jk(o.eri_full()), z)
     print(f"{mol.name}: E = {res['energy']:.12f}  E_SCF = {float(z['E_SCF']):.12f}")
     assert res["converged"] and abs(res["energy"] - float(z["E_SCF"])) <= bar
     L = o.cholesky(thrcom=1e-9)["L"]
@@ -73,7 +76,7 @@ def test_reference_scf_energy_exact_and_cholesky(refscf_all):
         J, K = o.cho_jk(L, Cf.numpy())
         return torch.from_numpy(J), torch.from_numpy(K)
 
-    rc = _rhf_071(mol, nocc, jk)
+    rc = _rhf_ref(mol, nocc, jk, z)
     assert rc["converged"] and abs(rc["energy"] - float(z["E_SCF"])) <= bar
 
 
