@@ -1,6 +1,6 @@
 """The differentiable J/K energy: backward (the gradient kernel and
 dE/dC = 2(J - K/2)C) against central finite differences of the forward
-(h = 1e-4 bohr, north-star bar 1e-6 Eh/bohr), and mg_rys_roots (the device
+(h = 1e-4 bohr, bar 1e-6 Eh/bohr), and mg_rys_roots (the device
 table evaluation) against the reference's own Rys table values."""
 import os
 

@@ -1,7 +1,7 @@
 """GPU two-electron gradient (adjoint Rys kernel) against the CPU oracle
 (which is itself pinned to central finite differences in test_oracle.py).
 
-Bars: the north-star gradient bar, 1e-6 Eh/bohr, for the synthetic bases
+Bars: the 1e-6 Eh/bohr gradient bar for the synthetic bases
 with random general contractions over exponents 0.08..14171 (the 2D HRR
 transfer between such primitives 5 bohr apart cancels by many orders, so any
 two FP64 implementations differ at 1e-8..1e-7 there); 1e-9 relative for the
