@@ -173,6 +173,10 @@ int mg_rys_roots(mg_handle* h, int nrys, int64_t n, const double* T, double* x, 
 /* Number of kernels of this library launched so far in this process (library
  * calls such as cuBLAS are not counted).  No reference counterpart. */
 long long mg_kernel_launches(void);
+/* Number of device allocations (cudaMalloc) this library has made so far in
+ * this process, all handles together (allocations inside cuBLAS are not
+ * counted).  No reference counterpart. */
+long long mg_device_allocations(void);
 
 #ifdef __cplusplus
 }

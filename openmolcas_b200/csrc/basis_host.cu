@@ -66,7 +66,7 @@ int load_rys_table(Handle* h, const char* path) {
   std::vector<double> coef(off);
   if (fread(coef.data(), 8, off, f) != (size_t)off) { fclose(f); h->err = "truncated Rys table"; return 5; }
   fclose(f);
-  if (cudaMalloc(&h->d_rys, sizeof(double) * off) != cudaSuccess) { h->err = "cudaMalloc rys"; return 6; }
+  if (dev_malloc(&h->d_rys, sizeof(double) * off) != cudaSuccess) { h->err = "cudaMalloc rys"; return 6; }
   cudaMemcpy(h->d_rys, coef.data(), sizeof(double) * off, cudaMemcpyHostToDevice);
   return 0;
 }
@@ -284,10 +284,10 @@ int setup_pairs(Handle* h) {
   for (size_t i = 0; i < zeta.size(); ++i) izeta[i] = 1.0 / zeta[i];
   std::vector<double> prim;
   for (auto* v : {&zeta, &kappa, &px, &py, &pz, &al, &be, &izeta}) prim.insert(prim.end(), v->begin(), v->end());
-  if (cudaMalloc(&h->d_prim, sizeof(double) * prim.size()) != cudaSuccess ||
-      cudaMalloc(&h->d_coef, sizeof(double) * std::max<size_t>(coef.size(), 1)) != cudaSuccess ||
-      cudaMalloc(&h->d_hrr, sizeof(double) * std::max<size_t>(hrr.size(), 1)) != cudaSuccess ||
-      cudaMalloc(&h->d_pairs, sizeof(DPair) * h->pairs.size()) != cudaSuccess) {
+  if (dev_malloc(&h->d_prim, sizeof(double) * prim.size()) != cudaSuccess ||
+      dev_malloc(&h->d_coef, sizeof(double) * std::max<size_t>(coef.size(), 1)) != cudaSuccess ||
+      dev_malloc(&h->d_hrr, sizeof(double) * std::max<size_t>(hrr.size(), 1)) != cudaSuccess ||
+      dev_malloc(&h->d_pairs, sizeof(DPair) * h->pairs.size()) != cudaSuccess) {
     h->err = "cudaMalloc pair data";
     return 1;
   }
@@ -307,7 +307,7 @@ void* ws_get(Handle* h, size_t bytes, cudaStream_t st) {
   h->ws.ptr = nullptr;
   h->ws.size = 0;
   size_t sz = std::max(bytes, (size_t)1 << 20);
-  if (cudaMalloc(&h->ws.ptr, sz) != cudaSuccess) return nullptr;
+  if (dev_malloc(&h->ws.ptr, sz) != cudaSuccess) return nullptr;
   h->ws.size = sz;
   return h->ws.ptr;
 }

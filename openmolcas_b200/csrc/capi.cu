@@ -16,6 +16,7 @@ struct mg_handle {
 
 namespace mg {
 std::atomic<long long> g_launches{0};
+std::atomic<long long> g_allocs{0};
 
 // Accumulator budget (doubles) of one work item: nc * nef <= this.
 static const int kAccBudget = 12288;
@@ -99,7 +100,7 @@ int build_eri_items(Handle* h, const int32_t* q4, int64_t nq, const int64_t* off
 int run_eri_items(Handle* h, const std::vector<EriItem>& items, const std::vector<EriClass>& classes, double* d_out,
                   cudaStream_t st) {
   if (items.empty()) return 0;
-  if (!h->d_eri_counters && cudaMalloc(&h->d_eri_counters, sizeof(int) * 64) != cudaSuccess) {
+  if (!h->d_eri_counters && dev_malloc(&h->d_eri_counters, sizeof(int) * 64) != cudaSuccess) {
     h->err = "ERI work counters: allocation failed";
     return MG_ERR_MEMORY;
   }
@@ -315,7 +316,7 @@ int mg_schwarz(mg_handle* H, double* tmax) {
     std::vector<int64_t> off(nq + 1);
     mg_eri_quartets_size(H, q.data(), nq, off.data());
     double* d_out = nullptr;
-    if (cudaMalloc(&d_out, sizeof(double) * std::max<int64_t>(off[nq], 1)) != cudaSuccess) {
+    if (dev_malloc(&d_out, sizeof(double) * std::max<int64_t>(off[nq], 1)) != cudaSuccess) {
       h->err = "cudaMalloc Schwarz";
       return MG_ERR_MEMORY;
     }
@@ -445,6 +446,7 @@ int mg_cho_jk(mg_handle* H, const double* d_C, int r, double* d_J, double* d_K, 
 }
 
 long long mg_kernel_launches(void) { return g_launches.load(); }
+long long mg_device_allocations(void) { return g_allocs.load(); }
 
 int mg_rys_roots(mg_handle* H, int nrys, int64_t n, const double* T, double* x, double* w) {
   if (!H || nrys < 1 || nrys > MG_MAX_RYS || n < 0 || (n && (!T || !x || !w))) return MG_ERR_ARG;
@@ -458,7 +460,7 @@ int mg_rys_roots(mg_handle* H, int nrys, int64_t n, const double* T, double* x, 
   if (cudaSetDevice(h->device) != cudaSuccess) return MG_ERR_CUDA;
   double* d = nullptr;
   const size_t bytes = sizeof(double) * (size_t)n * (1 + 2 * nrys);
-  if (cudaMalloc(&d, bytes) != cudaSuccess) {
+  if (dev_malloc(&d, bytes) != cudaSuccess) {
     h->err = "mg_rys_roots: device allocation failed";
     return MG_ERR_MEMORY;
   }

@@ -259,15 +259,15 @@ static void make_rs(Handle* h, ChoState* c) {
       c->sp_count.push_back((int)(c->rs_a.size() - c->sp_first.back()));
     }
   c->nrs = c->rs_a.size();
-  cudaMalloc(&c->d_rs_a, sizeof(int) * c->nrs);
-  cudaMalloc(&c->d_rs_b, sizeof(int) * c->nrs);
+  dev_malloc(&c->d_rs_a, sizeof(int) * c->nrs);
+  dev_malloc(&c->d_rs_b, sizeof(int) * c->nrs);
   cudaMemcpy(c->d_rs_a, c->rs_a.data(), sizeof(int) * c->nrs, cudaMemcpyHostToDevice);
   cudaMemcpy(c->d_rs_b, c->rs_b.data(), sizeof(int) * c->nrs, cudaMemcpyHostToDevice);
-  cudaMalloc(&c->d_rs, sizeof(RsDev) * c->nrs);
+  dev_malloc(&c->d_rs, sizeof(RsDev) * c->nrs);
   cudaMemcpy(c->d_rs, rsd.data(), sizeof(RsDev) * c->nrs, cudaMemcpyHostToDevice);
-  cudaMalloc(&c->d_sp_first, sizeof(int64_t) * c->sp_first.size());
+  dev_malloc(&c->d_sp_first, sizeof(int64_t) * c->sp_first.size());
   cudaMemcpy(c->d_sp_first, c->sp_first.data(), sizeof(int64_t) * c->sp_first.size(), cudaMemcpyHostToDevice);
-  cudaMalloc(&c->d_sp_count, sizeof(int) * c->sp_count.size());
+  dev_malloc(&c->d_sp_count, sizeof(int) * c->sp_count.size());
   cudaMemcpy(c->d_sp_count, c->sp_count.data(), sizeof(int) * c->sp_count.size(), cudaMemcpyHostToDevice);
 }
 
@@ -286,7 +286,7 @@ static double* eri_blocks(Handle* h, const std::vector<int32_t>& q4, std::vector
     cudaStreamSynchronize(st);
     cudaFree(buf);
     buf = nullptr;
-    if (cudaMalloc(&buf, need) != cudaSuccess) { rc = MG_ERR_MEMORY; bufsz = 0; return nullptr; }
+    if (dev_malloc(&buf, need) != cudaSuccess) { rc = MG_ERR_MEMORY; bufsz = 0; return nullptr; }
     bufsz = need;
   }
   std::vector<EriItem> items;
@@ -367,11 +367,11 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
   const double damp = cho_default_damp(cfg.thrcom);
   if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS) { err = "cublasCreate failed"; return MG_ERR_CUDA; }
   cublasSetStream(c->cublas, st);
-  cudaMalloc(&c->d_diag, sizeof(double) * nrs);
-  cudaMalloc(&c->d_diag0, sizeof(double) * nrs);
-  cudaMalloc(&c->d_inred, nrs);
+  dev_malloc(&c->d_diag, sizeof(double) * nrs);
+  dev_malloc(&c->d_diag0, sizeof(double) * nrs);
+  dev_malloc(&c->d_inred, nrs);
   double* d_tmp = nullptr;
-  cudaMalloc(&d_tmp, sizeof(double) * std::max<int64_t>(2 * 296, nsp));
+  dev_malloc(&d_tmp, sizeof(double) * std::max<int64_t>(2 * 296, nsp));
   double* buf = nullptr;
   size_t bufsz = 0;
   int rc = 0;
@@ -386,7 +386,7 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
     eri_blocks(h, q4, off, buf, bufsz, st, rc);
     if (rc) { err = "diagonal integrals failed"; cudaFree(buf); cudaFree(d_tmp); return rc; }
     int64_t* d_off = nullptr;
-    cudaMalloc(&d_off, sizeof(int64_t) * nsp);
+    dev_malloc(&d_off, sizeof(int64_t) * nsp);
     cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * nsp, cudaMemcpyHostToDevice, st);
     k_extract_diag<<<nblk(nrs), 256, 0, st>>>(c->d_rs, nrs, h->d_pairs, d_off, buf, c->d_diag0);
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -405,21 +405,21 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
   int* d_flags = nullptr;
-  cudaMalloc(&d_flags, sizeof(int));
+  dev_malloc(&d_flags, sizeof(int));
   cudaMemsetAsync(d_flags, 0, sizeof(int), st);
   double *d_xint = nullptr, *d_X = nullptr, *d_K = nullptr, *d_fac = nullptr, *d_lq = nullptr, *d_Q = nullptr;
   int *d_cols = nullptr, *d_qrs = nullptr;
   int64_t* d_off = nullptr;
-  cudaMalloc(&d_off, sizeof(int64_t) * nsp);
+  dev_malloc(&d_off, sizeof(int64_t) * nsp);
   const int MQ = cfg.maxqual;
-  cudaMalloc(&d_xint, sizeof(double) * nrs * MQ);
-  cudaMalloc(&d_X, sizeof(double) * nrs * MQ);
-  cudaMalloc(&d_K, sizeof(double) * MQ * MQ);
-  cudaMalloc(&d_fac, sizeof(double) * MQ);
-  cudaMalloc(&d_cols, sizeof(int) * MQ);
-  cudaMalloc(&d_qrs, sizeof(int) * MQ);
-  cudaMalloc(&d_Q, sizeof(double) * MQ * MQ);
-  cudaMalloc(&d_lq, sizeof(double) * (size_t)MQ * kVecBlock);
+  dev_malloc(&d_xint, sizeof(double) * nrs * MQ);
+  dev_malloc(&d_X, sizeof(double) * nrs * MQ);
+  dev_malloc(&d_K, sizeof(double) * MQ * MQ);
+  dev_malloc(&d_fac, sizeof(double) * MQ);
+  dev_malloc(&d_cols, sizeof(int) * MQ);
+  dev_malloc(&d_qrs, sizeof(int) * MQ);
+  dev_malloc(&d_Q, sizeof(double) * MQ * MQ);
+  dev_malloc(&d_lq, sizeof(double) * (size_t)MQ * kVecBlock);
   std::vector<double> hdiash(nsp), hq;
   std::vector<int64_t> off_sp(nsp);
   auto Lcol = [&](int J) -> double* { return c->Lblk[J / kVecBlock] + (size_t)nrs * (J % kVecBlock); };
@@ -515,7 +515,7 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
     // destination columns of this pass
     while ((int)c->Lblk.size() * kVecBlock < M + nk) {
       double* p = nullptr;
-      if (cudaMalloc(&p, sizeof(double) * nrs * kVecBlock) != cudaSuccess) { rc = MG_ERR_MEMORY; break; }
+      if (dev_malloc(&p, sizeof(double) * nrs * kVecBlock) != cudaSuccess) { rc = MG_ERR_MEMORY; break; }
       cudaMemsetAsync(p, 0, sizeof(double) * nrs * kVecBlock, st);
       c->Lblk.push_back(p);
     }
@@ -565,7 +565,7 @@ int cho_make_fp32(ChoState* c, cudaStream_t st) {
   c->Lblk32.clear();
   for (size_t b = 0; b < c->Lblk.size(); ++b) {
     float* p = nullptr;
-    if (cudaMalloc(&p, sizeof(float) * c->nrs * kVecBlock) != cudaSuccess) return MG_ERR_MEMORY;
+    if (dev_malloc(&p, sizeof(float) * c->nrs * kVecBlock) != cudaSuccess) return MG_ERR_MEMORY;
     k_to_fp32<<<nblk(c->nrs * kVecBlock), 256, 0, st>>>(c->Lblk[b], p, c->nrs * kVecBlock);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     c->Lblk32.push_back(p);

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "eri_kernel.cuh"
@@ -17,20 +18,33 @@ EriFn eri_kernel_pick(int nab, int ncd) {
   return nab <= 3 ? eri_kernel_pick_lo(nab, ncd) : eri_kernel_pick_hi(nab, ncd);
 }
 
-// Cartesian exponent table of the kernel (l = 0..7, C3 order, packed).
-static const double* eri_tables(int device) {
-  static double* tab[64] = {nullptr};
-  if (device < 0 || device >= 64) return nullptr;
-  if (!tab[device]) {
-    std::vector<int> t(2 * kETabD, 0);
+// Cartesian exponent table of the kernel (l = 0..7, C3 order, packed as
+// lx | ly << 8 | lz << 16), built at compile time into a file-scope device
+// array: the launcher only looks its address up, so an ERI launch never
+// allocates device memory.
+struct EriCartTable {
+  int v[2 * kETabD];
+  constexpr EriCartTable() : v() {
     int k = 0;
     for (int l = 0; l <= 7; ++l)
       for (int lx = l; lx >= 0; --lx)
-        for (int ly = l - lx; ly >= 0; --ly) t[k++] = lx | (ly << 8) | ((l - lx - ly) << 16);
-    double* d = nullptr;
-    if (cudaMalloc(&d, sizeof(double) * kETabD) != cudaSuccess) return nullptr;
-    cudaMemcpy(d, t.data(), sizeof(double) * kETabD, cudaMemcpyHostToDevice);
-    tab[device] = d;
+        for (int ly = l - lx; ly >= 0; --ly) v[k++] = lx | (ly << 8) | ((l - lx - ly) << 16);
+  }
+};
+static_assert(sizeof(EriCartTable) == sizeof(double) * kETabD, "exponent table size");
+static __device__ __align__(16) const EriCartTable g_eri_cart_table{};
+
+// Device address of the table on `device` (looked up once per device, with
+// that device current; cudaGetSymbolAddress does not allocate).
+static const double* eri_tables(int device) {
+  static const double* tab[64] = {nullptr};
+  static std::mutex mu;
+  if (device < 0 || device >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!tab[device]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_eri_cart_table) != cudaSuccess) return nullptr;
+    tab[device] = (const double*)p;
   }
   return tab[device];
 }

@@ -326,11 +326,7 @@ __global__ void __launch_bounds__(kEriThreads, 1) eri_kernel(const EriArgs a, co
 
 template <int A, int B>
 EriFn eri_fn() {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(eri_kernel<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    attr = true;
-  }
+  if (!smem_attr_once((const void*)eri_kernel<A, B>, 227 * 1024)) return nullptr;
   return eri_kernel<A, B>;
 }
 template <int A>

@@ -38,7 +38,7 @@ static int make_grad_tables(const Handle* h, double** d_tab) {
   for (int l = 0; l <= 7; ++l)
     for (int lx = l; lx >= 0; --lx)
       for (int ly = l - lx; ly >= 0; --ly) cart[k++] = lx | (ly << 8) | ((l - lx - ly) << 16);
-  if (cudaMalloc(d_tab, sizeof(double) * kGTabD) != cudaSuccess) return MG_ERR_MEMORY;
+  if (dev_malloc(d_tab, sizeof(double) * kGTabD) != cudaSuccess) return MG_ERR_MEMORY;
   cudaMemcpy(*d_tab, t.data(), sizeof(double) * kGTabD, cudaMemcpyHostToDevice);
   return 0;
 }
@@ -219,7 +219,7 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
   cudaFree(plan.d_items);
   plan.d_items = nullptr;
   if (!plan.items.empty()) {
-    if (cudaMalloc(&plan.d_items, sizeof(GradItem) * plan.items.size()) != cudaSuccess) return MG_ERR_MEMORY;
+    if (dev_malloc(&plan.d_items, sizeof(GradItem) * plan.items.size()) != cudaSuccess) return MG_ERR_MEMORY;
     cudaMemcpy(plan.d_items, plan.items.data(), sizeof(GradItem) * plan.items.size(), cudaMemcpyHostToDevice);
   }
   cudaFree(plan.d_scratch);
@@ -228,8 +228,8 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
   plan.d_counters = nullptr;
   // one scratch region per side stream: class kernels on different streams run concurrently
   plan.scratch_stride = (std::max<size_t>(scratch_need, 32) + 31) & ~(size_t)31;
-  if (cudaMalloc(&plan.d_scratch, sizeof(double) * plan.scratch_stride * MG_ERI_STREAMS) != cudaSuccess ||
-      cudaMalloc(&plan.d_counters, sizeof(int) * std::max<size_t>(plan.classes.size(), 1)) != cudaSuccess) {
+  if (dev_malloc(&plan.d_scratch, sizeof(double) * plan.scratch_stride * MG_ERI_STREAMS) != cudaSuccess ||
+      dev_malloc(&plan.d_counters, sizeof(int) * std::max<size_t>(plan.classes.size(), 1)) != cudaSuccess) {
     h->err = "gradient scratch allocation failed";
     return MG_ERR_MEMORY;
   }

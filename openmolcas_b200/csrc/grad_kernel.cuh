@@ -539,11 +539,7 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
 
 template <int MINB, int A, int B>
 GradFn grad_fn() {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(grad_kernel<A, B, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    attr = true;
-  }
+  if (!smem_attr_once((const void*)grad_kernel<A, B, MINB>, 227 * 1024)) return nullptr;
   return grad_kernel<A, B, MINB>;
 }
 template <int MINB, int A>

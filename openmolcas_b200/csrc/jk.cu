@@ -30,6 +30,7 @@
 #include <mutex>
 #include <vector>
 
+#include "kern_common.cuh"
 #include "mg_internal.h"
 #include "tc_syrk.cuh"
 #include "tc_xgemm.cuh"
@@ -301,11 +302,11 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
     h->err = "tensor maps for the exchange GEMMs could not be encoded";
     return MG_ERR_CUDA;
   }
-  static std::once_flag smem_once;
-  std::call_once(smem_once, [] {
-    cudaFuncSetAttribute(tc_syrk3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
-    cudaFuncSetAttribute(tc_xgemm3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kXgSmem);
-  });
+  if (!smem_attr_once((const void*)tc_syrk3_kernel, kTcSmem) ||
+      !smem_attr_once((const void*)tc_xgemm3_kernel, kXgSmem)) {
+    h->err = "exchange GEMMs: shared-memory limit could not be raised";
+    return MG_ERR_CUDA;
+  }
   cudaMemsetAsync(d_err, 0, sizeof(int), st);
   const double one = 1.0, zero = 0.0;
   cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, r, &one, d_C, n, d_C, n, &zero, D, n);

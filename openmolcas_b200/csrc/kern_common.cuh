@@ -2,9 +2,28 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "mg_internal.h"
 
 namespace mg {
+
+// Raise the dynamic shared-memory limit of kernel `fn` on the current device.
+// The attribute belongs to a (kernel, device) pair, so it is set once per
+// device, under a lock (threads may make their first calls together).
+inline bool smem_attr_once(const void* fn, int bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({fn, dev})) return true;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) return false;
+  done.insert({fn, dev});
+  return true;
+}
 
 // Rys root/weight table: per-order metadata and the device coefficient pool.
 struct RysArgs {

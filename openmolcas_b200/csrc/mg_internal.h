@@ -17,6 +17,15 @@ namespace mg {
 
 // number of kernels of this library launched so far (all handles)
 extern std::atomic<long long> g_launches;
+// number of device allocations this library has requested so far (all handles)
+extern std::atomic<long long> g_allocs;
+
+// Every device allocation of the library goes through here (counted).
+template <typename T>
+inline cudaError_t dev_malloc(T** p, size_t bytes) {
+  g_allocs.fetch_add(1, std::memory_order_relaxed);
+  return cudaMalloc((void**)p, bytes);
+}
 
 // Per-order metadata of the Rys root/weight table (constant memory).
 struct RysMeta {

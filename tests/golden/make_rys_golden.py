@@ -17,6 +17,14 @@ import sys
 import numpy as np
 
 
+def reference_tree():
+    """The OpenMolcas source tree: the first argument, or $OPENMOLCAS_SRC."""
+    src = os.environ.get("OPENMOLCAS_SRC")
+    if not src:
+        sys.exit("usage: python %s <OpenMolcas source tree>  (or set OPENMOLCAS_SRC)" % sys.argv[0])
+    return src
+
+
 def read_rysrw(path):
     with open(path) as f:
         lines = f.read().splitlines()
@@ -92,4 +100,4 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else reference_tree())
