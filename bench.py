@@ -265,7 +265,16 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="molgpu", choices=["molgpu", "reference"])
+    ap.add_argument("--leg", default=None, choices=["eri", "grad", "jk"],
+                    help="run one leg alone (timing / profiling driver), no JSON line")
+    ap.add_argument("--cfg", default=None, help="--leg eri/grad: configuration (c2, c4, small, medium)")
+    ap.add_argument("--quartets", type=int, default=20000, help="--leg eri: sample size")
+    ap.add_argument("--natom", type=int, default=40, help="--leg jk: atoms of the 1500-function cluster mix")
+    ap.add_argument("--reps", type=int, default=2, help="--leg: timed repetitions")
+    ap.add_argument("--precision", default="mixed,fp64", help="--leg jk: precisions to run (mixed, fp64, s<k>)")
     args = ap.parse_args()
+    if args.leg:
+        return run_leg(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
@@ -446,44 +455,141 @@ def grad_flops(g):
         return None
 
 
-def cpu_baseline(S=None, budget_s=20.0, threads=None):
-    """Oracle (CPU restatement) on a bounded sample of the same workload,
-    extrapolated to one full step.  J/K: the oracle's J/K over a subset of
-    vectors of the same shape (cost is value-independent), scaled by M;
-    gradient: every k-th unique quartet, scaled by k."""
-    from oracle import oracle as O
+CPU_SAMPLE_FACTOR = 100  # each CPU leg times at least 1/100 of its workload
+
+
+class CpuRef:
+    """The CPU restatement of the reference path on bounded samples of the
+    step's workload, extrapolated to one full step:
+      J/K       CHO_LK_SCF through numpy's BLAS (oracle.cho_jk_blas: DGEMV for J,
+                DGEMM for the half-transform and the exchange product, as the
+                reference calls its BLAS) over nv of the M vectors,
+                nv = max(8 per thread, M / 100), scaled by M / nv (the cost does
+                not depend on the vector values);
+      gradient  the oracle's Drvg1 restatement (OpenMP over shell quartets) over
+                every 100th Schwarz-screened unique quartet, scaled by 100; each
+                step starts at the next offset, so successive steps time
+                disjoint samples.
+    Both arms of the bench use this same sampler."""
+
+    def __init__(self, M=None, threads=None):
+        from oracle import oracle as O
+        from openmolcas_b200 import basis as B
+        self.O = O
+        self.threads = threads or os.cpu_count() or 1
+        m3 = B.config_molecule(JK_CFG)
+        self.M = int(M or C3_NVEC)
+        self.n = m3.nbf
+        self.rs_a, self.rs_b, _ = O.Oracle(m3).rs_list()
+        nrs = self.rs_a.size
+        self.nv = max(8 * self.threads, -(-self.M // CPU_SAMPLE_FACTOR))
+        self.L = np.random.default_rng(0).standard_normal((nrs, self.nv)) * 1e-3
+        cfg = B.CONFIGS[JK_CFG]
+        self.C3 = B.density_factor(m3.nbf, cfg["rank"], cfg["seed"])
+        m4 = B.config_molecule(GRAD_CFG)
+        self.o4 = O.Oracle(m4)
+        self.o4.schwarz()
+        C4 = B.density_factor(m4.nbf, B.CONFIGS[GRAD_CFG]["rank"], B.CONFIGS[GRAD_CFG]["seed"])
+        self.D4 = C4 @ C4.T
+        self.k = 0
+
+    def step(self):
+        t0 = time.time()
+        self.O.cho_jk_blas(self.rs_a, self.rs_b, self.n, self.L, self.C3)
+        t_jk_s = time.time() - t0
+        t0 = time.time()
+        _, nq = self.O.grad_sampled(self.o4, self.D4, CUTINT, CPU_SAMPLE_FACTOR, self.k)
+        t_gr_s = time.time() - t0
+        self.k += 1
+        f_jk = self.M / self.nv
+        return {"value": t_jk_s * f_jk + t_gr_s * CPU_SAMPLE_FACTOR, "unit": "s", "cores": self.threads,
+                "kind": "port",
+                "sample": f"J/K: CHO_LK_SCF through BLAS over {self.nv} of {self.M} vectors ({t_jk_s:.2f} s measured, "
+                          f"x{f_jk:.1f}); gradient: every {CPU_SAMPLE_FACTOR}th of {nq} screened unique quartets "
+                          f"({t_gr_s:.2f} s measured, x{CPU_SAMPLE_FACTOR})",
+                "legs_s": {"jk": t_jk_s * f_jk, "grad": t_gr_s * CPU_SAMPLE_FACTOR},
+                "measured_s": {"jk": t_jk_s, "grad": t_gr_s},
+                "extrapolation": {"jk": f_jk, "grad": CPU_SAMPLE_FACTOR}}
+
+
+def cpu_baseline(S=None, threads=None):
+    """One step of the CPU sampler (CpuRef) for the GPU arm's line."""
+    return CpuRef(M=S["cho"]["M"] if S else None, threads=threads).step()
+
+
+def run_leg(args):
+    """One leg alone, inside an NVTX range named after it (ncu --nvtx
+    --nvtx-include "<leg>/" selects its kernels), timed with CUDA events:
+      --leg eri  --cfg c2 --quartets N   seeded sample of the screened unique quartets
+      --leg grad --cfg c4|small|medium   two-electron gradient (small/medium: 4/8 atoms of 4s3p2d)
+      --leg jk   --natom N               Cholesky (ThrCom 1e-6) + J/K, N atoms of the 1500-bf mix"""
+    import torch
     from openmolcas_b200 import basis as B
-    if threads:
-        os.environ["OMP_NUM_THREADS"] = str(threads)
-    m3 = S["m3"] if S else B.config_molecule(JK_CFG)
-    m4 = S["m4"] if S else B.config_molecule(GRAD_CFG)
-    # without a GPU run: the vector count of this decomposition (ThrCom 1e-6), which the
-    # GPU arm reports as cholesky.M (its pivots equal the oracle's)
-    M = S["cho"]["M"] if S else C3_NVEC
-    o3 = O.Oracle(m3)
-    nrs = m3.nbf * (m3.nbf + 1) // 2
-    rng = np.random.default_rng(0)
-    r = B.CONFIGS[JK_CFG]["rank"]
-    Cm = B.density_factor(m3.nbf, r, B.CONFIGS[JK_CFG]["seed"])
-    nv = 2
-    Ls = rng.standard_normal((nrs, nv)) * 1e-3
-    t0 = time.time()
-    o3.cho_jk(Ls, Cm)
-    t_jk_sample = time.time() - t0
-    t_jk = t_jk_sample * M / nv
-    o4 = O.Oracle(m4)
-    C4 = B.density_factor(m4.nbf, B.CONFIGS[GRAD_CFG]["rank"], B.CONFIGS[GRAD_CFG]["seed"])
-    D4 = C4 @ C4.T
-    o4.schwarz()
-    stride = 4000
-    t0 = time.time()
-    _, nq = O.grad_sampled(o4, D4, CUTINT, stride)
-    t_gr_sample = time.time() - t0
-    t_gr = t_gr_sample * stride
-    return {"value": t_jk + t_gr, "unit": "s", "cores": O.num_threads(), "kind": "port",
-            "sample": f"J/K: {nv} of {M} vectors (scaled x{M / nv:.0f}, {t_jk_sample:.1f}s); gradient: every "
-                      f"{stride}th of {nq} unique quartets (scaled x{stride}, {t_gr_sample:.1f}s)",
-            "legs_s": {"jk": t_jk, "grad": t_gr}}
+    from openmolcas_b200.molgpu import MolGpu, unique_quartets
+
+    def timed(fn):
+        ms = []
+        for _ in range(args.reps):
+            e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+            torch.cuda.nvtx.range_push(args.leg)
+            e0.record()
+            out = fn()
+            e1.record()
+            torch.cuda.nvtx.range_pop()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return out, ms
+
+    if args.leg == "eri":
+        cfg = args.cfg or ERI_CFG
+        m = B.config_molecule(cfg)
+        g = MolGpu(m)
+        q = unique_quartets(len(m.shells), g.schwarz(), CUTINT)
+        sel = q[np.sort(np.random.default_rng(0).choice(len(q), min(args.quartets, len(q)), replace=False))]
+        out = torch.empty(int(g.quartet_offsets(sel)[-1]), dtype=torch.float64, device="cuda")
+        _, ms = timed(lambda: g.eri_quartets(sel, out))
+        print(f"eri {cfg}: {len(sel)} of {len(q)} quartets, last {ms[-1]:.2f} ms, {len(sel) / ms[-1] * 1e3:.3e} quartets/s")
+    elif args.leg == "grad":
+        cfg = args.cfg or GRAD_CFG
+        if cfg in ("small", "medium"):
+            na = 4 if cfg == "small" else 8
+            m = B.make_molecule(f"{cfg}4s3p2d", na, [("4s3p2d", na)], 4)
+            rank = 10 if cfg == "small" else 20
+        else:
+            m = B.config_molecule(cfg)
+            rank = B.CONFIGS[cfg]["rank"] or 40
+        g = MolGpu(m)
+        Cn = B.density_factor(m.nbf, rank, 4)
+        D = torch.from_numpy(Cn @ Cn.T).cuda()
+        grad, ms = timed(lambda: g.drvg1(D, cutint=CUTINT))
+        print(f"grad {cfg}: nbf {m.nbf}, last {ms[-1]:.1f} ms, |sum F| = {float(grad.sum(0).abs().max()):.2e}")
+    else:
+        c3 = B.CONFIGS[JK_CFG]
+        natom = args.natom
+        if natom >= c3["natom"]:
+            m = B.config_molecule(JK_CFG)
+        else:
+            mix = [(t, max(1, round(k * natom / c3["natom"]))) for t, k in c3["mix"]]
+            mix[-1] = (mix[-1][0], natom - sum(k for _, k in mix[:-1]))
+            m = B.make_molecule(f"jk{natom}", natom, mix, c3["seed"])
+        g = MolGpu(m)
+        info = g.cho_drv(thrcom=THRCOM)
+        Cd = torch.from_numpy(B.density_factor(m.nbf, min(c3["rank"], m.nbf // 2), c3["seed"])).cuda()
+        D = Cd @ Cd.t()
+        res = {}
+        for name in args.precision.split(","):
+            prec = {"mixed": MolGpu.PREC_MIXED, "fp64": MolGpu.PREC_FP64}.get(name)
+            if prec is None:
+                prec = MolGpu.PREC_SLICED(int(name[1:]))
+            g.cho_jk(Cd, precision=prec)
+            torch.cuda.synchronize()
+            (J, K), ms = timed(lambda: g.cho_jk(Cd, precision=prec))
+            res[name] = (ms[-1], float(0.5 * (D * J).sum() - 0.25 * (D * K).sum()))
+        line = f"jk {natom} atoms: nbf {m.nbf}, M {info['M']}"
+        for name, (ms, E) in res.items():
+            line += f", {name} {ms:.2f} ms (E {E:.10f})"
+        print(line)
+    return 0
 
 
 def run_reference(args):
@@ -492,11 +598,17 @@ def run_reference(args):
     os.environ["OMP_NUM_THREADS"] = str(cores)
     vals = []
     cb = None
+    ref = CpuRef(threads=cores)
+    measured = {"jk": 0.0, "grad": 0.0}
     for k in range(args.warmup + args.steps):
-        cb = cpu_baseline(None, threads=cores)
+        cb = ref.step()
         if k >= args.warmup:
             vals.append(cb["value"])
+            for leg in measured:
+                measured[leg] += cb["measured_s"][leg]
     v = float(np.mean(vals))
+    cb["sample"] += f"; over the {args.steps} timed steps {measured['jk']:.1f} s (J/K) and {measured['grad']:.1f} s " \
+                    f"(gradient) were measured"
     eri_ref = None
     try:  # ERI throughput of the CPU restatement on the same seeded quartet sample
         from oracle import oracle as O

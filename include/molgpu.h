@@ -28,12 +28,13 @@ extern "C" {
 
 typedef struct mg_handle mg_handle;
 
-/* Error codes (mirroring Cho_Drv's 0/1/2 where they apply). */
+/* Error codes (mirroring Cho_Drv's iReturn 0/1/2, cholesky_util/
+ * cho_drv_inner.F90:14-19, where they apply). */
 #define MG_OK 0
 #define MG_ERR_ARG 1       /* bad argument / unsupported input          */
-#define MG_ERR_MEMORY 2    /* device allocation failed                  */
+#define MG_ERR_DECOMP 1    /* Cholesky decomposition failed (iReturn 1) */
+#define MG_ERR_MEMORY 2    /* device allocation failed (iReturn 2)      */
 #define MG_ERR_CUDA 3      /* CUDA launch or runtime error              */
-#define MG_ERR_DECOMP 104  /* Cholesky decomposition error (Cho_Quit 104) */
 
 /* Create a handle on `device`, loading the Rys root/weight table
  * (replaces SetUpR/Read_RysRW, rys_util/setupr.F90:15, read_rysrw.F90:14). */
@@ -73,6 +74,20 @@ int mg_eri_work(mg_handle* h, const int32_t* quartets, int64_t nq, double* prim_
 int mg_eri_quartets(mg_handle* h, const int32_t* quartets, int64_t nq, const int64_t* offsets, double* d_out,
                     void* stream);
 
+/* One shell quartet in the calling convention of the per-quartet kernel
+ * Do_TwoEl (procedure(twoel_kernel), selected at integral_util/
+ * eval_ijkl.F90:93-95; arguments in integral_util/twoel_interface.fh):
+ * coor[12] = Coor(3,4) (checked against the handle's shell centres),
+ * isd4 = iSD4(0:nsd, 4) (column-major, nsd+1 entries per shell; entry 20 is
+ * the 1-based shell index nSkal of Def_Shells, integral_util/
+ * def_shells.F90:148, entries 1 and 3 (l, nBasis) are checked), wrk[nwork]
+ * (host) receives the AO integrals Wrk(1:nijkl*nabcd) in the layout of
+ * Eval_IJKL (contracted index fastest, then iCmp1..iCmp4), any shell order.
+ * *noints is set to 0 (integrals were computed).  Synchronous, one quartet:
+ * a compatibility path, the batched entry point is the fast one. */
+int mg_twoel_nosym(mg_handle* h, const double* coor, int* noints, double* wrk, int64_t nwork, const int64_t* isd4,
+                   int64_t nsd);
+
 /* Allocation-free variant of mg_eri_quartets.  No counterpart in the
  * reference.  For callers that cannot let the library allocate device memory
  * during a call: programs that reserve all device memory in their own pool
@@ -109,8 +124,12 @@ typedef struct mg_cho_cfg {
 } mg_cho_cfg;
 
 int mg_cho_default(mg_cho_cfg* cfg);
-/* Returns 0 ok, MG_ERR_DECOMP (104) on a decomposition failure (Cho_Quit 104),
- * MG_ERR_MEMORY when the vectors do not fit.  Synchronous. */
+/* Returns Cho_Drv's iReturn: 0 ok, 1 (MG_ERR_DECOMP) when the decomposition
+ * failed (cho_drv_inner.F90:155,192: no qualifying diagonal, a negative
+ * diagonal below TooNeg, CD_InCore failure; also an invalid argument), 2
+ * (MG_ERR_MEMORY) when the vectors do not fit in device memory
+ * (cho_drv_inner.F90:338); 3 on a CUDA error.  mg_last_error() names the
+ * cause.  Synchronous. */
 int mg_cho_drv(mg_handle* h, const mg_cho_cfg* cfg, void* stream);
 int mg_cho_info(mg_handle* h, int64_t* nrs, int* nvec, int* npass);
 /* pivot (rs index) and pass of every vector, in vector order */
@@ -128,13 +147,26 @@ int mg_cho_diag(mg_handle* h, double* d_diag, void* stream);
  *   D = C C^T, C (nbf x r, column-major, device);
  *   J_ab = sum_cd (ab|cd) D_cd,  K_ab = sum_cd (ac|bd) D_cd
  * with (ab|cd) ~ sum_J L_ab,J L_cd,J.  J, K: nbf x nbf device, overwritten
- * (the reference accumulates into FLT/KLT; callers add).
- * precision: MG_PREC_FP64 (FP64 vectors, FP64 products) or MG_PREC_MIXED
- * (FP32 vectors, 3-term split-BF16 tensor-core products, FP32 accumulation).
+ * (the reference accumulates into FLT/KLT; mg_cho_lk_scf below does).
+ * precision:
+ *   MG_PREC_FP64     FP64 vectors, FP64 products (DGEMM/DSYRK);
+ *   MG_PREC_MIXED    FP64 vectors cut into MG_JK_SLICES 8-bit slices per row
+ *                    (power-of-two row scaling), both exchange GEMMs on the
+ *                    tensor cores in 8-bit integers with exact INT32
+ *                    accumulation, FP64 recombination; Coulomb part FP64;
+ *   MG_PREC_SLICED(s) the same with s slices (2..8).
  */
 #define MG_PREC_FP64 0
 #define MG_PREC_MIXED 1
+#define MG_PREC_SLICED(s) (100 + (s))
+#define MG_JK_SLICES 6
 int mg_cho_jk(mg_handle* h, const double* d_C, int r, double* d_J, double* d_K, int precision, void* stream);
+/* The accumulating form of CHO_LK_SCF (fock_util/cho_lk_scf.F90:14, one
+ * density): d_FLT += J[D] - factxi * K[D] (FLT nbf x nbf, device), the sum the
+ * reference builds into FLT (Coulomb, cho_lk_scf.F90:919) and KLT (exchange
+ * with -FactXI, :785-831, added into FLT at :993-1018).  Synchronous. */
+int mg_cho_lk_scf(mg_handle* h, const double* d_C, int r, double factxi, double* d_FLT, int precision,
+                  void* stream);
 
 /* ---------------------------------------------------------------------
  * Two-electron nuclear gradient (replaces Drvg1, alaska/drvg1.F90:15, with
@@ -169,6 +201,17 @@ double mg_drvg1_flops(mg_handle* h, double cutint);
  * 1..9 or a negative T.
  */
 int mg_rys_roots(mg_handle* h, int nrys, int64_t n, const double* T, double* x, double* w);
+
+/* The 8-bit sliced tensor-core engine of MG_PREC_MIXED on given dense FP64
+ * matrices (verification; no reference counterpart): X = A B^T with A
+ * (ld x ld) and B (r x ld) row-major, X row-major (ld x r), then
+ * K = X X^T into the lower triangle of K (column-major ld x ld; the upper
+ * part of the diagonal 128 x 128 tiles is also written).  ld a multiple of
+ * 128, slices 2..8.  d_slices (slices x ld x ld bytes) and d_exps (ld ints),
+ * when not NULL, receive the 8-bit slices and row exponents of A.
+ * Synchronous. */
+int mg_sliced_selftest(mg_handle* h, int ld, int r, int slices, const double* d_A, const double* d_B, double* d_X,
+                       double* d_K, void* d_slices, int* d_exps, void* stream);
 
 /* Number of kernels of this library launched so far in this process (library
  * calls such as cuBLAS are not counted).  No reference counterpart. */

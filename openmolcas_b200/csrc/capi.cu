@@ -188,6 +188,7 @@ int mg_destroy(mg_handle* H) {
   free_basis(h);
   cudaFree(h->d_rys);
   cudaFree(h->d_eri_counters);
+  cudaFree(h->d_lk);
   for (int k = 0; k < MG_ERI_STREAMS; ++k) {
     if (h->eri_streams[k]) cudaStreamDestroy(h->eri_streams[k]);
     if (h->eri_events[k]) cudaEventDestroy(h->eri_events[k]);
@@ -301,6 +302,79 @@ int mg_eri_quartets(mg_handle* H, const int32_t* q4, int64_t nq, const int64_t* 
   int rc = build_eri_items(h, q4, nq, offsets, items, classes);
   if (rc) return rc;
   return run_eri_items(h, items, classes, d_out, (cudaStream_t)stream);
+}
+
+int mg_twoel_nosym(mg_handle* H, const double* coor, int* noints, double* wrk, int64_t nwork, const int64_t* isd4,
+                   int64_t nsd) {
+  if (!H || !coor || !noints || !wrk || !isd4 || nsd < 20) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  const int ns = h->sh.size();
+  int sh[4];
+  int64_t nijkl = 1, nabcd = 1;
+  for (int x = 0; x < 4; ++x) {
+    const int64_t* d = isd4 + (nsd + 1) * x;
+    sh[x] = (int)d[20] - 1;
+    if (sh[x] < 0 || sh[x] >= ns) { h->err = "mg_twoel_nosym: iSD4(20,*) is not a shell of the handle"; return MG_ERR_ARG; }
+    const ShellH& S = h->sh[sh[x]];
+    if (d[1] != S.l || d[3] != S.nc) {
+      h->err = "mg_twoel_nosym: iSD4 angular momentum or contraction count differs from the handle's shell";
+      return MG_ERR_ARG;
+    }
+    for (int c = 0; c < 3; ++c)
+      if (std::fabs(coor[3 * x + c] - S.A[c]) > 1e-10 * std::max(1.0, std::fabs(S.A[c]))) {
+        h->err = "mg_twoel_nosym: Coor differs from the handle's shell centre";
+        return MG_ERR_ARG;
+      }
+    nijkl *= S.nc;
+    nabcd *= S.ncomp;
+  }
+  if (nwork < nijkl * nabcd) { h->err = "mg_twoel_nosym: Wrk too small"; return MG_ERR_ARG; }
+  cudaSetDevice(h->device);
+  // canonical quartet (i >= j, k >= l) for the batched kernel, then the block
+  // is transposed back to the caller's shell order
+  const bool sab = sh[0] < sh[1], scd = sh[2] < sh[3];
+  const int32_t q[4] = {sab ? sh[1] : sh[0], sab ? sh[0] : sh[1], scd ? sh[3] : sh[2], scd ? sh[2] : sh[3]};
+  int64_t off[2];
+  int rc = mg_eri_quartets_size(H, q, 1, off);
+  if (rc) return rc;
+  const int64_t nout = off[1];
+  std::vector<EriItem> items;
+  std::vector<EriClass> classes;
+  rc = build_eri_items(h, q, 1, off, items, classes);
+  if (rc) return rc;
+  double* blk = nullptr;
+  if (dev_malloc(&blk, sizeof(double) * nout) != cudaSuccess) { h->err = "mg_twoel_nosym: allocation failed"; return MG_ERR_MEMORY; }
+  rc = run_eri_items(h, items, classes, blk, nullptr);
+  std::vector<double> hb(nout);
+  if (!rc && cudaMemcpy(hb.data(), blk, sizeof(double) * nout, cudaMemcpyDeviceToHost) != cudaSuccess) rc = MG_ERR_CUDA;
+  cudaFree(blk);
+  if (rc) return rc;
+  // canonical layout: [i'][j'][k'][l'] contracted (i' fastest) x [ci'][cj'][ck'][cl'] components
+  const ShellH *A = &h->sh[sh[0]], *B = &h->sh[sh[1]], *Cs = &h->sh[sh[2]], *Ds = &h->sh[sh[3]];
+  const int n0 = A->nc, n1 = B->nc, n2 = Cs->nc, n3 = Ds->nc;
+  const int m0 = A->ncomp, m1 = B->ncomp, m2 = Cs->ncomp, m3 = Ds->ncomp;
+  const int cn0 = sab ? n1 : n0, cn1 = sab ? n0 : n1, cn2 = scd ? n3 : n2;
+  const int cm0 = sab ? m1 : m0, cm1 = sab ? m0 : m1, cm2 = scd ? m3 : m2;
+  const int64_t cnijkl = nijkl;
+  for (int d3 = 0; d3 < m3; ++d3)
+    for (int d2 = 0; d2 < m2; ++d2)
+      for (int d1 = 0; d1 < m1; ++d1)
+        for (int d0 = 0; d0 < m0; ++d0) {
+          const int e0 = sab ? d1 : d0, e1 = sab ? d0 : d1, e2 = scd ? d3 : d2, e3 = scd ? d2 : d3;
+          const int64_t csrc = e0 + (int64_t)cm0 * (e1 + (int64_t)cm1 * (e2 + (int64_t)cm2 * e3));
+          const int64_t cdst = d0 + (int64_t)m0 * (d1 + (int64_t)m1 * (d2 + (int64_t)m2 * d3));
+          for (int i3 = 0; i3 < n3; ++i3)
+            for (int i2 = 0; i2 < n2; ++i2)
+              for (int i1 = 0; i1 < n1; ++i1)
+                for (int i0 = 0; i0 < n0; ++i0) {
+                  const int j0 = sab ? i1 : i0, j1 = sab ? i0 : i1, j2 = scd ? i3 : i2, j3 = scd ? i2 : i3;
+                  const int64_t src = j0 + (int64_t)cn0 * (j1 + (int64_t)cn1 * (j2 + (int64_t)cn2 * j3));
+                  const int64_t dst = i0 + (int64_t)n0 * (i1 + (int64_t)n1 * (i2 + (int64_t)n2 * i3));
+                  wrk[dst + nijkl * cdst] = hb[src + cnijkl * csrc];
+                }
+        }
+  *noints = 0;
+  return 0;
 }
 
 int mg_schwarz(mg_handle* H, double* tmax) {
@@ -440,9 +514,40 @@ int mg_cho_jk(mg_handle* H, const double* d_C, int r, double* d_J, double* d_K, 
   if (!h->cho) { h->err = "mg_cho_jk: no Cholesky vectors (call mg_cho_drv)"; return MG_ERR_ARG; }
   cudaSetDevice(h->device);
   if (precision == MG_PREC_FP64) return jk_fp64(h, d_C, r, d_J, d_K, (cudaStream_t)stream, 32);
-  if (precision == MG_PREC_MIXED) return jk_mixed(h, d_C, r, d_J, d_K, (cudaStream_t)stream, 64);
+  if (precision == MG_PREC_MIXED) return jk_mixed(h, d_C, r, d_J, d_K, (cudaStream_t)stream, 64, MG_JK_SLICES);
+  if (precision > 100 && precision <= 108)
+    return jk_mixed(h, d_C, r, d_J, d_K, (cudaStream_t)stream, 64, precision - 100);
   h->err = "mg_cho_jk: unsupported precision";
   return MG_ERR_ARG;
+}
+
+int mg_cho_lk_scf(mg_handle* H, const double* d_C, int r, double factxi, double* d_FLT, int precision,
+                  void* stream) {
+  if (!H || !d_C || !d_FLT || r < 1) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  if (!h->cho) { h->err = "mg_cho_lk_scf: no Cholesky vectors (call mg_cho_drv)"; return MG_ERR_ARG; }
+  cudaSetDevice(h->device);
+  const size_t nn = (size_t)h->nbf * h->nbf;
+  if (h->lk_cap < nn) {
+    cudaFree(h->d_lk);
+    h->d_lk = nullptr;
+    h->lk_cap = 0;
+    if (dev_malloc(&h->d_lk, 2 * nn * sizeof(double)) != cudaSuccess) {
+      h->err = "mg_cho_lk_scf: allocation failed";
+      return MG_ERR_MEMORY;
+    }
+    h->lk_cap = nn;
+  }
+  int rc = mg_cho_jk(H, d_C, r, h->d_lk, h->d_lk + nn, precision, stream);
+  if (rc) return rc;
+  return fock_accumulate(d_FLT, h->d_lk, h->d_lk + nn, factxi, (int64_t)nn, (cudaStream_t)stream);
+}
+
+int mg_sliced_selftest(mg_handle* H, int ld, int r, int slices, const double* d_A, const double* d_B, double* d_X,
+                       double* d_K, void* d_slices, int* d_exps, void* stream) {
+  if (!H || !d_A || !d_B || !d_X || !d_K) return MG_ERR_ARG;
+  cudaSetDevice(H->h.device);
+  return oz_selftest(&H->h, ld, r, slices, d_A, d_B, d_X, d_K, (uint8_t*)d_slices, d_exps, (cudaStream_t)stream);
 }
 
 long long mg_kernel_launches(void) { return g_launches.load(); }

@@ -16,8 +16,7 @@
 // DGEMM, row-parallel CompVec, reductions.  Host work per pass: the choice
 // of shell pair, the qualification list and the in-core CD of the <=100 x 100
 // qualified block (sequential, exact reference semantics).  Vectors are FP64
-// in reduced-set ("rs") layout, blocks of kVecBlock columns; an FP32 copy is
-// made on request for the mixed-precision J/K.
+// in reduced-set ("rs") layout, blocks of kVecBlock columns.
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
@@ -188,11 +187,6 @@ __global__ void k_gather_rows(const double* __restrict__ L, int64_t nrs, int nco
   lq[o] = L[rows[i] + nrs * J];
 }
 
-__global__ void k_to_fp32(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t < n) b[t] = (float)a[t];
-}
-
 static inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
 
 // --------------------------------------------------------------- host side
@@ -210,7 +204,6 @@ struct ChoState {
   double* d_diag0 = nullptr;    // exact (ab|ab)
   unsigned char* d_inred = nullptr;
   std::vector<double*> Lblk;    // FP64 vector blocks, nrs x kVecBlock each
-  std::vector<float*> Lblk32;
   int M = 0;
   std::vector<int> piv, pass_of;
   int npass = 0;
@@ -224,7 +217,6 @@ void cho_free(ChoState* c) {
   cudaFree(c->d_rs); cudaFree(c->d_sp_first); cudaFree(c->d_sp_count); cudaFree(c->d_rs_a); cudaFree(c->d_rs_b);
   cudaFree(c->d_diag); cudaFree(c->d_diag0); cudaFree(c->d_inred);
   for (auto p : c->Lblk) cudaFree(p);
-  for (auto p : c->Lblk32) cudaFree(p);
   if (c->cublas) cublasDestroy(c->cublas);
   delete c;
 }
@@ -560,19 +552,6 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
   return rc;
 }
 
-int cho_make_fp32(ChoState* c, cudaStream_t st) {
-  for (auto p : c->Lblk32) cudaFree(p);
-  c->Lblk32.clear();
-  for (size_t b = 0; b < c->Lblk.size(); ++b) {
-    float* p = nullptr;
-    if (dev_malloc(&p, sizeof(float) * c->nrs * kVecBlock) != cudaSuccess) return MG_ERR_MEMORY;
-    k_to_fp32<<<nblk(c->nrs * kVecBlock), 256, 0, st>>>(c->Lblk[b], p, c->nrs * kVecBlock);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-    c->Lblk32.push_back(p);
-  }
-  return 0;
-}
-
 int64_t cho_nrs(const ChoState* c) { return c->nrs; }
 int cho_nvec(const ChoState* c) { return c->M; }
 int cho_npass(const ChoState* c) { return c->npass; }
@@ -606,10 +585,6 @@ const int* cho_rs_b_dev(const ChoState* c) { return c->d_rs_b; }
 const double* cho_vec_ptr(const ChoState* c, int J0, int nb, cudaStream_t, Handle*) {
   if (J0 / kVecBlock != (J0 + nb - 1) / kVecBlock) return nullptr;
   return c->Lblk[J0 / kVecBlock] + (size_t)c->nrs * (J0 % kVecBlock);
-}
-const float* cho_vec_ptr32(const ChoState* c, int J0, int nb) {
-  if (c->Lblk32.empty() || J0 / kVecBlock != (J0 + nb - 1) / kVecBlock) return nullptr;
-  return c->Lblk32[J0 / kVecBlock] + (size_t)c->nrs * (J0 % kVecBlock);
 }
 int cho_vec_block() { return kVecBlock; }
 

@@ -6,15 +6,15 @@
 //   J_ab = sum_J L_ab,J V_J,  V_J = sum_cd L_cd,J D_cd     (cho_lk_scf.F90:442-449)
 //   K_ab = sum_J sum_k X_J[a,k] X_J[b,k],  X_J = L_J C      (cho_lk_scf.F90:507-830)
 //
-// Mixed path: vectors stored FP32; per block of vectors the rs-packed L_J
-// are unpacked into dense split BF16 squares (hi + lo, hi = bf16(x),
-// lo = bf16(x - hi)); both exchange GEMMs are hand-written tcgen05 kernels
-// with 3 BF16 products (hi*hi + hi*lo + lo*hi) into FP32 tensor memory, fed
-// by TMA: the half-transform X_J = L_J C (tc_xgemm.cuh) writes the split,
-// K-major X^T directly, and K += X X^T (tc_syrk.cuh: lower-triangle tiles,
-// FP32 over one block's nb*r terms, FP64 atomic accumulation) keeps the
-// accumulation error from growing with the number of vectors.  J uses FP32
-// loads with FP64 accumulation.
+// Mixed path: the FP64 vectors are cut into s 8-bit slices per row
+// (oz_gemm.cuh gives the scheme) and both exchange GEMMs run on the tcgen05
+// tensor cores in 8-bit integers with exact INT32 accumulation: per block of
+// vectors, a slicing kernel unpacks the rs-packed L_J into sliced dense
+// squares (and forms the Coulomb contractions V_J on the way), the
+// half-transform X_J = L_J C writes X in FP64, X is sliced per row over the
+// block, and the exchange product K += X X^T runs over groups of blocks
+// (lower-triangle tiles, CTA-private FP64 tiles, FP64 atomics into K).  J
+// is FP64 throughout.
 //
 // FP64 path ("plain FP64 GPU path"): vectors in FP64, per block of vectors
 // the rs-packed L_J are unpacked to dense symmetric nbf x nbf matrices, the
@@ -32,8 +32,7 @@
 
 #include "kern_common.cuh"
 #include "mg_internal.h"
-#include "tc_syrk.cuh"
-#include "tc_xgemm.cuh"
+#include "oz_gemm.cuh"
 
 namespace mg {
 
@@ -78,6 +77,20 @@ __global__ void k_symmetrize_lower(double* __restrict__ K, int n) {
 }
 
 static inline unsigned nb256(int64_t n) { return (unsigned)((n + 255) / 256); }
+
+// F += J - factxi K (CHO_LK_SCF's FLT update)
+__global__ void k_fock_acc(double* __restrict__ F, const double* __restrict__ J, const double* __restrict__ K,
+                           double factxi, int64_t n) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < n) F[t] += J[t] - factxi * K[t];
+}
+
+int fock_accumulate(double* F, const double* J, const double* K, double factxi, int64_t n, cudaStream_t st) {
+  k_fock_acc<<<nb256(n), 256, 0, st>>>(F, J, K, factxi, n);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (cudaGetLastError() != cudaSuccess) return MG_ERR_CUDA;
+  return cudaStreamSynchronize(st) == cudaSuccess ? 0 : MG_ERR_CUDA;
+}
 
 struct JkWork {
   int* d_rs_a = nullptr;
@@ -135,14 +148,157 @@ int jk_fp64(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaS
 }
 
 // ------------------------------------------------------------ mixed path
-// split x -> (hi, lo) BF16
-__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
-  hi = __float2bfloat16_rn(x);
-  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+// Slicing of one value y in (-1, 1) into s 8-bit pieces (oz_gemm.cuh):
+// byte p of the result, S_0 signed, U_p (p >= 1) unsigned.  Every slice but
+// the last is a floor (remainder in [0, 1)); the last one is rounded to
+// nearest (clamped to 255), so the dropped tail has no systematic sign.
+__device__ __forceinline__ void oz_cut(double y, int s, uint32_t (&w)[2 * kOzMaxSlices], int u) {
+  const int word = u >> 2, sh = 8 * (u & 3);
+  double t = floor(y * 128.0);
+  y = y * 128.0 - t;
+  // a tiny negative y (|128 y| < 2^-53) leaves 1 - |128 y|, which rounds to
+  // exactly 1: carry it back (the value is then 0 to within 2^-53 of the row
+  // maximum) so that every later slice stays within [0, 255]
+  if (y >= 1.0) {
+    t += 1.0;
+    y -= 1.0;
+  }
+  w[word] |= ((uint32_t)(int)t & 255u) << sh;
+  for (int p = 1; p < s; ++p) {
+    t = p + 1 < s ? floor(y * 256.0) : fmin(floor(fma(y, 256.0, 0.5)), 255.0);
+    w[2 * p + word] |= ((uint32_t)(int)t & 255u) << sh;
+    y = y * 256.0 - t;
+  }
 }
 
-// inv[a*n + b] = inv[b*n + a] = t for every rs pair t (entries outside the
-// reduced set stay -1)
+__device__ __forceinline__ int oz_exponent(double m) {
+  int e = 0;
+  if (m > 0.0) frexp(m, &e);
+  return e;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// One warp per row (J, a) of a block of nb vectors (slice p starts at
+// LS + p * slice, the stride of the tensor map over a full block): gathers the square row
+// L_J[a, 0..n) from the rs-packed FP64 vectors through the inverse rs table,
+// writes its s slices LS[p][J*ld + a][0..ld) (zero beyond n) and the row
+// exponent eA[J*ld + a], and adds sum_b L_J[a,b] D[a,b] to V[J] (the Coulomb
+// contraction V_J = sum_cd L_cd,J D_cd over the full square).
+__global__ void k_oz_slice_l(const int* __restrict__ inv, int n, int64_t nrs, const double* __restrict__ L, int nb,
+                             int ld, int s, int64_t slice, const double* __restrict__ D, uint8_t* __restrict__ LS,
+                             int* __restrict__ eA, double* __restrict__ V) {
+  const int lane = threadIdx.x & 31;
+  const int64_t row = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (row >= (int64_t)nb * ld) return;
+  const int J = (int)(row / ld), a = (int)(row - (int64_t)J * ld);
+  const double* LJ = L + nrs * J;
+  const int* ir = inv + (size_t)a * n;
+  double m = 0.0, v = 0.0;
+  if (a < n)
+    for (int b = lane; b < n; b += 32) {
+      const double x = LJ[ir[b]];
+      m = fmax(m, fabs(x));
+      v = fma(x, D[(size_t)a * n + b], v);
+    }
+  m = warp_max(m);
+  v = warp_sum(v);
+  const int e = oz_exponent(m);
+  if (lane == 0) {
+    eA[row] = e;
+    if (a < n) atomicAdd(&V[J], v);
+  }
+  uint8_t* out = LS + (size_t)row * ld;
+  for (int b0 = 8 * lane; b0 < ld; b0 += 256) {
+    uint32_t w[2 * kOzMaxSlices];
+#pragma unroll
+    for (int k = 0; k < 2 * kOzMaxSlices; ++k) w[k] = 0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int b = b0 + u;
+      const double x = (a < n && b < n) ? LJ[ir[b]] : 0.0;
+      oz_cut(ldexp(x, -e), s, w, u);
+    }
+    for (int p = 0; p < s; ++p) *reinterpret_cast<uint2*>(out + p * slice + b0) = make_uint2(w[2 * p], w[2 * p + 1]);
+  }
+}
+
+// C (n x r, column-major FP64) -> slices CS[q][k][0..ld) for k < npad
+// (rows k >= r and columns b >= n zero), column exponents fC[k].  One warp
+// per column k.
+__global__ void k_oz_slice_c(const double* __restrict__ C, int n, int r, int npad, int ld, int s,
+                             uint8_t* __restrict__ CS, int* __restrict__ fC) {
+  const int lane = threadIdx.x & 31;
+  const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (k >= npad) return;
+  const double* ck = C + (size_t)n * k;
+  double m = 0.0;
+  if (k < r)
+    for (int b = lane; b < n; b += 32) m = fmax(m, fabs(ck[b]));
+  const int e = oz_exponent(warp_max(m));
+  if (lane == 0) fC[k] = e;
+  uint8_t* out = CS + (size_t)k * ld;
+  const size_t slice = (size_t)npad * ld;
+  for (int b0 = 8 * lane; b0 < ld; b0 += 256) {
+    uint32_t w[2 * kOzMaxSlices];
+#pragma unroll
+    for (int q = 0; q < 2 * kOzMaxSlices; ++q) w[q] = 0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int b = b0 + u;
+      oz_cut(ldexp((k < r && b < n) ? ck[b] : 0.0, -e), s, w, u);
+    }
+    for (int q = 0; q < s; ++q) *reinterpret_cast<uint2*>(out + q * slice + b0) = make_uint2(w[2 * q], w[2 * q + 1]);
+  }
+}
+
+// One warp per row a of X (FP64, row stride xrow, columns [0, kx)):
+// slices XS[p][a][col0 + 0..kblk) (zero beyond kx and for rows a >= n) and
+// the row exponent eX[a] over this block.
+__global__ void k_oz_slice_x(const double* __restrict__ X, int64_t xrow, int n, int kx, int ld, int kblk, int s,
+                             int64_t xs_row, int64_t col0, uint8_t* __restrict__ XS, int* __restrict__ eX) {
+  const int lane = threadIdx.x & 31;
+  const int a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (a >= ld) return;
+  const double* xa = X + (size_t)a * xrow;
+  double m = 0.0;
+  if (a < n)
+    for (int c = lane; c < kx; c += 32) m = fmax(m, fabs(xa[c]));
+  const int e = oz_exponent(warp_max(m));
+  if (lane == 0) eX[a] = e;
+  const size_t slice = (size_t)ld * xs_row;
+  uint8_t* out = XS + (size_t)a * xs_row + col0;
+  for (int c0 = 8 * lane; c0 < kblk; c0 += 256) {
+    uint32_t w[2 * kOzMaxSlices];
+#pragma unroll
+    for (int q = 0; q < 2 * kOzMaxSlices; ++q) w[q] = 0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int c = c0 + u;
+      oz_cut(ldexp((a < n && c < kx) ? xa[c] : 0.0, -e), s, w, u);
+    }
+    for (int q = 0; q < s; ++q) *reinterpret_cast<uint2*>(out + q * slice + c0) = make_uint2(w[2 * q], w[2 * q + 1]);
+  }
+}
+
+// jrs[t] += sum_J L[t, J] V[J] over one block of nb FP64 vectors
+__global__ void k_jacc64(const double* __restrict__ L, int64_t nrs, int nb, const double* __restrict__ V,
+                         double* __restrict__ jrs) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nrs) return;
+  double s = 0.0;
+  for (int J = 0; J < nb; ++J) s = fma(L[t + nrs * J], V[J], s);
+  jrs[t] += s;
+}
+
+// inv[a*n + b] = inv[b*n + a] = t for every rs pair t
 __global__ void k_rs_inverse(const int* __restrict__ rs_a, const int* __restrict__ rs_b, int64_t nrs, int n,
                              int* __restrict__ inv) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -150,49 +306,6 @@ __global__ void k_rs_inverse(const int* __restrict__ rs_a, const int* __restrict
   const int a = rs_a[t], b = rs_b[t];
   inv[(size_t)a * n + b] = (int)t;
   inv[(size_t)b * n + a] = (int)t;
-}
-
-// Dense split squares Lhi/Llo[J][a][b] (leading dimension ld, padding zero)
-// written row by row, two columns per thread (coalesced 4-byte stores); the
-// packed value is gathered through the inverse rs table.
-__global__ void k_unpack_dense_split(const int* __restrict__ inv, int n, int64_t nrs, const float* __restrict__ L,
-                                     int nb, int ld, __nv_bfloat162* __restrict__ Lhi,
-                                     __nv_bfloat162* __restrict__ Llo) {
-  const int64_t half = ld / 2;
-  int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (o >= (int64_t)nb * ld * half) return;
-  const int b2 = (int)(o % half);
-  const int64_t r1 = o / half;
-  const int a = (int)(r1 % ld);
-  const int J = (int)(r1 / ld);
-  float v[2];
-#pragma unroll
-  for (int u = 0; u < 2; ++u) {
-    const int b = 2 * b2 + u;
-    float x = 0.0f;
-    if (a < n && b < n) {
-      const int t = inv[(size_t)a * n + b];
-      if (t >= 0) x = L[t + nrs * J];
-    }
-    v[u] = x;
-  }
-  __nv_bfloat16 h0, l0, h1, l1;
-  split_bf16(v[0], h0, l0);
-  split_bf16(v[1], h1, l1);
-  Lhi[o] = __halves2bfloat162(h0, h1);
-  Llo[o] = __halves2bfloat162(l0, l1);
-}
-
-// C (n x r, column-major FP64) -> split BF16 with leading dimension ld (padding zero)
-__global__ void k_split_c(const double* __restrict__ C, int n, int r, int ld, __nv_bfloat16* __restrict__ hi,
-                          __nv_bfloat16* __restrict__ lo) {
-  int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (o >= (int64_t)ld * r) return;
-  const int a = (int)(o % ld), k = (int)(o / ld);
-  __nv_bfloat16 h = __float2bfloat16_rn(0.0f), l = h;
-  if (a < n) split_bf16((float)C[a + (size_t)n * k], h, l);
-  hi[o] = h;
-  lo[o] = l;
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
@@ -210,158 +323,215 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// 2D BF16 tensor map over rows x kpad (K contiguous), 64 x box_rows boxes, 128-byte swizzle.
-static bool make_operand_map(CUtensorMap* m, const __nv_bfloat16* base, int rows, int kpad, int box_rows = kTcTile) {
+// 3D 8-bit tensor map over slices [s][rows][kx] (kx contiguous), boxes of
+// 32 bytes x box_rows x 1 slice, 32-byte swizzle.
+static bool make_slice_map(CUtensorMap* m, const uint8_t* base, int64_t kx, int64_t rows, int s, int box_rows) {
   auto enc = tensor_map_encoder();
-  if (!enc || ((uintptr_t)base & 15) || (kpad * 2) % 16 || box_rows < 1 || box_rows > 256) return false;
-  cuuint64_t gdim[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
-  cuuint64_t gstr[1] = {(cuuint64_t)kpad * 2};
-  cuuint32_t box[2] = {(cuuint32_t)kTcBK, (cuuint32_t)box_rows}, es[2] = {1, 1};
-  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+  if (!enc || ((uintptr_t)base & 15) || kx % 32 || box_rows < 1 || box_rows > 256) return false;
+  cuuint64_t gdim[3] = {(cuuint64_t)kx, (cuuint64_t)rows, (cuuint64_t)s};
+  cuuint64_t gstr[2] = {(cuuint64_t)kx, (cuuint64_t)(kx * rows)};
+  cuuint32_t box[3] = {32u, (cuuint32_t)box_rows, 1u}, es[3] = {1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void*)base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// V[J] += sum_t L[t,J] dw[t] over one row chunk (FP32 loads, FP64 accumulation);
-// grid (vectors, row chunks); V must be zeroed first
-__global__ void k_jvec(const float* __restrict__ L, int64_t nrs, const double* __restrict__ dw, double* __restrict__ V) {
-  const int J = blockIdx.x;
-  const float* l = L + nrs * J;
-  const int64_t chunk = (nrs + gridDim.y - 1) / gridDim.y;
-  const int64_t t0 = chunk * blockIdx.y, t1 = min(nrs, t0 + chunk);
-  double s = 0.0;
-  for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) s = fma((double)l[t], dw[t], s);
-  __shared__ double red[32];
-  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-    if (threadIdx.x == 0) atomicAdd(&V[J], s);
-  }
+static inline int rup(int x, int m) { return (x + m - 1) / m * m; }
+
+// Pass plan of one kind of output tile: accumulators of acc_stride TMEM
+// columns, at most 512 columns; shared-memory ring of the slices 0..s-1.
+static void oz_plan(OzArgs& a, int s, int Nt) {
+  a.s = s;
+  a.Nt = Nt;
+  a.acc_stride = rup(Nt, 32);
+  a.nd = std::min(s, 512 / a.acc_stride);
+  a.b_bytes = rup(32 * Nt, 1024);
+  a.stage_bytes = s * (kOzABytes + a.b_bytes);
+  a.stages = std::min(kOzMaxStages, (kOzSmemLimit - 1024) / a.stage_bytes);
 }
 
-// jrs[t] += sum_J L[t,J] V[J]
-__global__ void k_jacc(const float* __restrict__ L, int64_t nrs, int nb, const double* __restrict__ V,
-                       double* __restrict__ jrs) {
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= nrs) return;
-  double s = 0.0;
-  for (int J = 0; J < nb; ++J) s = fma((double)L[t + nrs * J], V[J], s);
-  jrs[t] += s;
-}
-
-
-int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block) {
+int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block, int s) {
   ChoState* c = h->cho;
   const int64_t nrs = cho_nrs(c);
   const int M = cho_nvec(c);
   const int n = h->nbf;
-  // rows of the squares and of X^T padded to the 128-row tensor-core tile (padding zero)
-  const int ld = (n + 127) / 128 * 128;
-  if (!cho_vec_ptr32(c, 0, 1)) {
-    int rc = cho_make_fp32(c, st);
-    if (rc) { h->err = "FP32 vector copy failed"; return rc; }
-  }
+  if (s < 2 || s > kOzMaxSlices) { h->err = "mixed J/K: slices must be 2..8"; return MG_ERR_ARG; }
+  const int ld = rup(n, 128);
+  // column tiles of C: at most 256 rows per MMA
+  const int nnt = (r + 255) / 256;
+  const int Nt = rup((r + nnt - 1) / nnt, 16);
+  const int npad = nnt * Nt;
+  // vectors per block: one block's K extent of the exchange product, nb r
+  const int nb = std::min(block, M);
+  const int kx = nb * r;
+  const int kblk = rup(kx, 32);
+  const int nsub = (kblk + kOzKChunk - 1) / kOzKChunk;
+  const int ksub = rup((kblk + nsub - 1) / nsub, 32);
+  const int nblocks = (M + nb - 1) / nb;
+  const int G = std::min(16, nblocks);  // blocks per exchange-product group
+  const int ntile = (ld / 128) * (ld / 128 + 1) / 2;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
   cublasHandle_t cb = cho_cublas(c);
   cublasSetStream(cb, st);
   const int* d_ra = cho_rs_a_dev(c);
   const int* d_rb = cho_rs_b_dev(c);
-  const size_t nn = (size_t)n * n, ll = (size_t)ld * ld;
-  // exchange product: K range split so that the lower-triangle tiles x splits cover the SMs
-  const int ntile = (ld / kTcTile) * (ld / kTcTile + 1) / 2;
-  int nsm = 148;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
-  const int nsplit = std::max(1, std::min(8, (nsm + ntile - 1) / ntile));
-  const int kq = kTcBK * nsplit;
-  const int kpad = (block * r + kq - 1) / kq * kq;
-  const size_t xt = (size_t)ld * kpad;
-  const int bbox = r <= kXgMaxN ? (r + 15) / 16 * 16 : kXgMaxN;  // rows of a C box
-  size_t need = 8 * ((size_t)2 * nrs + block + nn) + 2 * (2 * (size_t)ld * r) + 2 * (2 * (size_t)block * ll) +
-                2 * (2 * xt) + 4 * nn + 16 * 256;
+  const size_t nn = (size_t)n * n;
+  const int64_t xs_row = (int64_t)G * kblk;
+  size_t need = 8 * (nrs + (size_t)nb + nn) + 4 * nn + (size_t)s * npad * ld + 4 * (size_t)npad +
+                (size_t)s * nb * ld * ld + 4 * (size_t)nb * ld + 8 * (size_t)n * kx + (size_t)s * ld * xs_row +
+                4 * (size_t)G * ld + 8 * (size_t)nsm * 128 * 128 + 16 * 256;
   char* ws = (char*)ws_get(h, need, st);
   if (!ws) { h->err = "jk workspace allocation failed"; return MG_ERR_MEMORY; }
   auto take = [&](size_t bytes) { char* p = ws; ws += (bytes + 255) & ~(size_t)255; return (void*)p; };
-  double* dw = (double*)take(8 * nrs);
   double* jrs = (double*)take(8 * nrs);
-  double* V = (double*)take(8 * block);
+  double* V = (double*)take(8 * (size_t)nb);
   double* D = (double*)take(8 * nn);
-  __nv_bfloat16* Chi = (__nv_bfloat16*)take(2 * (size_t)ld * r);
-  __nv_bfloat16* Clo = (__nv_bfloat16*)take(2 * (size_t)ld * r);
-  __nv_bfloat16* Lhi = (__nv_bfloat16*)take(2 * (size_t)block * ll);
-  __nv_bfloat16* Llo = (__nv_bfloat16*)take(2 * (size_t)block * ll);
-  __nv_bfloat16* XThi = (__nv_bfloat16*)take(2 * xt);
-  __nv_bfloat16* XTlo = (__nv_bfloat16*)take(2 * xt);
-  int* d_err = (int*)take(sizeof(int));
   int* inv = (int*)take(4 * nn);
-  CUtensorMap map_hi, map_lo, map_lhi, map_llo, map_chi, map_clo;
-  if (!make_operand_map(&map_hi, XThi, ld, kpad) || !make_operand_map(&map_lo, XTlo, ld, kpad) ||
-      !make_operand_map(&map_lhi, Lhi, block * ld, ld) || !make_operand_map(&map_llo, Llo, block * ld, ld) ||
-      !make_operand_map(&map_chi, Chi, r, ld, bbox) || !make_operand_map(&map_clo, Clo, r, ld, bbox)) {
+  uint8_t* CS = (uint8_t*)take((size_t)s * npad * ld);
+  int* fC = (int*)take(4 * (size_t)npad);
+  uint8_t* LS = (uint8_t*)take((size_t)s * nb * ld * ld);
+  int* eA = (int*)take(4 * (size_t)nb * ld);
+  double* Xf = (double*)take(8 * (size_t)n * kx);
+  uint8_t* XS = (uint8_t*)take((size_t)s * ld * xs_row);
+  int* eX = (int*)take(4 * (size_t)G * ld);
+  double* P = (double*)take(8 * (size_t)nsm * 128 * 128);
+  int* d_err = (int*)take(sizeof(int));
+  CUtensorMap map_l, map_c, map_x;
+  if (!make_slice_map(&map_l, LS, ld, (int64_t)nb * ld, s, 128) || !make_slice_map(&map_c, CS, ld, npad, s, Nt) ||
+      !make_slice_map(&map_x, XS, xs_row, ld, s, 128)) {
     h->err = "tensor maps for the exchange GEMMs could not be encoded";
     return MG_ERR_CUDA;
   }
-  if (!smem_attr_once((const void*)tc_syrk3_kernel, kTcSmem) ||
-      !smem_attr_once((const void*)tc_xgemm3_kernel, kXgSmem)) {
+  OzArgs ax{}, ak{};
+  oz_plan(ax, s, Nt);
+  oz_plan(ak, s, 128);
+  if (ax.stages < 2 || ak.stages < 2) { h->err = "mixed J/K: slice tiles do not fit in shared memory"; return MG_ERR_ARG; }
+  if (!smem_attr_once((const void*)oz_gemm_kernel<false>, kOzSmemLimit) ||
+      !smem_attr_once((const void*)oz_gemm_kernel<true>, kOzSmemLimit)) {
     h->err = "exchange GEMMs: shared-memory limit could not be raised";
     return MG_ERR_CUDA;
   }
+  ax.err = ak.err = d_err;
+  ax.nrt = ld / 128; ax.nnt = nnt; ax.ld = ld; ax.n = n; ax.r = r; ax.eA = eA; ax.eB = fC; ax.X = Xf; ax.xrow = kx;
+  ak.ld = ld; ak.n = n; ak.ntile = ntile; ak.nsub = nsub; ak.kblk = kblk; ak.ksub = ksub; ak.eX = eX; ak.P = P;
+  ak.K = d_K;
   cudaMemsetAsync(d_err, 0, sizeof(int), st);
   const double one = 1.0, zero = 0.0;
   cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, r, &one, d_C, n, d_C, n, &zero, D, n);
-  k_pack_density<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, D, n, dw);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_split_c<<<nb256((int64_t)ld * r), 256, 0, st>>>(d_C, n, r, ld, Chi, Clo);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
   cudaMemsetAsync(jrs, 0, 8 * nrs, st);
   cudaMemsetAsync(d_K, 0, 8 * nn, st);
-  cudaMemsetAsync(XThi, 0, 2 * xt, st);  // columns beyond nb*r stay zero
-  cudaMemsetAsync(XTlo, 0, 2 * xt, st);
-  cudaMemsetAsync(inv, 0xFF, 4 * nn, st);
   k_rs_inverse<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, n, inv);
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  const unsigned jchunks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(64, nrs / 8192));
-  for (int J0 = 0; J0 < M; J0 += block) {
-    const int nb = std::min(block, M - J0);
-    const float* Lb = cho_vec_ptr32(c, J0, nb);
-    if (!Lb) { h->err = "vector block straddles storage blocks"; return MG_ERR_ARG; }
-    // Coulomb
-    cudaMemsetAsync(V, 0, 8 * nb, st);
-    k_jvec<<<dim3(nb, jchunks), 256, 0, st>>>(Lb, nrs, dw, V);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-    k_jacc<<<nb256(nrs), 256, 0, st>>>(Lb, nrs, nb, V, jrs);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-    // Exchange: split squares of the block, X_J = L_J C written as split X^T (tcgen05),
-    // then K += X X^T (tcgen05; 3 products into one FP32 accumulator per tile, FP64
-    // atomic add into K).  A short last block leaves stale X^T columns of the previous
-    // block beyond nb*r: clear them first.
-    k_unpack_dense_split<<<nb256((int64_t)nb * ld * (ld / 2)), 256, 0, st>>>(
-        inv, n, nrs, Lb, nb, ld, (__nv_bfloat162*)Lhi, (__nv_bfloat162*)Llo);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-    if (nb < block && J0 > 0) {
-      cudaMemsetAsync(XThi, 0, 2 * xt, st);
-      cudaMemsetAsync(XTlo, 0, 2 * xt, st);
+  k_oz_slice_c<<<(npad + 7) / 8, 256, 0, st>>>(d_C, n, r, npad, ld, s, CS, fC);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  for (int g0 = 0; g0 < nblocks; g0 += G) {
+    const int gn = std::min(G, nblocks - g0);
+    for (int bi = 0; bi < gn; ++bi) {
+      const int J0 = (g0 + bi) * nb;
+      const int nv = std::min(nb, M - J0);
+      const double* Lb = cho_vec_ptr(c, J0, nv, st, h);
+      if (!Lb) { h->err = "vector block straddles storage blocks"; return MG_ERR_ARG; }
+      // a short last block: clear the columns of the missing vectors
+      if (nv < nb) cudaMemsetAsync(Xf, 0, 8 * (size_t)n * kx, st);
+      cudaMemsetAsync(V, 0, 8 * (size_t)nb, st);
+      const int64_t rows = (int64_t)nv * ld;
+      k_oz_slice_l<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(inv, n, nrs, Lb, nv, ld, s, (int64_t)nb * ld * ld, D,
+                                                                LS, eA, V);
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      k_jacc64<<<nb256(nrs), 256, 0, st>>>(Lb, nrs, nv, V, jrs);
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      // X_J = L_J C for the block (the slice map covers nb vectors; nv <= nb of them are used)
+      ax.nJ = nv;
+      ax.nitems = ax.nrt * nv * nnt;
+      const int gx = std::min(ax.nitems, nsm);
+      oz_gemm_kernel<false><<<gx, kOzThreads, ax.stages * ax.stage_bytes + 1024, st>>>(map_l, map_c, ax);
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      k_oz_slice_x<<<(ld + 7) / 8, 256, 0, st>>>(Xf, kx, n, kx, ld, kblk, s, xs_row, (int64_t)bi * kblk, XS,
+                                                eX + (size_t)bi * ld);
+      g_launches.fetch_add(1, std::memory_order_relaxed);
     }
-    tc_xgemm3_kernel<<<dim3(ld / kTcTile, nb, (r + kXgMaxN - 1) / kXgMaxN), 128, kXgSmem, st>>>(
-        map_lhi, map_llo, map_chi, map_clo, ld, r, bbox, kpad, XThi, XTlo, d_err);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-    tc_syrk3_kernel<<<dim3(ntile, nsplit), 128, kTcSmem, st>>>(map_hi, map_lo, n, kpad, d_K, d_err);
+    // K += X X^T over the group (lower tiles)
+    ak.nblk = gn;
+    ak.nitems = ntile * gn * nsub;
+    const int gk = std::min(ak.nitems, nsm);
+    oz_gemm_kernel<true><<<gk, kOzThreads, ak.stages * ak.stage_bytes + 1024, st>>>(map_x, map_x, ak);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
   k_symmetrize_lower<<<nb256((int64_t)nn), 256, 0, st>>>(d_K, n);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_unpack_sym<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, jrs, n, d_J);
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  if (cudaGetLastError() != cudaSuccess) return MG_ERR_CUDA;
+  if (cudaGetLastError() != cudaSuccess) { h->err = "mixed J/K: launch failed"; return MG_ERR_CUDA; }
   int herr = 0;
   cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess) return MG_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) { h->err = "mixed J/K: device error"; return MG_ERR_CUDA; }
   if (herr) {
     h->err = "exchange GEMMs: a pipeline wait ran out (result incomplete)";
     return MG_ERR_CUDA;
   }
   return 0;
+}
+
+// The sliced engine on given dense matrices (verification of the kernels
+// used by jk_mixed): X = A B^T (A: ld x ld, B: r x ld, both row-major; X
+// row-major ld x r) and K = X X^T (lower triangle, column-major ld x ld).
+int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double* d_B, double* d_X, double* d_K,
+                uint8_t* d_slices, int* d_exps, cudaStream_t st) {
+  if (ld < 128 || ld % 128 || r < 1 || s < 2 || s > kOzMaxSlices) return MG_ERR_ARG;
+  const int nnt = (r + 255) / 256;
+  const int Nt = rup((r + nnt - 1) / nnt, 16);
+  const int npad = nnt * Nt;
+  const int kblk = rup(r, 32);
+  const int nsub = (kblk + kOzKChunk - 1) / kOzKChunk;
+  const int ksub = rup((kblk + nsub - 1) / nsub, 32);
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+  const size_t need = (size_t)s * ld * ld + 4 * (size_t)ld + (size_t)s * npad * ld + 4 * (size_t)npad +
+                      (size_t)s * ld * kblk + 4 * (size_t)ld + 8 * (size_t)nsm * 128 * 128 + 16 * 256;
+  char* ws = (char*)ws_get(h, need, st);
+  if (!ws) return MG_ERR_MEMORY;
+  auto take = [&](size_t bytes) { char* p = ws; ws += (bytes + 255) & ~(size_t)255; return (void*)p; };
+  uint8_t* LS = (uint8_t*)take((size_t)s * ld * ld);
+  int* eA = (int*)take(4 * (size_t)ld);
+  uint8_t* CS = (uint8_t*)take((size_t)s * npad * ld);
+  int* fC = (int*)take(4 * (size_t)npad);
+  uint8_t* XS = (uint8_t*)take((size_t)s * ld * kblk);
+  int* eX = (int*)take(4 * (size_t)ld);
+  double* P = (double*)take(8 * (size_t)nsm * 128 * 128);
+  int* d_err = (int*)take(sizeof(int));
+  CUtensorMap map_l, map_c, map_x;
+  if (!make_slice_map(&map_l, LS, ld, ld, s, 128) || !make_slice_map(&map_c, CS, ld, npad, s, Nt) ||
+      !make_slice_map(&map_x, XS, kblk, ld, s, 128))
+    return MG_ERR_CUDA;
+  OzArgs ax{}, ak{};
+  oz_plan(ax, s, Nt);
+  oz_plan(ak, s, 128);
+  if (!smem_attr_once((const void*)oz_gemm_kernel<false>, kOzSmemLimit) ||
+      !smem_attr_once((const void*)oz_gemm_kernel<true>, kOzSmemLimit))
+    return MG_ERR_CUDA;
+  ax.err = ak.err = d_err;
+  ax.nrt = ld / 128; ax.nnt = nnt; ax.ld = ld; ax.n = ld; ax.r = r; ax.eA = eA; ax.eB = fC; ax.X = d_X; ax.xrow = r;
+  ax.nJ = 1; ax.nitems = ax.nrt * nnt;
+  ak.ld = ld; ak.n = ld; ak.ntile = (ld / 128) * (ld / 128 + 1) / 2; ak.nsub = nsub; ak.kblk = kblk; ak.ksub = ksub;
+  ak.eX = eX; ak.P = P; ak.K = d_K; ak.nblk = 1; ak.nitems = ak.ntile * nsub;
+  cudaMemsetAsync(d_err, 0, sizeof(int), st);
+  cudaMemsetAsync(d_K, 0, 8 * (size_t)ld * ld, st);
+  k_oz_slice_x<<<(ld + 7) / 8, 256, 0, st>>>(d_A, ld, ld, ld, ld, ld, s, ld, 0, LS, eA);
+  if (d_slices) cudaMemcpyAsync(d_slices, LS, (size_t)s * ld * ld, cudaMemcpyDeviceToDevice, st);
+  if (d_exps) cudaMemcpyAsync(d_exps, eA, 4 * (size_t)ld, cudaMemcpyDeviceToDevice, st);
+  k_oz_slice_c<<<(npad + 7) / 8, 256, 0, st>>>(d_B, ld, r, npad, ld, s, CS, fC);
+  oz_gemm_kernel<false><<<std::min(ax.nitems, nsm), kOzThreads, ax.stages * ax.stage_bytes + 1024, st>>>(map_l, map_c,
+                                                                                                       ax);
+  k_oz_slice_x<<<(ld + 7) / 8, 256, 0, st>>>(d_X, r, ld, r, ld, kblk, s, kblk, 0, XS, eX);
+  oz_gemm_kernel<true><<<std::min(ak.nitems, nsm), kOzThreads, ak.stages * ak.stage_bytes + 1024, st>>>(map_x, map_x,
+                                                                                                      ak);
+  g_launches.fetch_add(5, std::memory_order_relaxed);
+  if (cudaGetLastError() != cudaSuccess) return MG_ERR_CUDA;
+  int herr = 0;
+  cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return MG_ERR_CUDA;
+  return herr ? MG_ERR_CUDA : 0;
 }
 
 }  // namespace mg

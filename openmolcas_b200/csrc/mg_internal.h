@@ -114,6 +114,8 @@ struct Handle {
   cudaStream_t eri_streams[MG_ERI_STREAMS] = {};  // side streams of the ERI and gradient class launches
   cudaEvent_t eri_events[MG_ERI_STREAMS] = {};
   cudaEvent_t eri_fork = nullptr;
+  double* d_lk = nullptr;          // J and K of mg_cho_lk_scf (2 nbf^2)
+  size_t lk_cap = 0;
 };
 
 struct GradItem {
@@ -154,7 +156,6 @@ struct ChoCfgH {
   int minqual, maxqual, maxvec;
 };
 int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st, std::string& err);
-int cho_make_fp32(ChoState* c, cudaStream_t st);
 void cho_free(ChoState* c);
 int64_t cho_nrs(const ChoState* c);
 int cho_nvec(const ChoState* c);
@@ -168,10 +169,12 @@ cublasHandle_t cho_cublas(ChoState* c);
 const int* cho_rs_a_dev(const ChoState* c);
 const int* cho_rs_b_dev(const ChoState* c);
 const double* cho_vec_ptr(const ChoState* c, int J0, int nb, cudaStream_t st, Handle* h);
-const float* cho_vec_ptr32(const ChoState* c, int J0, int nb);
 int cho_vec_block();
+int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double* d_B, double* d_X, double* d_K,
+                uint8_t* d_slices, int* d_exps, cudaStream_t st);
+int fock_accumulate(double* F, const double* J, const double* K, double factxi, int64_t n, cudaStream_t st);
 int jk_fp64(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block);
-int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block);
+int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block, int s);
 
 inline int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 inline int ncart_cum(int l) { return l <= 0 ? 0 : l * (l + 1) * (l + 2) / 6; }

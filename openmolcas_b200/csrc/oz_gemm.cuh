@@ -1,0 +1,326 @@
+// Exact-integer sliced GEMMs on the tcgen05 tensor cores (kind::i8), the
+// engine of the mixed-precision exchange build.
+//
+// Scheme (Ozaki-style splitting).  Every row i of an operand is scaled by a
+// power of two 2^-e_i (e_i = frexp exponent of the row's largest |x|, so
+// y = x 2^-e_i lies in (-1, 1)) and cut into s 8-bit slices:
+//   y = 2^-7 S_0 + sum_{p>=1} 2^-(7+8p) U_p + tail,  |tail| < 2^-(7+8(s-1)),
+//   S_0 = floor(128 y) in [-128, 127] (signed), U_p in [0, 255] (unsigned)
+// (each remainder after a floor lies in [0, 1)).  A product of two sliced
+// operands is then
+//   (A B^T)_ij = 2^(e_i + f_j) sum_d 2^-(14+8d) sum_{p+q=d} (A_p B_q^T)_ij
+// truncated to d <= s-1.  Each (A_p B_q^T) runs on the tensor cores in 8-bit
+// integers with exact INT32 accumulation in tensor memory (one accumulator
+// per diagonal d); accumulators are read out and combined in FP64 after at
+// most kOzKChunk products per element (4096 * 6 * 255^2 < 2^31), so the only
+// roundings are the FP64 combination and the truncated tail.
+//
+// One CTA of 192 threads per SM:
+//   warp 4 lane 0   TMA producer: per K step of 32, the slices 0..d1-1 of the
+//                   A tile (128 rows) and of the B tile (Nt rows), 32-byte
+//                   swizzle, into a ring of stages guarded by mbarriers
+//   warp 5          allocates the 512 TMEM columns; lane 0 issues the MMAs
+//                   (M = 128, N = Nt, K = 32), releases stages with
+//                   tcgen05.commit and signals a full set of accumulators
+//   warps 0-3       epilogue: TMEM lanes 32w..32w+31, combine the diagonals
+//                   in FP64, scale, write (half-transform) or accumulate into
+//                   a CTA-private FP64 tile (exchange product)
+// The diagonals of one output tile are computed in passes of at most nd
+// accumulators (nd * acc_stride <= 512 TMEM columns); a pass loads only the
+// slices it needs.  Every mbarrier wait is bounded: a wait that runs out sets
+// *err, the CTA stops issuing work, waits (bounded) for its own loads and
+// MMAs in flight and still frees its tensor memory.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tc_common.cuh"
+
+namespace mg {
+
+constexpr int kOzThreads = 192;
+constexpr int kOzMaxStages = 8;
+constexpr int kOzMaxSlices = 8;
+constexpr int kOzKChunk = 4096;  // K elements between accumulator read-outs
+constexpr int kOzABytes = 128 * 32;
+// dynamic shared memory of every launch of the kernels (the attribute is set
+// once per device to this size; stages are planned within it)
+constexpr int kOzSmemLimit = 221 * 1024;
+
+struct OzArgs {
+  int s;           // slices
+  int nd;          // accumulators per pass
+  int acc_stride;  // TMEM columns per accumulator
+  int Nt;          // rows of a B tile (MMA N)
+  int stages, stage_bytes;
+  int b_bytes;     // shared-memory stride of one B slice tile (multiple of 1024)
+  int nitems;
+  int* err;
+  // half-transform X_J = L_J C (SYRK == false): items (row tile, vector, column tile)
+  int nrt, nJ, nnt;
+  int ld;          // rows (and K extent) of one vector's square
+  int n;           // valid rows / columns (nbf)
+  int r;           // columns of C
+  const int* eA;   // row exponents of the L slices, [J * ld + a]
+  const int* eB;   // column exponents of C, [k]
+  double* X;       // X[a * xrow + J * r + k] (FP64)
+  long long xrow;
+  // exchange product K += X X^T (SYRK == true): items (lower tile, block, sub-chunk)
+  int ntile, nblk, nsub;
+  int kblk;        // K extent of one block (multiple of 32)
+  int ksub;        // K elements of a sub-chunk (multiple of 32)
+  const int* eX;   // row exponents of the X slices, [blk * ld + a]
+  double* P;       // CTA-private FP64 tiles, 128 x 128 per CTA
+  double* K;       // column-major n x n (lower triangle accumulated)
+};
+
+// One unit of tensor-core work: an output tile, a K range, one pass of diagonals.
+struct OzUnit {
+  int rowA, rowB;  // first row of the A and B tiles in their tensor maps
+  int k0, nk;      // K range [k0, k0 + 32 nk)
+  int d0, d1;      // diagonals [d0, d1)
+  bool same;       // B tile == A tile (diagonal tile of the exchange product)
+  // epilogue context
+  int t0, t1, J, nt;  // X: row tile, (unused), vector, column tile; SYRK: ti, tj, block
+  bool first;      // first unit of this output tile (write instead of add)
+  bool last;       // last unit of this output tile in this CTA
+};
+
+__device__ __forceinline__ void oz_tile_ij(int x, int& ti, int& tj) {
+  ti = (int)((sqrtf(8.0f * x + 1.0f) - 1.0f) * 0.5f);
+  while ((ti + 1) * (ti + 2) / 2 <= x) ++ti;
+  while (ti * (ti + 1) / 2 > x) --ti;
+  tj = x - ti * (ti + 1) / 2;
+}
+
+// Enumerate this CTA's units in a fixed order (every role walks the same list).
+template <bool SYRK, typename F>
+__device__ __forceinline__ void oz_for_units(const OzArgs& a, F&& f) {
+  const int npass = (a.s + a.nd - 1) / a.nd;
+  if (!SYRK) {
+    const int nsubk = (a.ld + kOzKChunk - 1) / kOzKChunk;
+    for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
+      const int nt = item % a.nnt, r1 = item / a.nnt, J = r1 % a.nJ, rt = r1 / a.nJ;
+      for (int sk = 0; sk < nsubk; ++sk)
+        for (int g = 0; g < npass; ++g) {
+          OzUnit u;
+          u.rowA = J * a.ld + rt * 128;
+          u.rowB = nt * a.Nt;
+          u.k0 = sk * kOzKChunk;
+          u.nk = (min(a.ld, u.k0 + kOzKChunk) - u.k0) / 32;
+          u.d0 = g * a.nd;
+          u.d1 = min(a.s, u.d0 + a.nd);
+          u.same = false;
+          u.t0 = rt; u.t1 = 0; u.J = J; u.nt = nt;
+          u.first = sk == 0 && g == 0;
+          u.last = sk == nsubk - 1 && g == npass - 1;
+          if (!f(u)) return;
+        }
+    }
+  } else {
+    const long long per = (long long)a.nitems;
+    const int i0 = (int)(per * blockIdx.x / gridDim.x), i1 = (int)(per * (blockIdx.x + 1) / gridDim.x);
+    const int per_tile = a.nblk * a.nsub;
+    for (int item = i0; item < i1; ++item) {
+      const int tile = item / per_tile, r1 = item - tile * per_tile, blk = r1 / a.nsub, sub = r1 - blk * a.nsub;
+      int ti, tj;
+      oz_tile_ij(tile, ti, tj);
+      const int kb0 = sub * a.ksub;
+      const int kb1 = min(a.kblk, kb0 + a.ksub);
+      if (kb1 <= kb0) {  // the planner never makes an empty sub-chunk; every role stops here alike
+        if (threadIdx.x == 0) atomicExch(a.err, 2);
+        return;
+      }
+      const bool seg_first = item == i0 || r1 == 0;
+      const bool seg_last = item == i1 - 1 || r1 == per_tile - 1;
+      for (int g = 0; g < npass; ++g) {
+        OzUnit u;
+        u.rowA = ti * 128;
+        u.rowB = tj * 128;
+        u.k0 = blk * a.kblk + kb0;
+        u.nk = (kb1 - kb0) / 32;
+        u.d0 = g * a.nd;
+        u.d1 = min(a.s, u.d0 + a.nd);
+        u.same = ti == tj;
+        u.t0 = ti; u.t1 = tj; u.J = blk; u.nt = 0;
+        u.first = seg_first && g == 0;
+        u.last = seg_last && g == npass - 1;
+        if (!f(u)) return;
+      }
+    }
+  }
+}
+
+template <bool SYRK>
+__global__ void __launch_bounds__(kOzThreads, 1)
+    oz_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                   const OzArgs a) {
+  extern __shared__ uint8_t oz_smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[kOzMaxStages], empty_bar[kOzMaxStages], accf_bar, acce_bar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag;
+  uint8_t* smem = (uint8_t*)(((uintptr_t)oz_smem_raw + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  volatile int* abort = &abort_flag;
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    for (int s = 0; s < a.stages; ++s) {
+      tc_mbar_init(tc_smem_addr(&full_bar[s]), 1);
+      tc_mbar_init(tc_smem_addr(&empty_bar[s]), 1);
+    }
+    tc_mbar_init(tc_smem_addr(&accf_bar), 1);
+    tc_mbar_init(tc_smem_addr(&acce_bar), 4);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem_addr(&tmem_base)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  const int S = a.stages;
+  if (warp == 4) {
+    if (lane == 0) {
+      // ---- TMA producer
+      int it = 0;
+      oz_for_units<SYRK>(a, [&](const OzUnit& u) -> bool {
+        const int nsl = u.d1;  // slices 0..d1-1 of both operands
+        const uint32_t bytes = nsl * (kOzABytes + (u.same ? 0 : 32 * a.Nt));
+        for (int kk = 0; kk < u.nk; ++kk, ++it) {
+          const int st = it % S;
+          const uint32_t ph = (it / S) & 1;
+          if (it >= S && !tc_mbar_wait(tc_smem_addr(&empty_bar[st]), ph ^ 1, abort)) return false;
+          uint8_t* base = smem + (size_t)st * a.stage_bytes;
+          const uint32_t fb = tc_smem_addr(&full_bar[st]);
+          tc_mbar_expect_tx(fb, bytes);
+          const int kx = u.k0 + 32 * kk;
+          for (int p = 0; p < nsl; ++p) tc_tma_load3(tc_smem_addr(base + p * kOzABytes), &mapA, fb, kx, u.rowA, p);
+          if (!u.same)
+            for (int q = 0; q < nsl; ++q)
+              tc_tma_load3(tc_smem_addr(base + a.s * kOzABytes + q * a.b_bytes), &mapB, fb, kx, u.rowB, q);
+        }
+        return true;
+      });
+      // do not leave while loads of this CTA are still landing: wait (bounded)
+      // for the last ring's worth of stages to fill
+      int never = 0;
+      for (int k = (it > S ? it - S : 0); k < it; ++k)
+        tc_mbar_wait(tc_smem_addr(&full_bar[k % S]), (k / S) & 1, (volatile int*)&never);
+    }
+  } else if (warp == 5) {
+    if (lane == 0) {
+      // ---- MMA issuer
+      int it = 0, un = 0;
+      oz_for_units<SYRK>(a, [&](const OzUnit& u) -> bool {
+        // the accumulators must have been read out by the epilogue
+        if (un > 0 && !tc_mbar_wait(tc_smem_addr(&acce_bar), (un - 1) & 1, abort)) return false;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        bool ok = true;
+        for (int kk = 0; kk < u.nk; ++kk, ++it) {
+          const int st = it % S;
+          const uint32_t ph = (it / S) & 1;
+          if (!tc_mbar_wait(tc_smem_addr(&full_bar[st]), ph, abort)) { ok = false; break; }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          uint8_t* base = smem + (size_t)st * a.stage_bytes;
+          const uint32_t abase = tc_smem_addr(base);
+          const uint32_t bbase = u.same ? abase : tc_smem_addr(base + a.s * kOzABytes);
+          const uint32_t bstep = u.same ? kOzABytes : a.b_bytes;
+          for (int d = u.d0; d < u.d1; ++d) {
+            const uint32_t acc = tmem + (uint32_t)((d - u.d0) * a.acc_stride);
+            for (int p = 0; p <= d; ++p) {
+              const int q = d - p;
+              const uint32_t idesc = tc_idesc_i8(a.Nt, p == 0, q == 0);
+              tc_mma_i8(acc, tc_desc_sw32(abase + p * kOzABytes), tc_desc_sw32(bbase + q * bstep), idesc,
+                        (kk > 0 || p > 0) ? 1u : 0u);
+            }
+          }
+          tc_commit(tc_smem_addr(&empty_bar[st]));
+        }
+        // accumulators complete (also after a failure, so the epilogue's wait drains the MMAs in flight)
+        tc_commit(tc_smem_addr(&accf_bar));
+        ++un;
+        return ok;
+      });
+    }
+  } else {
+    // ---- epilogue, warps 0-3: row 32 warp + lane of the output tile
+    const int row = warp * 32 + lane;
+    const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
+    int un = 0;
+    oz_for_units<SYRK>(a, [&](const OzUnit& u) -> bool {
+      int never = 0;
+      bool ok = tc_mbar_wait(tc_smem_addr(&accf_bar), un & 1, (volatile int*)&never) && !*abort;
+      ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld below needs the whole warp
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (ok) {
+        const int ncol = SYRK ? 128 : a.Nt;
+        for (int c0 = 0; c0 < ncol; c0 += 32) {
+          double sum[32];
+#pragma unroll
+          for (int i = 0; i < 32; ++i) sum[i] = 0.0;
+          for (int d = u.d0; d < u.d1; ++d) {
+            uint32_t v[32];
+            tc_ld32(tl + (uint32_t)((d - u.d0) * a.acc_stride + c0), v);
+            const double w = ldexp(1.0, -14 - 8 * d);
+#pragma unroll
+            for (int i = 0; i < 32; ++i) sum[i] = fma((double)(int)v[i], w, sum[i]);
+          }
+          if (!SYRK) {
+            const int arow = u.t0 * 128 + row;
+            if (arow < a.n) {
+              const int ea = a.eA[u.J * a.ld + arow];
+              double* xr = a.X + (size_t)arow * a.xrow + (size_t)u.J * a.r;
+#pragma unroll
+              for (int i = 0; i < 32; ++i) {
+                const int k = u.nt * a.Nt + c0 + i;
+                if (k < a.r && c0 + i < a.Nt) {
+                  const double val = ldexp(sum[i], ea + a.eB[k]);
+                  xr[k] = u.first ? val : xr[k] + val;
+                }
+              }
+            }
+          } else {
+            const int ea = a.eX[u.J * a.ld + u.t0 * 128 + row];
+            const int* eb = a.eX + u.J * a.ld + u.t1 * 128 + c0;
+            double* pr = a.P + (size_t)blockIdx.x * 128 * 128 + (size_t)row * 128 + c0;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+              const double val = ldexp(sum[i], ea + eb[i]);
+              pr[i] = u.first ? val : pr[i] + val;
+            }
+          }
+        }
+        if (SYRK && u.last) {
+          // this CTA's share of the tile is complete: add it into K
+          const int arow = u.t0 * 128 + row;
+          const double* pr = a.P + (size_t)blockIdx.x * 128 * 128 + (size_t)row * 128;
+          if (arow < a.n)
+            for (int c = 0; c < 128; ++c) {
+              const int bcol = u.t1 * 128 + c;
+              if (bcol < a.n) atomicAdd(&a.K[(size_t)arow + (size_t)a.n * bcol], pr[c]);
+            }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) tc_mbar_arrive(tc_smem_addr(&acce_bar));
+      ++un;
+      if (!ok && threadIdx.x == 0) atomicExch(a.err, 1);
+      return ok;
+    });
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (*abort && threadIdx.x == 0) atomicExch(a.err, 1);
+  if (warp == 5) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+}
+
+}  // namespace mg

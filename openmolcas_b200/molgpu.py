@@ -214,6 +214,11 @@ class MolGpu:
     PREC_FP64 = 0
     PREC_MIXED = 1
 
+    @staticmethod
+    def PREC_SLICED(s: int) -> int:
+        """Mixed path with s 8-bit slices per operand row (2..8)."""
+        return 100 + int(s)
+
     def cho_jk(self, Cfac: torch.Tensor, precision: int = 0, J: torch.Tensor | None = None,
                K: torch.Tensor | None = None):
         """CHO_LK_SCF for one density D = C C^T: returns (J, K), nbf x nbf device tensors."""

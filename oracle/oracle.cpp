@@ -1153,56 +1153,121 @@ int or_cholesky_x(void* h, double thrcom, double span, int minqual, int maxqual,
 
 // J, K (nbf x nbf) from vectors L (nrs x M) and density factor C (nbf x r,
 // column-major): D = C C^T.  J_ab = sum_J L_ab,J V_J, V_J = sum_cd L_cd,J D_cd;
-// K_ab = sum_J sum_k (L_J C)_ak (L_J C)_bk.
+// K_ab = sum_J sum_k (L_J C)_ak (L_J C)_bk (CHO_LK_SCF without screening,
+// cho_lk_scf.F90:442-449 and :507-830).  The loops are shaped like the DGEMV /
+// DGEMM calls of the reference: vectors in batches, every inner loop a
+// contiguous dot product (OpenMP SIMD), threads over rows.
+static inline double dot_simd(const double* __restrict__ x, const double* __restrict__ y, int n) {
+  double s = 0.0;
+#pragma omp simd reduction(+ : s)
+  for (int i = 0; i < n; ++i) s += x[i] * y[i];
+  return s;
+}
+
 int or_cho_jk(void* h, const double* L, int M, const double* C, int r, double* J, double* K) {
   Basis& bs = ((Handle*)h)->bs;
   RSList R = make_rs(bs);
-  size_t nrs = R.a.size();
-  int n = bs.nbf;
-  std::vector<double> D((size_t)n * n, 0.0);
-  for (int a = 0; a < n; ++a)
-    for (int b = 0; b < n; ++b) {
+  const size_t nrs = R.a.size();
+  const int n = bs.nbf;
+  std::vector<double> D((size_t)n * n, 0.0), Ct((size_t)n * r);
+  for (int k = 0; k < r; ++k)
+    for (int a = 0; a < n; ++a) Ct[(size_t)a * r + k] = C[a + (size_t)n * k];
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < n; ++b)
+    for (int a = 0; a < n; ++a) D[a + (size_t)n * b] = dot_simd(Ct.data() + (size_t)a * r, Ct.data() + (size_t)b * r, r);
+  std::vector<double> Jrs(nrs, 0.0), Kl((size_t)n * n, 0.0);
+  const int rp = (r + 7) / 8 * 8;  // C row-major, k contiguous, padded to 8
+  std::vector<double> Cr((size_t)n * rp, 0.0);
+  for (int b = 0; b < n; ++b)
+    for (int k = 0; k < r; ++k) Cr[(size_t)b * rp + k] = C[b + (size_t)n * k];
+  const int nvb = std::max(1, std::min(M, 16));  // vectors per batch
+  const int np8 = (n + 7) / 8 * 8;
+  std::vector<double> Lf((size_t)nvb * n * n), X((size_t)n * nvb * r), Xt((size_t)nvb * r * np8, 0.0), V(nvb);
+  const int xr = nvb * r;
+  for (int J0 = 0; J0 < M; J0 += nvb) {
+    const int nb = std::min(nvb, M - J0);
+    // unpack the batch's L_J into full symmetric squares; V_J (DGEMV)
+#pragma omp parallel for schedule(static)
+    for (int jb = 0; jb < nb; ++jb) {
+      double* lf = Lf.data() + (size_t)jb * n * n;
+      const double* l = L + nrs * (J0 + jb);
+      double v = 0;
+      for (size_t t = 0; t < nrs; ++t) {  // the stored (a >= b) half, column b contiguous in a
+        const int a = R.a[t], b = R.b[t];
+        lf[a + (size_t)n * b] = l[t];
+        v += (a == b ? 1.0 : 2.0) * l[t] * D[a + (size_t)n * b];
+      }
+      V[jb] = v;
+      for (int b0 = 0; b0 < n; b0 += 64)  // mirror into the upper half in 64 x 64 blocks
+        for (int a0 = b0; a0 < n; a0 += 64)
+          for (int b = b0; b < std::min(n, b0 + 64); ++b)
+            for (int a = std::max(a0, b + 1); a < std::min(n, a0 + 64); ++a) lf[b + (size_t)n * a] = lf[a + (size_t)n * b];
+    }
+    // Coulomb accumulation (DGEMV): Jrs += L_batch V
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < (int64_t)nrs; ++t) {
       double s = 0;
-      for (int k = 0; k < r; ++k) s += C[a + (size_t)n * k] * C[b + (size_t)n * k];
-      D[a + (size_t)n * b] = s;
+      for (int jb = 0; jb < nb; ++jb) s += L[t + nrs * (J0 + jb)] * V[jb];
+      Jrs[t] += s;
     }
-  std::fill(J, J + (size_t)n * n, 0.0);
-  std::fill(K, K + (size_t)n * n, 0.0);
-  std::vector<double> Jt((size_t)n * n, 0.0);
-#pragma omp parallel
-  {
-    std::vector<double> Lf((size_t)n * n), X((size_t)n * r), Kl((size_t)n * n, 0.0), Jl((size_t)n * n, 0.0);
-#pragma omp for schedule(dynamic)
-    for (int Jv = 0; Jv < M; ++Jv) {
-      std::fill(Lf.begin(), Lf.end(), 0.0);
-      const double* l = L + nrs * Jv;
-      double V = 0;
-      for (size_t t = 0; t < nrs; ++t) {
-        int a = R.a[t], b = R.b[t];
-        Lf[a + (size_t)n * b] = Lf[b + (size_t)n * a] = l[t];
-        V += (a == b ? 1.0 : 2.0) * l[t] * D[a + (size_t)n * b];
-      }
-      for (size_t t = 0; t < nrs; ++t) {
-        int a = R.a[t], b = R.b[t];
-        Jl[a + (size_t)n * b] += l[t] * V;
-        if (a != b) Jl[b + (size_t)n * a] += l[t] * V;
-      }
-      for (int k = 0; k < r; ++k)
-        for (int a = 0; a < n; ++a) {
-          double s = 0;
-          for (int b = 0; b < n; ++b) s += Lf[a + (size_t)n * b] * C[b + (size_t)n * k];
-          X[a + (size_t)n * k] = s;
+    // half-transform X[a][jb*r + k] = sum_b L_J[b,a] C[b,k] (DGEMM; L_J symmetric):
+    // 4 x 8 register blocks over (a, k), Cr = C row-major (k contiguous)
+    const int na4 = (n + 3) / 4, nk8 = (r + 7) / 8;
+#pragma omp parallel for schedule(static) collapse(3)
+    for (int jb = 0; jb < nb; ++jb)
+      for (int ab = 0; ab < na4; ++ab)
+        for (int kb = 0; kb < nk8; ++kb) {
+          const double* lf = Lf.data() + (size_t)jb * n * n;
+          double acc[4][8] = {};
+          int ai[4];
+          for (int i = 0; i < 4; ++i) ai[i] = std::min(n - 1, 4 * ab + i);
+          const int k0 = 8 * kb;
+          for (int b = 0; b < n; ++b) {
+            const double* cr = Cr.data() + (size_t)b * rp + k0;
+#pragma GCC unroll 4
+            for (int i = 0; i < 4; ++i) {
+              const double l = lf[b + (size_t)n * ai[i]];
+#pragma omp simd
+              for (int j = 0; j < 8; ++j) acc[i][j] += l * cr[j];
+            }
+          }
+          for (int i = 0; i < 4 && 4 * ab + i < n; ++i)
+            for (int j = 0; j < 8 && k0 + j < r; ++j) X[(size_t)(4 * ab + i) * xr + (size_t)jb * r + k0 + j] = acc[i][j];
         }
-      for (int b = 0; b < n; ++b)
-        for (int a = 0; a < n; ++a) {
-          double s = 0;
-          for (int k = 0; k < r; ++k) s += X[a + (size_t)n * k] * X[b + (size_t)n * k];
-          Kl[a + (size_t)n * b] += s;
+    // exchange K[a,b] += sum_c X[a][c] X[b][c], b <= a (DSYRK): X transposed to
+    // Xt[c][b] (b contiguous), then 4 x 8 register blocks over (a, b) as above
+    const int kx = nb * r;
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < kx; ++c)
+      for (int b = 0; b < n; ++b) Xt[(size_t)c * np8 + b] = X[(size_t)b * xr + c];
+    const int nb8 = (n + 7) / 8;
+#pragma omp parallel for schedule(dynamic, 4) collapse(2)
+    for (int ab = 0; ab < na4; ++ab)
+      for (int bb = 0; bb < nb8; ++bb) {
+        if (8 * bb > 4 * ab + 3) continue;
+        int ai[4];
+        for (int i = 0; i < 4; ++i) ai[i] = std::min(n - 1, 4 * ab + i);
+        double acc[4][8] = {};
+        for (int c = 0; c < kx; ++c) {
+          const double* xt = Xt.data() + (size_t)c * np8 + 8 * bb;
+#pragma GCC unroll 4
+          for (int i = 0; i < 4; ++i) {
+            const double x = X[(size_t)ai[i] * xr + c];
+#pragma omp simd
+            for (int j = 0; j < 8; ++j) acc[i][j] += x * xt[j];
+          }
         }
-    }
-#pragma omp critical
-    for (size_t t = 0; t < (size_t)n * n; ++t) { J[t] += Jl[t]; K[t] += Kl[t]; }
+        for (int i = 0; i < 4 && 4 * ab + i < n; ++i)
+          for (int j = 0; j < 8 && 8 * bb + j <= 4 * ab + i; ++j) Kl[(size_t)(4 * ab + i) * n + 8 * bb + j] += acc[i][j];
+      }
   }
+  std::fill(J, J + (size_t)n * n, 0.0);
+  for (size_t t = 0; t < nrs; ++t) {
+    const int a = R.a[t], b = R.b[t];
+    J[a + (size_t)n * b] = J[b + (size_t)n * a] = Jrs[t];
+  }
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b <= a; ++b) K[a + (size_t)n * b] = K[b + (size_t)n * a] = Kl[(size_t)a * n + b];
   return 0;
 }
 
@@ -1225,6 +1290,15 @@ int or_grad_x(void* h, const double* D, const double* Ds, double coulfac, double
 int or_grad_sampled(void* h, const double* D, double cutint, int stride, double* grad, int64_t* nquartets) {
   return grad_sampled_x(h, D, nullptr, 1.0, 1.0, cutint, stride, grad, nquartets);
 }
+// the same starting at quartet `offset` (offset < stride): disjoint samples
+static int g_sample_offset = 0;
+int or_grad_sampled_at(void* h, const double* D, double cutint, int stride, int offset, double* grad,
+                       int64_t* nquartets) {
+  g_sample_offset = offset;
+  const int rc = grad_sampled_x(h, D, nullptr, 1.0, 1.0, cutint, stride, grad, nquartets);
+  g_sample_offset = 0;
+  return rc;
+}
 static int grad_sampled_x(void* h, const double* D, const double* Ds, double coulfac, double exfac, double cutint,
                           int stride, double* grad, int64_t* nquartets) {
   Basis& bs = ((Handle*)h)->bs;
@@ -1242,7 +1316,7 @@ static int grad_sampled_x(void* h, const double* D, const double* Ds, double cou
   if (nquartets) *nquartets = qs.size();
   if (stride > 1) {
     std::vector<std::array<int, 5>> sub;
-    for (size_t t = 0; t < qs.size(); t += stride) sub.push_back(qs[t]);
+    for (size_t t = g_sample_offset; t < qs.size(); t += stride) sub.push_back(qs[t]);
     qs.swap(sub);
   }
   int na = bs.natom;

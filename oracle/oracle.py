@@ -53,6 +53,7 @@ def lib():
         L.or_grad.argtypes = [vp, d, C.c_double, d]
         L.or_grad_x.argtypes = [vp, d, C.c_void_p, C.c_double, C.c_double, C.c_double, d]
         L.or_grad_sampled.argtypes = [vp, d, C.c_double, C.c_int, d, C.POINTER(C.c_int64)]
+        L.or_grad_sampled_at.argtypes = [vp, d, C.c_double, C.c_int, C.c_int, d, C.POINTER(C.c_int64)]
         L.or_num_threads.restype = C.c_int
         rc = L.or_load_rys(TABLE.encode())
         if rc != 0:
@@ -192,13 +193,43 @@ def eri_tolerance(S):
     return ERI_ABS_TOL + ERI_REL_S * S
 
 
-def grad_sampled(orc, D, cutint, stride):
-    """Oracle gradient over every stride-th unique quartet; returns (grad, nquartets)."""
+def grad_sampled(orc, D, cutint, stride, offset=0):
+    """Oracle gradient over every stride-th unique quartet starting at
+    `offset`; returns (grad, nquartets)."""
     Dc = np.ascontiguousarray(D, dtype=np.float64)
     g = np.empty(3 * orc.mol.natom)
     nq = C.c_int64(0)
-    lib().or_grad_sampled(orc.h, _p(Dc), cutint, stride, _p(g), C.byref(nq))
+    lib().or_grad_sampled_at(orc.h, _p(Dc), cutint, stride, offset % stride, _p(g), C.byref(nq))
     return g.reshape(-1, 3), nq.value
+
+
+def cho_jk_blas(rs_a, rs_b, n, L, Cm, batch=16):
+    """CHO_LK_SCF's J and K without screening, driven through numpy's BLAS the
+    way the reference drives its linked BLAS: V = L^T d and J = L V as DGEMV
+    (fock_util/cho_lk_scf.F90:442-449), X_J = L_J C as DGEMM and K += X X^T as
+    DGEMM (:507-830).  L: vectors (nrs x M) in the rs order (rs_a, rs_b);
+    Cm: density factor (n x r).  Returns J, K (n x n).  Used as the timed CPU
+    baseline of the exchange build (cost does not depend on the values)."""
+    rs_a = np.asarray(rs_a, dtype=np.int64)
+    rs_b = np.asarray(rs_b, dtype=np.int64)
+    D = Cm @ Cm.T
+    w = np.where(rs_a == rs_b, 1.0, 2.0) * D[rs_a, rs_b]
+    V = L.T @ w
+    Jrs = L @ V
+    K = np.zeros((n, n))
+    M = L.shape[1]
+    for J0 in range(0, M, batch):
+        Lb = L[:, J0:J0 + batch].T
+        Lsq = np.zeros((Lb.shape[0], n, n))
+        Lsq[:, rs_a, rs_b] = Lb
+        Lsq[:, rs_b, rs_a] = Lb
+        X = np.matmul(Lsq, Cm)
+        Xa = X.transpose(1, 0, 2).reshape(n, -1)
+        K += Xa @ Xa.T
+    J = np.zeros((n, n))
+    J[rs_a, rs_b] = Jrs
+    J[rs_b, rs_a] = Jrs
+    return J, K
 
 
 def num_threads():

@@ -161,6 +161,19 @@ def test_cho_jk_matches_exact_within_cd_error(small):
     assert np.abs(K - Ke).max() < 1e-8 * scale
 
 
+def test_cho_jk_blas_equals_loop_restatement(small):
+    """The BLAS-driven J/K (the timed CPU baseline) and the oracle's loop
+    restatement of CHO_LK_SCF agree to rounding."""
+    mol, o, eri = small
+    res = o.cholesky(thrcom=1e-8)
+    Cm = B.density_factor(o.nbf, 7, 3)
+    J, K = o.cho_jk(res["L"], Cm)
+    a, b, _ = o.rs_list()
+    Jb, Kb = O.cho_jk_blas(a, b, o.nbf, res["L"], Cm, batch=5)
+    assert np.abs(Jb - J).max() < 1e-12 * np.abs(J).max()
+    assert np.abs(Kb - K).max() < 1e-12 * np.abs(K).max()
+
+
 def test_gradient_vs_central_fd():
     mol = B.small_molecule(3, seed=7)
     o = O.Oracle(mol)
