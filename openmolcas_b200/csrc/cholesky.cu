@@ -208,6 +208,8 @@ struct ChoState {
   std::vector<int> piv, pass_of;
   int npass = 0;
   cublasHandle_t cublas = nullptr;
+  short* d_lexp = nullptr;      // row exponents of the square L_J (mixed J/K), M x lexp_ld
+  int lexp_ld = 0;
 };
 
 static const int kVecBlock = 1024;
@@ -215,7 +217,7 @@ static const int kVecBlock = 1024;
 void cho_free(ChoState* c) {
   if (!c) return;
   cudaFree(c->d_rs); cudaFree(c->d_sp_first); cudaFree(c->d_sp_count); cudaFree(c->d_rs_a); cudaFree(c->d_rs_b);
-  cudaFree(c->d_diag); cudaFree(c->d_diag0); cudaFree(c->d_inred);
+  cudaFree(c->d_diag); cudaFree(c->d_diag0); cudaFree(c->d_inred); cudaFree(c->d_lexp);
   for (auto p : c->Lblk) cudaFree(p);
   if (c->cublas) cublasDestroy(c->cublas);
   delete c;
@@ -587,5 +589,11 @@ const double* cho_vec_ptr(const ChoState* c, int J0, int nb, cudaStream_t, Handl
   return c->Lblk[J0 / kVecBlock] + (size_t)c->nrs * (J0 % kVecBlock);
 }
 int cho_vec_block() { return kVecBlock; }
+short* cho_lexp(const ChoState* c, int ld) { return c->lexp_ld == ld ? c->d_lexp : nullptr; }
+void cho_set_lexp(ChoState* c, short* p, int ld) {
+  cudaFree(c->d_lexp);
+  c->d_lexp = p;
+  c->lexp_ld = ld;
+}
 
 }  // namespace mg

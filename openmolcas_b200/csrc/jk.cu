@@ -186,48 +186,66 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// One warp per row (J, a) of a block of nb vectors (slice p starts at
-// LS + p * slice, the stride of the tensor map over a full block): gathers the square row
-// L_J[a, 0..n) from the rs-packed FP64 vectors through the inverse rs table,
-// writes its s slices LS[p][J*ld + a][0..ld) (zero beyond n) and the row
-// exponent eA[J*ld + a], and adds sum_b L_J[a,b] D[a,b] to V[J] (the Coulomb
-// contraction V_J = sum_cd L_cd,J D_cd over the full square).
-__global__ void k_oz_slice_l(const int* __restrict__ inv, int n, int64_t nrs, const double* __restrict__ L, int nb,
-                             int ld, int s, int64_t slice, const double* __restrict__ D, uint8_t* __restrict__ LS,
-                             int* __restrict__ eA, double* __restrict__ V) {
+// Row exponents of the square Cholesky vectors, computed once per
+// decomposition: one warp per row (J, a) gathers L_J[a, 0..n) from the
+// rs-packed FP64 vectors through the inverse rs table and stores the frexp
+// exponent of its largest |element| (0 for a zero row and for a >= n).
+__global__ void k_oz_lexp(const int* __restrict__ inv, int n, int64_t nrs, const double* __restrict__ L, int nb,
+                          int ld, short* __restrict__ eL) {
   const int lane = threadIdx.x & 31;
   const int64_t row = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
   if (row >= (int64_t)nb * ld) return;
   const int J = (int)(row / ld), a = (int)(row - (int64_t)J * ld);
   const double* LJ = L + nrs * J;
-  const int* ir = inv + (size_t)a * n;
-  double m = 0.0, v = 0.0;
+  double m = 0.0;
   if (a < n)
-    for (int b = lane; b < n; b += 32) {
-      const double x = LJ[ir[b]];
-      m = fmax(m, fabs(x));
-      v = fma(x, D[(size_t)a * n + b], v);
-    }
+    for (int b = lane; b < n; b += 32) m = fmax(m, fabs(LJ[inv[(size_t)a * n + b]]));
   m = warp_max(m);
-  v = warp_sum(v);
-  const int e = oz_exponent(m);
-  if (lane == 0) {
-    eA[row] = e;
-    if (a < n) atomicAdd(&V[J], v);
-  }
-  uint8_t* out = LS + (size_t)row * ld;
-  for (int b0 = 8 * lane; b0 < ld; b0 += 256) {
+  if (lane == 0) eL[row] = (short)max(-32000, oz_exponent(m));
+}
+
+// One thread per 8 consecutive columns of a row (J, a) of a block of nb
+// vectors (slice p starts at LS + p * slice, the stride of the tensor map
+// over a full block): gathers L_J[a, b0..b0+8) from the rs-packed FP64
+// vectors through the inverse rs table, writes the s slices
+// LS[p][J*ld + a][b0..b0+8) (zero beyond n) with the cached row exponent
+// eL[J*ld + a] (copied to eA for the epilogue), and adds
+// sum_b L_J[a,b] D[a,b] to V[J] (the Coulomb contraction
+// V_J = sum_cd L_cd,J D_cd over the full square).
+__global__ void k_oz_slice_l(const int* __restrict__ inv, int n, int64_t nrs, const double* __restrict__ L, int nb,
+                             int ld, int s, int64_t slice, const short* __restrict__ eL, const double* __restrict__ D,
+                             uint8_t* __restrict__ LS, int* __restrict__ eA, double* __restrict__ V) {
+  const int per_row = ld / 8;
+  const int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const bool live = o < (int64_t)nb * ld * per_row;
+  const int64_t row = live ? o / per_row : 0;
+  const int b0 = live ? 8 * (int)(o - row * per_row) : 0;
+  const int J = (int)(row / ld), a = (int)(row - (int64_t)J * ld);
+  const int e = eL[row];
+  double v = 0.0;
+  if (live) {
+    const double* LJ = L + nrs * J;
     uint32_t w[2 * kOzMaxSlices];
 #pragma unroll
     for (int k = 0; k < 2 * kOzMaxSlices; ++k) w[k] = 0;
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int b = b0 + u;
-      const double x = (a < n && b < n) ? LJ[ir[b]] : 0.0;
+      double x = 0.0;
+      if (a < n && b < n) {
+        x = LJ[inv[(size_t)a * n + b]];
+        v = fma(x, D[(size_t)a * n + b], v);
+      }
       oz_cut(ldexp(x, -e), s, w, u);
     }
-    for (int p = 0; p < s; ++p) *reinterpret_cast<uint2*>(out + p * slice + b0) = make_uint2(w[2 * p], w[2 * p + 1]);
+    uint8_t* out = LS + (size_t)row * ld + b0;
+    for (int p = 0; p < s; ++p) *reinterpret_cast<uint2*>(out + p * slice) = make_uint2(w[2 * p], w[2 * p + 1]);
+    if (b0 == 0) eA[row] = e;
   }
+  // V[J]: a warp covers one row when ld / 8 >= 32 (ld is a multiple of 128), so
+  // reduce over the warp and add once
+  v = warp_sum(v);
+  if (live && (threadIdx.x & 31) == 0 && a < n) atomicAdd(&V[J], v);
 }
 
 // C (n x r, column-major FP64) -> slices CS[q][k][0..ld) for k < npad
@@ -259,33 +277,42 @@ __global__ void k_oz_slice_c(const double* __restrict__ C, int n, int r, int npa
   }
 }
 
-// One warp per row a of X (FP64, row stride xrow, columns [0, kx)):
-// slices XS[p][a][col0 + 0..kblk) (zero beyond kx and for rows a >= n) and
-// the row exponent eX[a] over this block.
+// One thread per 8 consecutive columns of a row a of X (FP64, row stride
+// xrow, columns [0, kx)): slices XS[p][a][col0 + c0 .. +8) (zero beyond kx and
+// for rows a >= n) with the row exponent of xmax[a] (the largest |X| of the
+// row, recorded by the half-transform), stored in eX[a].
 __global__ void k_oz_slice_x(const double* __restrict__ X, int64_t xrow, int n, int kx, int ld, int kblk, int s,
-                             int64_t xs_row, int64_t col0, uint8_t* __restrict__ XS, int* __restrict__ eX) {
-  const int lane = threadIdx.x & 31;
-  const int a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (a >= ld) return;
+                             int64_t xs_row, int64_t col0, const unsigned long long* __restrict__ xmax,
+                             uint8_t* __restrict__ XS, int* __restrict__ eX) {
+  const int per_row = kblk / 8;
+  const int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (o >= (int64_t)ld * per_row) return;
+  const int a = (int)(o / per_row), c0 = 8 * (int)(o - (int64_t)a * per_row);
+  const int e = a < n ? oz_exponent(__longlong_as_double((long long)xmax[a])) : 0;
+  if (c0 == 0) eX[a] = e;
   const double* xa = X + (size_t)a * xrow;
+  uint32_t w[2 * kOzMaxSlices];
+#pragma unroll
+  for (int q = 0; q < 2 * kOzMaxSlices; ++q) w[q] = 0;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int c = c0 + u;
+    oz_cut(ldexp((a < n && c < kx) ? xa[c] : 0.0, -e), s, w, u);
+  }
+  const size_t slice = (size_t)ld * xs_row;
+  uint8_t* out = XS + (size_t)a * xs_row + col0 + c0;
+  for (int q = 0; q < s; ++q) *reinterpret_cast<uint2*>(out + q * slice) = make_uint2(w[2 * q], w[2 * q + 1]);
+}
+
+// xmax[a] = bits of max_c |X[a][c]| (for the self-test, where X is given)
+__global__ void k_row_absmax(const double* __restrict__ X, int64_t xrow, int n, int kx,
+                             unsigned long long* __restrict__ xmax) {
+  const int a = blockIdx.x;
   double m = 0.0;
   if (a < n)
-    for (int c = lane; c < kx; c += 32) m = fmax(m, fabs(xa[c]));
-  const int e = oz_exponent(warp_max(m));
-  if (lane == 0) eX[a] = e;
-  const size_t slice = (size_t)ld * xs_row;
-  uint8_t* out = XS + (size_t)a * xs_row + col0;
-  for (int c0 = 8 * lane; c0 < kblk; c0 += 256) {
-    uint32_t w[2 * kOzMaxSlices];
-#pragma unroll
-    for (int q = 0; q < 2 * kOzMaxSlices; ++q) w[q] = 0;
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int c = c0 + u;
-      oz_cut(ldexp((a < n && c < kx) ? xa[c] : 0.0, -e), s, w, u);
-    }
-    for (int q = 0; q < s; ++q) *reinterpret_cast<uint2*>(out + q * slice + c0) = make_uint2(w[2 * q], w[2 * q + 1]);
-  }
+    for (int c = threadIdx.x; c < kx; c += blockDim.x) m = fmax(m, fabs(X[(size_t)a * xrow + c]));
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(xmax + a, (unsigned long long)__double_as_longlong(m));
 }
 
 // jrs[t] += sum_J L[t, J] V[J] over one block of nb FP64 vectors
@@ -338,16 +365,45 @@ static bool make_slice_map(CUtensorMap* m, const uint8_t* base, int64_t kx, int6
 
 static inline int rup(int x, int m) { return (x + m - 1) / m * m; }
 
+// Column tiles of the half-transform: the widest multiple of 16 (<= 256)
+// whose s accumulators fit the 512 TMEM columns (one pass per tile), then
+// spread evenly over the r columns.
+static void oz_col_tiles(int r, int s, int& nnt, int& Nt) {
+  const int nmax = std::min(256, (512 / s) / 16 * 16);
+  nnt = (r + nmax - 1) / nmax;
+  Nt = rup((r + nnt - 1) / nnt, 16);
+}
+
 // Pass plan of one kind of output tile: accumulators of acc_stride TMEM
 // columns, at most 512 columns; shared-memory ring of the slices 0..s-1.
 static void oz_plan(OzArgs& a, int s, int Nt) {
   a.s = s;
   a.Nt = Nt;
-  a.acc_stride = rup(Nt, 32);
+  a.acc_stride = Nt;
   a.nd = std::min(s, 512 / a.acc_stride);
   a.b_bytes = rup(32 * Nt, 1024);
   a.stage_bytes = s * (kOzABytes + a.b_bytes);
   a.stages = std::min(kOzMaxStages, (kOzSmemLimit - 1024) / a.stage_bytes);
+}
+
+// Row exponents of the handle's Cholesky vectors for squares of ld rows
+// (computed once per decomposition, cached in the Cholesky state).
+static const short* oz_row_exponents(Handle* h, const int* inv, int ld, cudaStream_t st) {
+  ChoState* c = h->cho;
+  if (const short* e = cho_lexp(c, ld)) return e;
+  const int M = cho_nvec(c), n = h->nbf, vb = cho_vec_block();
+  const int64_t nrs = cho_nrs(c);
+  short* e = nullptr;
+  if (dev_malloc(&e, sizeof(short) * (size_t)M * ld) != cudaSuccess) return nullptr;
+  for (int J0 = 0; J0 < M; J0 += vb) {
+    const int nv = std::min(vb, M - J0);
+    const double* L = cho_vec_ptr(c, J0, nv, st, h);
+    const int64_t rows = (int64_t)nv * ld;
+    k_oz_lexp<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(inv, n, nrs, L, nv, ld, e + (size_t)J0 * ld);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+  cho_set_lexp(c, e, ld);
+  return e;
 }
 
 int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block, int s) {
@@ -357,9 +413,8 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   const int n = h->nbf;
   if (s < 2 || s > kOzMaxSlices) { h->err = "mixed J/K: slices must be 2..8"; return MG_ERR_ARG; }
   const int ld = rup(n, 128);
-  // column tiles of C: at most 256 rows per MMA
-  const int nnt = (r + 255) / 256;
-  const int Nt = rup((r + nnt - 1) / nnt, 16);
+  int nnt, Nt;
+  oz_col_tiles(r, s, nnt, Nt);
   const int npad = nnt * Nt;
   // vectors per block: one block's K extent of the exchange product, nb r
   const int nb = std::min(block, M);
@@ -379,8 +434,8 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   const size_t nn = (size_t)n * n;
   const int64_t xs_row = (int64_t)G * kblk;
   size_t need = 8 * (nrs + (size_t)nb + nn) + 4 * nn + (size_t)s * npad * ld + 4 * (size_t)npad +
-                (size_t)s * nb * ld * ld + 4 * (size_t)nb * ld + 8 * (size_t)n * kx + (size_t)s * ld * xs_row +
-                4 * (size_t)G * ld + 8 * (size_t)nsm * 128 * 128 + 16 * 256;
+                (size_t)s * nb * ld * ld + 4 * (size_t)nb * ld + 8 * (size_t)n * kx + 8 * (size_t)ld +
+                (size_t)s * ld * xs_row + 4 * (size_t)G * ld + 8 * (size_t)nsm * 128 * 128 + 17 * 256;
   char* ws = (char*)ws_get(h, need, st);
   if (!ws) { h->err = "jk workspace allocation failed"; return MG_ERR_MEMORY; }
   auto take = [&](size_t bytes) { char* p = ws; ws += (bytes + 255) & ~(size_t)255; return (void*)p; };
@@ -393,6 +448,7 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   uint8_t* LS = (uint8_t*)take((size_t)s * nb * ld * ld);
   int* eA = (int*)take(4 * (size_t)nb * ld);
   double* Xf = (double*)take(8 * (size_t)n * kx);
+  unsigned long long* xmax = (unsigned long long*)take(8 * (size_t)ld);
   uint8_t* XS = (uint8_t*)take((size_t)s * ld * xs_row);
   int* eX = (int*)take(4 * (size_t)G * ld);
   double* P = (double*)take(8 * (size_t)nsm * 128 * 128);
@@ -414,6 +470,7 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   }
   ax.err = ak.err = d_err;
   ax.nrt = ld / 128; ax.nnt = nnt; ax.ld = ld; ax.n = n; ax.r = r; ax.eA = eA; ax.eB = fC; ax.X = Xf; ax.xrow = kx;
+  ax.xmax = xmax;
   ak.ld = ld; ak.n = n; ak.ntile = ntile; ak.nsub = nsub; ak.kblk = kblk; ak.ksub = ksub; ak.eX = eX; ak.P = P;
   ak.K = d_K;
   cudaMemsetAsync(d_err, 0, sizeof(int), st);
@@ -423,6 +480,8 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   cudaMemsetAsync(d_K, 0, 8 * nn, st);
   k_rs_inverse<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, n, inv);
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  const short* eL = oz_row_exponents(h, inv, ld, st);
+  if (!eL) { h->err = "mixed J/K: row exponents could not be stored"; return MG_ERR_MEMORY; }
   k_oz_slice_c<<<(npad + 7) / 8, 256, 0, st>>>(d_C, n, r, npad, ld, s, CS, fC);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   for (int g0 = 0; g0 < nblocks; g0 += G) {
@@ -435,9 +494,10 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
       // a short last block: clear the columns of the missing vectors
       if (nv < nb) cudaMemsetAsync(Xf, 0, 8 * (size_t)n * kx, st);
       cudaMemsetAsync(V, 0, 8 * (size_t)nb, st);
-      const int64_t rows = (int64_t)nv * ld;
-      k_oz_slice_l<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(inv, n, nrs, Lb, nv, ld, s, (int64_t)nb * ld * ld, D,
-                                                                LS, eA, V);
+      cudaMemsetAsync(xmax, 0, 8 * (size_t)ld, st);
+      const int64_t nthr = (int64_t)nv * ld * (ld / 8);
+      k_oz_slice_l<<<nb256(nthr), 256, 0, st>>>(inv, n, nrs, Lb, nv, ld, s, (int64_t)nb * ld * ld,
+                                               eL + (size_t)J0 * ld, D, LS, eA, V);
       g_launches.fetch_add(1, std::memory_order_relaxed);
       k_jacc64<<<nb256(nrs), 256, 0, st>>>(Lb, nrs, nv, V, jrs);
       g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -447,8 +507,8 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
       const int gx = std::min(ax.nitems, nsm);
       oz_gemm_kernel<false><<<gx, kOzThreads, ax.stages * ax.stage_bytes + 1024, st>>>(map_l, map_c, ax);
       g_launches.fetch_add(1, std::memory_order_relaxed);
-      k_oz_slice_x<<<(ld + 7) / 8, 256, 0, st>>>(Xf, kx, n, kx, ld, kblk, s, xs_row, (int64_t)bi * kblk, XS,
-                                                eX + (size_t)bi * ld);
+      k_oz_slice_x<<<nb256((int64_t)ld * (kblk / 8)), 256, 0, st>>>(Xf, kx, n, kx, ld, kblk, s, xs_row,
+                                                                   (int64_t)bi * kblk, xmax, XS, eX + (size_t)bi * ld);
       g_launches.fetch_add(1, std::memory_order_relaxed);
     }
     // K += X X^T over the group (lower tiles)
@@ -479,8 +539,8 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
 int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double* d_B, double* d_X, double* d_K,
                 uint8_t* d_slices, int* d_exps, cudaStream_t st) {
   if (ld < 128 || ld % 128 || r < 1 || s < 2 || s > kOzMaxSlices) return MG_ERR_ARG;
-  const int nnt = (r + 255) / 256;
-  const int Nt = rup((r + nnt - 1) / nnt, 16);
+  int nnt, Nt;
+  oz_col_tiles(r, s, nnt, Nt);
   const int npad = nnt * Nt;
   const int kblk = rup(r, 32);
   const int nsub = (kblk + kOzKChunk - 1) / kOzKChunk;
@@ -488,7 +548,8 @@ int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
   const size_t need = (size_t)s * ld * ld + 4 * (size_t)ld + (size_t)s * npad * ld + 4 * (size_t)npad +
-                      (size_t)s * ld * kblk + 4 * (size_t)ld + 8 * (size_t)nsm * 128 * 128 + 16 * 256;
+                      (size_t)s * ld * kblk + 4 * (size_t)ld + 16 * (size_t)ld + 8 * (size_t)nsm * 128 * 128 +
+                      18 * 256;
   char* ws = (char*)ws_get(h, need, st);
   if (!ws) return MG_ERR_MEMORY;
   auto take = [&](size_t bytes) { char* p = ws; ws += (bytes + 255) & ~(size_t)255; return (void*)p; };
@@ -498,6 +559,8 @@ int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double
   int* fC = (int*)take(4 * (size_t)npad);
   uint8_t* XS = (uint8_t*)take((size_t)s * ld * kblk);
   int* eX = (int*)take(4 * (size_t)ld);
+  unsigned long long* amax = (unsigned long long*)take(8 * (size_t)ld);
+  unsigned long long* xmax = (unsigned long long*)take(8 * (size_t)ld);
   double* P = (double*)take(8 * (size_t)nsm * 128 * 128);
   int* d_err = (int*)take(sizeof(int));
   CUtensorMap map_l, map_c, map_x;
@@ -512,21 +575,24 @@ int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double
     return MG_ERR_CUDA;
   ax.err = ak.err = d_err;
   ax.nrt = ld / 128; ax.nnt = nnt; ax.ld = ld; ax.n = ld; ax.r = r; ax.eA = eA; ax.eB = fC; ax.X = d_X; ax.xrow = r;
-  ax.nJ = 1; ax.nitems = ax.nrt * nnt;
+  ax.xmax = xmax; ax.nJ = 1; ax.nitems = ax.nrt * nnt;
   ak.ld = ld; ak.n = ld; ak.ntile = (ld / 128) * (ld / 128 + 1) / 2; ak.nsub = nsub; ak.kblk = kblk; ak.ksub = ksub;
   ak.eX = eX; ak.P = P; ak.K = d_K; ak.nblk = 1; ak.nitems = ak.ntile * nsub;
   cudaMemsetAsync(d_err, 0, sizeof(int), st);
   cudaMemsetAsync(d_K, 0, 8 * (size_t)ld * ld, st);
-  k_oz_slice_x<<<(ld + 7) / 8, 256, 0, st>>>(d_A, ld, ld, ld, ld, ld, s, ld, 0, LS, eA);
+  cudaMemsetAsync(amax, 0, 8 * (size_t)ld, st);
+  cudaMemsetAsync(xmax, 0, 8 * (size_t)ld, st);
+  k_row_absmax<<<ld, 256, 0, st>>>(d_A, ld, ld, ld, amax);
+  k_oz_slice_x<<<nb256((int64_t)ld * (ld / 8)), 256, 0, st>>>(d_A, ld, ld, ld, ld, ld, s, ld, 0, amax, LS, eA);
   if (d_slices) cudaMemcpyAsync(d_slices, LS, (size_t)s * ld * ld, cudaMemcpyDeviceToDevice, st);
   if (d_exps) cudaMemcpyAsync(d_exps, eA, 4 * (size_t)ld, cudaMemcpyDeviceToDevice, st);
   k_oz_slice_c<<<(npad + 7) / 8, 256, 0, st>>>(d_B, ld, r, npad, ld, s, CS, fC);
   oz_gemm_kernel<false><<<std::min(ax.nitems, nsm), kOzThreads, ax.stages * ax.stage_bytes + 1024, st>>>(map_l, map_c,
                                                                                                        ax);
-  k_oz_slice_x<<<(ld + 7) / 8, 256, 0, st>>>(d_X, r, ld, r, ld, kblk, s, kblk, 0, XS, eX);
+  k_oz_slice_x<<<nb256((int64_t)ld * (kblk / 8)), 256, 0, st>>>(d_X, r, ld, r, ld, kblk, s, kblk, 0, xmax, XS, eX);
   oz_gemm_kernel<true><<<std::min(ak.nitems, nsm), kOzThreads, ak.stages * ak.stage_bytes + 1024, st>>>(map_x, map_x,
                                                                                                       ak);
-  g_launches.fetch_add(5, std::memory_order_relaxed);
+  g_launches.fetch_add(6, std::memory_order_relaxed);
   if (cudaGetLastError() != cudaSuccess) return MG_ERR_CUDA;
   int herr = 0;
   cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);

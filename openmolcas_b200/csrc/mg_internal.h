@@ -170,6 +170,9 @@ const int* cho_rs_a_dev(const ChoState* c);
 const int* cho_rs_b_dev(const ChoState* c);
 const double* cho_vec_ptr(const ChoState* c, int J0, int nb, cudaStream_t st, Handle* h);
 int cho_vec_block();
+// cached row exponents of the square Cholesky vectors (M x ld), owned by the state
+short* cho_lexp(const ChoState* c, int ld);
+void cho_set_lexp(ChoState* c, short* p, int ld);
 int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double* d_B, double* d_X, double* d_K,
                 uint8_t* d_slices, int* d_exps, cudaStream_t st);
 int fock_accumulate(double* F, const double* J, const double* K, double factxi, int64_t n, cudaStream_t st);

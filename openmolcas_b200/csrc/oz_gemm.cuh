@@ -27,7 +27,10 @@
 //                   a CTA-private FP64 tile (exchange product)
 // The diagonals of one output tile are computed in passes of at most nd
 // accumulators (nd * acc_stride <= 512 TMEM columns); a pass loads only the
-// slices it needs.  Every mbarrier wait is bounded: a wait that runs out sets
+// slices it needs.  The half-transform picks its column tile so that all s
+// diagonals fit (one pass: the epilogue writes X once and records every row's
+// largest |X| for the slicing that follows); the exchange product runs its
+// 128 x 128 tiles in passes of 4 diagonals into CTA-private FP64 tiles.  Every mbarrier wait is bounded: a wait that runs out sets
 // *err, the CTA stops issuing work, waits (bounded) for its own loads and
 // MMAs in flight and still frees its tensor memory.
 #pragma once
@@ -66,6 +69,7 @@ struct OzArgs {
   const int* eB;   // column exponents of C, [k]
   double* X;       // X[a * xrow + J * r + k] (FP64)
   long long xrow;
+  unsigned long long* xmax;  // per row a: bits of the largest |X| written (atomicMax)
   // exchange product K += X X^T (SYRK == true): items (lower tile, block, sub-chunk)
   int ntile, nblk, nsub;
   int kblk;        // K extent of one block (multiple of 32)
@@ -259,16 +263,17 @@ __global__ void __launch_bounds__(kOzThreads, 1)
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       if (ok) {
         const int ncol = SYRK ? 128 : a.Nt;
-        for (int c0 = 0; c0 < ncol; c0 += 32) {
-          double sum[32];
+        double rmax = 0.0;
+        for (int c0 = 0; c0 < ncol; c0 += 16) {
+          double sum[16];
 #pragma unroll
-          for (int i = 0; i < 32; ++i) sum[i] = 0.0;
+          for (int i = 0; i < 16; ++i) sum[i] = 0.0;
           for (int d = u.d0; d < u.d1; ++d) {
-            uint32_t v[32];
-            tc_ld32(tl + (uint32_t)((d - u.d0) * a.acc_stride + c0), v);
+            uint32_t v[16];
+            tc_ld16(tl + (uint32_t)((d - u.d0) * a.acc_stride + c0), v);
             const double w = ldexp(1.0, -14 - 8 * d);
 #pragma unroll
-            for (int i = 0; i < 32; ++i) sum[i] = fma((double)(int)v[i], w, sum[i]);
+            for (int i = 0; i < 16; ++i) sum[i] = fma((double)(int)v[i], w, sum[i]);
           }
           if (!SYRK) {
             const int arow = u.t0 * 128 + row;
@@ -276,11 +281,12 @@ __global__ void __launch_bounds__(kOzThreads, 1)
               const int ea = a.eA[u.J * a.ld + arow];
               double* xr = a.X + (size_t)arow * a.xrow + (size_t)u.J * a.r;
 #pragma unroll
-              for (int i = 0; i < 32; ++i) {
+              for (int i = 0; i < 16; ++i) {
                 const int k = u.nt * a.Nt + c0 + i;
-                if (k < a.r && c0 + i < a.Nt) {
+                if (k < a.r) {
                   const double val = ldexp(sum[i], ea + a.eB[k]);
                   xr[k] = u.first ? val : xr[k] + val;
+                  rmax = fmax(rmax, fabs(val));
                 }
               }
             }
@@ -289,12 +295,14 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             const int* eb = a.eX + u.J * a.ld + u.t1 * 128 + c0;
             double* pr = a.P + (size_t)blockIdx.x * 128 * 128 + (size_t)row * 128 + c0;
 #pragma unroll
-            for (int i = 0; i < 32; ++i) {
+            for (int i = 0; i < 16; ++i) {
               const double val = ldexp(sum[i], ea + eb[i]);
               pr[i] = u.first ? val : pr[i] + val;
             }
           }
         }
+        if (!SYRK && u.last && rmax > 0.0)  // (a single pass: the values written are final)
+          atomicMax(a.xmax + u.t0 * 128 + row, (unsigned long long)__double_as_longlong(rmax));
         if (SYRK && u.last) {
           // this CTA's share of the tile is complete: add it into K
           const int arow = u.t0 * 128 + row;
