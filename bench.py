@@ -39,6 +39,7 @@ GRAD_CFG = "c4"
 ERI_CFG = "c2"
 ERI_SAMPLE = 2_000_000
 C3_NVEC = 12865  # Cholesky vectors of the 1500-function cluster at ThrCom 1e-6
+JK_SLICES = (6, 7)  # 8-bit slices of MG_PREC_MIXED: half-transform, exchange product (include/molgpu.h)
 THRCOM = 1e-6
 CUTINT = 1e-12
 
@@ -246,11 +247,20 @@ def eri_cpu_baseline(sel, budget_s=10.0, threads=None):
 def setup(torch, device):
     from openmolcas_b200 import basis as B
     from openmolcas_b200.molgpu import MolGpu
-    t0 = time.time()
     m3 = B.config_molecule(JK_CFG)
     g3 = MolGpu(m3, device)
+    g3.schwarz()  # basis set-up outside the decomposition's clock
+    import torch as _t
+    _t.cuda.synchronize()
+    t0 = time.time()
     info = g3.cho_drv(thrcom=THRCOM)
     t_cho = time.time() - t0
+    # bytes the passes' column updates must read: the previous vectors once per pass
+    # (X -= L LQ^T reads nrs x M_prev FP64 values, Cho_VecBuf_Subtr)
+    _, pass_of = g3.cho_pivots()
+    counts = np.bincount(pass_of, minlength=info["npass"])
+    m_prev = np.concatenate([[0], np.cumsum(counts)[:-1]])
+    info["subtr_bytes"] = float(8.0 * info["nrs"] * m_prev.sum())
     C3 = torch.from_numpy(B.density_factor(m3.nbf, B.CONFIGS[JK_CFG]["rank"], B.CONFIGS[JK_CFG]["seed"]))
     m4 = B.config_molecule(GRAD_CFG)
     g4 = MolGpu(m4, device)
@@ -383,14 +393,29 @@ def run_gpu(args, rank, world):
     peaks, src = _peaks()
     fp64_peak = measure_fp64_peak(torch)
     n, r, M = g3.nbf, C3.shape[1], S["cho"]["M"]
-    jk_flops = 4.0 * n * n * r * M  # half-transform + K contraction (ideal, exact FP32 products)
+    jk_flops = 4.0 * n * n * r * M  # half-transform + exchange product, exact (FP64-equivalent) flops
     jk_s = float(jk_m.mean()) / 1e3
     gr_s = float(gr_m.mean()) / 1e3
     gflops = grad_flops(g4)
+    # issued 8-bit tensor work of the sliced exchange GEMMs: s(s+1)/2 products of the
+    # padded shapes (half-transform: ld x npad x ld per vector; exchange product: the
+    # lower 128 x 128 tiles of ld x ld over M r); int8 dense peak taken as twice the
+    # measured BF16 burst (the B200 rates are 4.5 and 2.25 dense POPS/PFLOPS)
+    sx, sk = JK_SLICES
+    ld = -(-n // 128) * 128
+    nmax = min(256, (512 // sx) // 16 * 16)
+    nnt = -(-r // nmax)
+    npad = nnt * (-(-(-(-r // nnt)) // 16) * 16)
+    ntile = (ld // 128) * (ld // 128 + 1) // 2
+    i8_ops = (sx * (sx + 1) // 2) * 2.0 * ld * npad * ld * M + (sk * (sk + 1) // 2) * 2.0 * ntile * 128 * 128 * (M * r)
+    i8_peak = 2.0 * peaks["bf16_tflops"]
     legs = {
-        "jk": {"bound": "tensor", "achieved": jk_flops / jk_s / 1e12, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
-               "frac": jk_flops / jk_s / 1e12 / peaks["bf16_tflops"], "peak_source": f"{src} bf16 burst",
-               "algorithmic_flops": jk_flops, "seconds": jk_s},
+        "jk": {"bound": "tensor", "achieved": i8_ops / jk_s / 1e12, "peak": i8_peak, "unit": "TOP/s (int8)",
+               "frac": i8_ops / jk_s / 1e12 / i8_peak,
+               "peak_source": f"{src}: 2 x measured bf16 burst (int8 dense = 2 x bf16 dense on B200)",
+               "algorithmic_int8_ops": i8_ops, "slices": {"half_transform": sx, "exchange": sk},
+               "fp64_equivalent_flops": jk_flops,
+               "fp64_equivalent_tflops": jk_flops / jk_s / 1e12, "seconds": jk_s},
         "grad": {"bound": "fp64", "achieved": gflops / gr_s / 1e12 if gflops else None, "peak": fp64_peak,
                  "unit": "TFLOP/s", "frac": (gflops / gr_s / 1e12 / fp64_peak) if (gflops and fp64_peak) else None,
                  "peak_source": "DFMA microbenchmark measured in this run", "algorithmic_flops": gflops,
@@ -417,7 +442,8 @@ def run_gpu(args, rank, world):
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64 (gradient, Cholesky); fp32 vectors x split-bf16 (J/K)" if prec_mixed else "f64",
+        "dtype": ("f64 (gradient, Cholesky, vectors); J/K exchange in 8-bit slices of the f64 vectors with exact "
+                  "int32 tensor-core accumulation" if prec_mixed else "f64"),
         "data": "synthetic (seeded molecules, random contractions and densities)",
         "config": {"workload": f"J/K: {JK_CFG} 120 atoms {g3.nbf} bf, M={M} Cholesky vectors (ThrCom {THRCOM}), "
                                f"rank {r} density; gradient: {GRAD_CFG} 20 atoms {g4.nbf} bf, rank 40 density, "
@@ -427,7 +453,14 @@ def run_gpu(args, rank, world):
         "fp64_path_s": step_d,
         "speedup_vs_fp64_path": step_d / (ms / 1e3),
         "energy": {"E_mixed": E_m, "E_fp64": E_d, "dE": E_m - E_d},
-        "cholesky": {"M": M, "npass": S["cho"]["npass"], "setup_s": S["t_cho"]},
+        "cholesky": {"M": M, "npass": S["cho"]["npass"], "seconds": S["t_cho"],
+                     "roofline": {"bound": "hbm", "achieved": S["cho"]["subtr_bytes"] / S["t_cho"] / 1e9,
+                                  "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                                  "frac": S["cho"]["subtr_bytes"] / S["t_cho"] / 1e9 / peaks["hbm_gbs"],
+                                  "algorithmic_bytes": S["cho"]["subtr_bytes"],
+                                  "note": "bytes = the previous vectors read once per pass by the column update "
+                                          "(sum over passes of nrs x M_prev x 8); the passes' ERI columns and "
+                                          "host qualification are inside the time"}},
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches // max(1, args.steps)),
         "roofline": roof,

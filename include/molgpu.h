@@ -150,16 +150,20 @@ int mg_cho_diag(mg_handle* h, double* d_diag, void* stream);
  * (the reference accumulates into FLT/KLT; mg_cho_lk_scf below does).
  * precision:
  *   MG_PREC_FP64     FP64 vectors, FP64 products (DGEMM/DSYRK);
- *   MG_PREC_MIXED    FP64 vectors cut into MG_JK_SLICES 8-bit slices per row
- *                    (power-of-two row scaling), both exchange GEMMs on the
- *                    tensor cores in 8-bit integers with exact INT32
- *                    accumulation, FP64 recombination; Coulomb part FP64;
- *   MG_PREC_SLICED(s) the same with s slices (2..8).
+ *   MG_PREC_MIXED    FP64 vectors cut into 8-bit slices per row (power-of-two
+ *                    row scaling): MG_JK_SLICES for the half-transform
+ *                    X_J = L_J C, MG_JK_SLICES_K for the exchange product
+ *                    K = sum X X^T; both GEMMs on the tensor cores in 8-bit
+ *                    integers with exact INT32 accumulation and FP64
+ *                    recombination; Coulomb part FP64.  Energy within 1e-8 Eh
+ *                    of MG_PREC_FP64 at 1500 functions / 12865 vectors;
+ *   MG_PREC_SLICED(s) the same with s slices for both GEMMs (2..8).
  */
 #define MG_PREC_FP64 0
 #define MG_PREC_MIXED 1
 #define MG_PREC_SLICED(s) (100 + (s))
 #define MG_JK_SLICES 6
+#define MG_JK_SLICES_K 7
 int mg_cho_jk(mg_handle* h, const double* d_C, int r, double* d_J, double* d_K, int precision, void* stream);
 /* The accumulating form of CHO_LK_SCF (fock_util/cho_lk_scf.F90:14, one
  * density): d_FLT += J[D] - factxi * K[D] (FLT nbf x nbf, device), the sum the
@@ -203,12 +207,14 @@ double mg_drvg1_flops(mg_handle* h, double cutint);
 int mg_rys_roots(mg_handle* h, int nrys, int64_t n, const double* T, double* x, double* w);
 
 /* The 8-bit sliced tensor-core engine of MG_PREC_MIXED on given dense FP64
- * matrices (verification; no reference counterpart): X = A B^T with A
- * (ld x ld) and B (r x ld) row-major, X row-major (ld x r), then
- * K = X X^T into the lower triangle of K (column-major ld x ld; the upper
- * part of the diagonal 128 x 128 tiles is also written).  ld a multiple of
+ * matrices (verification; no reference counterpart): X = A B with A
+ * (ld x ld), B (ld x r) and X (ld x r) column-major, then K = X X^T into
+ * the lower triangle of K (column-major ld x ld; the upper part of the
+ * diagonal 128 x 128 tiles is also written).  ld a multiple of
  * 128, slices 2..8.  d_slices (slices x ld x ld bytes) and d_exps (ld ints),
- * when not NULL, receive the 8-bit slices and row exponents of A.
+ * when not NULL, receive the 8-bit slices and row exponents of A; slice p
+ * holds A's element (i, k) at byte ((i / 128) (ld / 32) + k / 32) 4096 +
+ * (i % 128) 32 + k % 32 (tiles of 128 rows x 32 columns, each contiguous).
  * Synchronous. */
 int mg_sliced_selftest(mg_handle* h, int ld, int r, int slices, const double* d_A, const double* d_B, double* d_X,
                        double* d_K, void* d_slices, int* d_exps, void* stream);

@@ -514,9 +514,10 @@ int mg_cho_jk(mg_handle* H, const double* d_C, int r, double* d_J, double* d_K, 
   if (!h->cho) { h->err = "mg_cho_jk: no Cholesky vectors (call mg_cho_drv)"; return MG_ERR_ARG; }
   cudaSetDevice(h->device);
   if (precision == MG_PREC_FP64) return jk_fp64(h, d_C, r, d_J, d_K, (cudaStream_t)stream, 32);
-  if (precision == MG_PREC_MIXED) return jk_mixed(h, d_C, r, d_J, d_K, (cudaStream_t)stream, 64, MG_JK_SLICES);
+  if (precision == MG_PREC_MIXED)
+    return jk_mixed(h, d_C, r, d_J, d_K, (cudaStream_t)stream, 64, MG_JK_SLICES, MG_JK_SLICES_K);
   if (precision > 100 && precision <= 108)
-    return jk_mixed(h, d_C, r, d_J, d_K, (cudaStream_t)stream, 64, precision - 100);
+    return jk_mixed(h, d_C, r, d_J, d_K, (cudaStream_t)stream, 64, precision - 100, precision - 100);
   h->err = "mg_cho_jk: unsupported precision";
   return MG_ERR_ARG;
 }

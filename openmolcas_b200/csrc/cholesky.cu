@@ -378,7 +378,7 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
     }
     std::vector<int64_t> off;
     eri_blocks(h, q4, off, buf, bufsz, st, rc);
-    if (rc) { err = "diagonal integrals failed"; cudaFree(buf); cudaFree(d_tmp); return rc; }
+    if (rc) { err = "diagonal integrals failed: " + err; cudaFree(buf); cudaFree(d_tmp); return rc; }
     int64_t* d_off = nullptr;
     dev_malloc(&d_off, sizeof(int64_t) * nsp);
     cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * nsp, cudaMemcpyHostToDevice, st);
@@ -461,7 +461,7 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
     }
     std::vector<int64_t> off;
     eri_blocks(h, q4, off, buf, bufsz, st, rc);
-    if (rc) { err = "column integrals failed"; break; }
+    if (rc) { err = "column integrals failed: " + err; break; }
     std::fill(off_sp.begin(), off_sp.end(), -1);
     for (size_t t = 0; t < qsp.size(); ++t) off_sp[qsp[t]] = off[t];
     cudaMemcpyAsync(d_off, off_sp.data(), sizeof(int64_t) * nsp, cudaMemcpyHostToDevice, st);
@@ -589,6 +589,7 @@ const double* cho_vec_ptr(const ChoState* c, int J0, int nb, cudaStream_t, Handl
   return c->Lblk[J0 / kVecBlock] + (size_t)c->nrs * (J0 % kVecBlock);
 }
 int cho_vec_block() { return kVecBlock; }
+const int64_t* cho_sp_first_dev(const ChoState* c) { return c->d_sp_first; }
 short* cho_lexp(const ChoState* c, int ld) { return c->lexp_ld == ld ? c->d_lexp : nullptr; }
 void cho_set_lexp(ChoState* c, short* p, int ld) {
   cudaFree(c->d_lexp);

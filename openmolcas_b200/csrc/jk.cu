@@ -6,8 +6,9 @@
 //   J_ab = sum_J L_ab,J V_J,  V_J = sum_cd L_cd,J D_cd     (cho_lk_scf.F90:442-449)
 //   K_ab = sum_J sum_k X_J[a,k] X_J[b,k],  X_J = L_J C      (cho_lk_scf.F90:507-830)
 //
-// Mixed path: the FP64 vectors are cut into s 8-bit slices per row
-// (oz_gemm.cuh gives the scheme) and both exchange GEMMs run on the tcgen05
+// Mixed path: the FP64 vectors are cut into 8-bit slices per row (oz_gemm.cuh
+// gives the scheme; s slices for the half-transform, sk for the exchange
+// product, whose error dominates) and both exchange GEMMs run on the tcgen05
 // tensor cores in 8-bit integers with exact INT32 accumulation: per block of
 // vectors, a slicing kernel unpacks the rs-packed L_J into sliced dense
 // squares (and forms the Coulomb contractions V_J on the way), the
@@ -28,6 +29,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "kern_common.cuh"
@@ -148,28 +150,73 @@ int jk_fp64(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaS
 }
 
 // ------------------------------------------------------------ mixed path
-// Slicing of one value y in (-1, 1) into s 8-bit pieces (oz_gemm.cuh):
-// byte p of the result, S_0 signed, U_p (p >= 1) unsigned.  Every slice but
-// the last is a floor (remainder in [0, 1)); the last one is rounded to
-// nearest (clamped to 255), so the dropped tail has no systematic sign.
-__device__ __forceinline__ void oz_cut(double y, int s, uint32_t (&w)[2 * kOzMaxSlices], int u) {
-  const int word = u >> 2, sh = 8 * (u & 3);
-  double t = floor(y * 128.0);
-  y = y * 128.0 - t;
-  // a tiny negative y (|128 y| < 2^-53) leaves 1 - |128 y|, which rounds to
-  // exactly 1: carry it back (the value is then 0 to within 2^-53 of the row
-  // maximum) so that every later slice stays within [0, 255]
-  if (y >= 1.0) {
-    t += 1.0;
-    y -= 1.0;
+// Slicing of one value x of a row with exponent e (y = x 2^-e in (-1, 1))
+// into S 8-bit pieces (oz_gemm.cuh): y as the S-byte two's-complement
+// fixed-point integer Y = floor(y 2^(8S-1)), its lowest byte rounded to
+// nearest where that does not carry out of the byte; slice p is byte S-1-p
+// of Y (S_0 the signed top byte, U_p unsigned), so every slice but the last
+// is the floor digit and the dropped tail is below one unit of the last.
+struct OzScale {
+  double lo, hi;  // 2^(8S-1-e) as two factors, each a normal double
+};
+
+template <int S>
+__device__ __forceinline__ OzScale oz_scale(int e) {
+  const int k = 8 * S - 1 - e, k1 = k >> 1;  // e in [-1073, 1024]: both halves in range
+  return {oz_pow2(k1), oz_pow2(k - k1)};
+}
+
+template <int S>
+__device__ __forceinline__ long long oz_fixed(double x, OzScale sc) {
+  const double z = (x * sc.lo) * sc.hi;  // exact power-of-two scaling, |z| < 2^(8S-1)
+  long long y;
+  double frac;
+  if (S <= 6) {
+    // |z| < 2^47: adding 1.5 2^52 rounded down leaves floor(z) in the low
+    // mantissa bits (the unit in the last place is 1 there), on the adder
+    constexpr double kM = 6755399441055744.0;  // 1.5 2^52
+    const double t = __dadd_rd(z, kM);
+    y = (__double_as_longlong(t) & ((1ll << 52) - 1)) - (1ll << 51);
+    frac = z - (t - kM);  // both differences exact
+  } else {
+    y = __double2ll_rd(z);
+    frac = z - (double)y;  // exact: z is integral beyond 2^52
   }
-  w[word] |= ((uint32_t)(int)t & 255u) << sh;
-  for (int p = 1; p < s; ++p) {
-    t = p + 1 < s ? floor(y * 256.0) : fmin(floor(fma(y, 256.0, 0.5)), 255.0);
-    w[2 * p + word] |= ((uint32_t)(int)t & 255u) << sh;
-    y = y * 256.0 - t;
+  if (frac >= 0.5 && (y & 255) != 255) ++y;
+  return y;
+}
+
+// slice p of 8 consecutive values: out[p] holds their bytes S-1-p
+template <int S>
+__device__ __forceinline__ void oz_pack8(const long long (&y)[8], uint2 (&out)[S]) {
+#pragma unroll
+  for (int p = 0; p < S; ++p) {
+    const int sh = 8 * (S - 1 - p);
+    uint32_t lo = 0, hi = 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      lo |= (uint32_t)((y[u] >> sh) & 255) << (8 * u);
+      hi |= (uint32_t)((y[4 + u] >> sh) & 255) << (8 * u);
+    }
+    out[p] = make_uint2(lo, hi);
   }
 }
+
+// f(std::integral_constant<int, s>) for s = 2..kOzMaxSlices
+template <typename F>
+static bool oz_with_slices(int s, F&& f) {
+  switch (s) {
+    case 2: f(std::integral_constant<int, 2>{}); return true;
+    case 3: f(std::integral_constant<int, 3>{}); return true;
+    case 4: f(std::integral_constant<int, 4>{}); return true;
+    case 5: f(std::integral_constant<int, 5>{}); return true;
+    case 6: f(std::integral_constant<int, 6>{}); return true;
+    case 7: f(std::integral_constant<int, 7>{}); return true;
+    case 8: f(std::integral_constant<int, 8>{}); return true;
+  }
+  return false;
+}
+static_assert(kOzMaxSlices == 8, "oz_with_slices covers 2..8 slices");
 
 __device__ __forceinline__ int oz_exponent(double m) {
   int e = 0;
@@ -204,55 +251,108 @@ __global__ void k_oz_lexp(const int* __restrict__ inv, int n, int64_t nrs, const
   if (lane == 0) eL[row] = (short)max(-32000, oz_exponent(m));
 }
 
-// One thread per 8 consecutive columns of a row (J, a) of a block of nb
-// vectors (slice p starts at LS + p * slice, the stride of the tensor map
-// over a full block): gathers L_J[a, b0..b0+8) from the rs-packed FP64
-// vectors through the inverse rs table, writes the s slices
-// LS[p][J*ld + a][b0..b0+8) (zero beyond n) with the cached row exponent
-// eL[J*ld + a] (copied to eA for the epilogue), and adds
-// sum_b L_J[a,b] D[a,b] to V[J] (the Coulomb contraction
-// V_J = sum_cd L_cd,J D_cd over the full square).
-__global__ void k_oz_slice_l(const int* __restrict__ inv, int n, int64_t nrs, const double* __restrict__ L, int nb,
-                             int ld, int s, int64_t slice, const short* __restrict__ eL, const double* __restrict__ D,
-                             uint8_t* __restrict__ LS, int* __restrict__ eA, double* __restrict__ V) {
-  const int per_row = ld / 8;
-  const int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const bool live = o < (int64_t)nb * ld * per_row;
-  const int64_t row = live ? o / per_row : 0;
-  const int b0 = live ? 8 * (int)(o - row * per_row) : 0;
-  const int J = (int)(row / ld), a = (int)(row - (int64_t)J * ld);
-  const int e = eL[row];
-  double v = 0.0;
-  if (live) {
-    const double* LJ = L + nrs * J;
-    uint32_t w[2 * kOzMaxSlices];
-#pragma unroll
-    for (int k = 0; k < 2 * kOzMaxSlices; ++k) w[k] = 0;
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int b = b0 + u;
-      double x = 0.0;
-      if (a < n && b < n) {
-        x = LJ[inv[(size_t)a * n + b]];
-        v = fma(x, D[(size_t)a * n + b], v);
-      }
-      oz_cut(ldexp(x, -e), s, w, u);
-    }
-    uint8_t* out = LS + (size_t)row * ld + b0;
-    for (int p = 0; p < s; ++p) *reinterpret_cast<uint2*>(out + p * slice) = make_uint2(w[2 * p], w[2 * p + 1]);
-    if (b0 == 0) eA[row] = e;
+// L slicing in blocks: one CTA per (column chunk of 256, block of 16 AO rows,
+// vector J).  Thread t owns column b = c0 + t and loads the 16 elements
+// L_J[a0..a0+16, b] straight from the rs-packed vector, the rs index worked
+// out from the shells of a and b (pair (I, J') with I > J' stores a-fastest,
+// I < J' the mirror, I = J' a triangle, plf_cho_diag.F90:60-72), all 16 loads
+// in flight at once; it cuts them with the cached row exponents into a byte
+// tile in shared memory (S x 16 rows x 256 columns), which the CTA then
+// writes out row by row in 16-byte pieces.  Columns b >= n are zero.
+// sh_off[ns + 1]: first AO of every shell (sh_off[ns] = n); ao_sh[n]: the
+// shell of every AO.
+constexpr int kOzChunk = 256;   // columns per CTA (= threads)
+constexpr int kOzRows = 16;     // AO rows per CTA
+
+template <int S>
+__global__ void __launch_bounds__(kOzChunk) k_oz_slice_l_blocks(const int64_t* __restrict__ sp_first,
+                                                                const int* __restrict__ sh_off,
+                                                                const int* __restrict__ ao_sh, int n, int64_t nrs,
+                                                                const double* __restrict__ L, int ld, int64_t slice,
+                                                                const short* __restrict__ eL,
+                                                                const double* __restrict__ D,
+                                                                uint8_t* __restrict__ LS, int* __restrict__ eA,
+                                                                double* __restrict__ V) {
+  __shared__ __align__(16) uint8_t Sb[S][kOzRows][kOzChunk];
+  __shared__ OzScale sc[kOzRows];
+  __shared__ int rI[kOzRows], rla[kOzRows], rnA[kOzRows];  // shell, index in it, its width
+  __shared__ double red[kOzChunk / 32];
+  const int c0 = blockIdx.x * kOzChunk;
+  const int a0 = blockIdx.y * kOzRows;
+  const int J = blockIdx.z;
+  const int nr = min(kOzRows, n - a0);
+  const int cw = min(kOzChunk, ld - c0);
+  if ((int)threadIdx.x < nr) {
+    const int r = threadIdx.x, a = a0 + r;
+    const int64_t row = (int64_t)J * ld + a;
+    const int e = eL[row];
+    sc[r] = oz_scale<S>(e);
+    if (c0 == 0) eA[row] = e;
+    const int I = ao_sh[a], aa = sh_off[I];
+    rI[r] = I;
+    rla[r] = a - aa;
+    rnA[r] = sh_off[I + 1] - aa;
   }
-  // V[J]: a warp covers one row when ld / 8 >= 32 (ld is a multiple of 128), so
-  // reduce over the warp and add once
+  __syncthreads();
+  const double* LJ = L + nrs * J;
+  const int b = c0 + threadIdx.x;
+  double x[kOzRows];
+  if (b < n) {
+    // rs indices fit in 32 bits (nrs < 2^31 for n < 65536)
+    const int Jp = ao_sh[b], bb = sh_off[Jp], nB = sh_off[Jp + 1] - bb, lb = b - bb, trib = Jp * (Jp + 1) / 2;
+#pragma unroll
+    for (int r = 0; r < kOzRows; ++r) {
+      x[r] = 0.0;
+      if (r < nr) {
+        const int I = rI[r], la = rla[r];
+        int t;
+        if (Jp < I) t = (int)__ldg(sp_first + I * (I + 1) / 2 + Jp) + la + rnA[r] * lb;
+        else if (Jp > I) t = (int)__ldg(sp_first + trib + I) + lb + nB * la;
+        else t = (int)__ldg(sp_first + trib + I) + (la >= lb ? la * (la + 1) / 2 + lb : lb * (lb + 1) / 2 + la);
+        x[r] = __ldg(LJ + t);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < kOzRows; ++r) x[r] = 0.0;
+  }
+  // cut (and the Coulomb contraction V_J += L_J[a, b] D[a, b])
+  double v = 0.0;
+#pragma unroll
+  for (int r = 0; r < kOzRows; ++r) {
+    if (r < nr) {
+      if (b < n) v = fma(x[r], __ldg(D + (size_t)(a0 + r) * n + b), v);
+      const long long y = oz_fixed<S>(x[r], sc[r]);
+#pragma unroll
+      for (int p = 0; p < S; ++p) Sb[p][r][threadIdx.x] = (uint8_t)(y >> (8 * (S - 1 - p)));
+    }
+  }
+  __syncthreads();
+  // blocked layout (oz_blk_off, 128-row tiles): the nr rows of one 32-byte
+  // column chunk are nr * 32 consecutive bytes; a thread writes 16 of them
+  const int nch = cw / 32;  // cw is a multiple of 128
+  const int64_t row0 = (int64_t)J * ld + a0;
+  for (int o = threadIdx.x; o < S * nch * nr * 2; o += kOzChunk) {
+    const int half = o & 1, rest = o >> 1, rr = rest % nr, r2 = rest / nr, ch = r2 % nch, p = r2 / nch;
+    uint8_t* dst = LS + p * slice + oz_blk_off(row0, c0 + 32 * ch, ld, 128) + rr * 32 + half * 16;
+    *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(&Sb[p][rr][32 * ch + 16 * half]);
+  }
   v = warp_sum(v);
-  if (live && (threadIdx.x & 31) == 0 && a < n) atomicAdd(&V[J], v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w8 = 0; w8 < kOzChunk / 32; ++w8) t += red[w8];
+    atomicAdd(&V[J], t);
+  }
 }
 
-// C (n x r, column-major FP64) -> slices CS[q][k][0..ld) for k < npad
-// (rows k >= r and columns b >= n zero), column exponents fC[k].  One warp
-// per column k.
-__global__ void k_oz_slice_c(const double* __restrict__ C, int n, int r, int npad, int ld, int s,
-                             uint8_t* __restrict__ CS, int* __restrict__ fC) {
+// C (n x r, column-major FP64) -> slices CS[q] of the npad x ld matrix C^T,
+// blocked in tiles of Nt rows (rows k >= r and columns b >= n zero), column
+// scale factors fC[k] = 2^e_k.  One warp per column k.
+template <int S>
+__global__ void k_oz_slice_c(const double* __restrict__ C, int n, int r, int npad, int ld, int Nt,
+                             uint8_t* __restrict__ CS, double* __restrict__ fC) {
   const int lane = threadIdx.x & 31;
   const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (k >= npad) return;
@@ -261,56 +361,73 @@ __global__ void k_oz_slice_c(const double* __restrict__ C, int n, int r, int npa
   if (k < r)
     for (int b = lane; b < n; b += 32) m = fmax(m, fabs(ck[b]));
   const int e = oz_exponent(warp_max(m));
-  if (lane == 0) fC[k] = e;
-  uint8_t* out = CS + (size_t)k * ld;
+  if (lane == 0) fC[k] = oz_pow2e(e);
+  const OzScale sc = oz_scale<S>(e);
   const size_t slice = (size_t)npad * ld;
   for (int b0 = 8 * lane; b0 < ld; b0 += 256) {
-    uint32_t w[2 * kOzMaxSlices];
-#pragma unroll
-    for (int q = 0; q < 2 * kOzMaxSlices; ++q) w[q] = 0;
+    uint8_t* out = CS + oz_blk_off(k, b0, ld, Nt);
+    long long y[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int b = b0 + u;
-      oz_cut(ldexp((k < r && b < n) ? ck[b] : 0.0, -e), s, w, u);
+      y[u] = oz_fixed<S>((k < r && b < n) ? ck[b] : 0.0, sc);
     }
-    for (int q = 0; q < s; ++q) *reinterpret_cast<uint2*>(out + q * slice + b0) = make_uint2(w[2 * q], w[2 * q + 1]);
+    uint2 w[S];
+    oz_pack8<S>(y, w);
+#pragma unroll
+    for (int q = 0; q < S; ++q) *reinterpret_cast<uint2*>(out + q * slice) = w[q];
   }
 }
 
-// One thread per 8 consecutive columns of a row a of X (FP64, row stride
-// xrow, columns [0, kx)): slices XS[p][a][col0 + c0 .. +8) (zero beyond kx and
-// for rows a >= n) with the row exponent of xmax[a] (the largest |X| of the
-// row, recorded by the half-transform), stored in eX[a].
-__global__ void k_oz_slice_x(const double* __restrict__ X, int64_t xrow, int n, int kx, int ld, int kblk, int s,
+// X (FP64, column-major: element (a, c) at X[c * xld + a], columns
+// [0, kx)) -> slices of XS (ld rows x xs_row columns, blocked in 128-row
+// tiles) at columns col0 + c (zero beyond kx and for rows a >= n), with the
+// row exponent of xmax[a] (the largest |X| of the row, recorded by the
+// half-transform), stored in eX[a].  One thread per (row a, 32-column
+// chunk): consecutive threads take consecutive rows, so that a warp reads
+// 256 consecutive bytes per column and writes 1 KB per slice.
+template <int S>
+__global__ void k_oz_slice_x(const double* __restrict__ X, int64_t xld, int n, int kx, int ld, int kblk,
                              int64_t xs_row, int64_t col0, const unsigned long long* __restrict__ xmax,
                              uint8_t* __restrict__ XS, int* __restrict__ eX) {
-  const int per_row = kblk / 8;
+  const int nch = kblk / 32;
   const int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (o >= (int64_t)ld * per_row) return;
-  const int a = (int)(o / per_row), c0 = 8 * (int)(o - (int64_t)a * per_row);
+  if (o >= (int64_t)ld * nch) return;
+  const int ri = (int)(o & 127);
+  const int64_t r2 = o >> 7;
+  const int ch = (int)(r2 % nch), tile = (int)(r2 / nch);
+  const int a = tile * 128 + ri;
   const int e = a < n ? oz_exponent(__longlong_as_double((long long)xmax[a])) : 0;
-  if (c0 == 0) eX[a] = e;
-  const double* xa = X + (size_t)a * xrow;
-  uint32_t w[2 * kOzMaxSlices];
+  if (ch == 0) eX[a] = e;
+  const OzScale sc = oz_scale<S>(e);
+  uint2 w[4][S];
 #pragma unroll
-  for (int q = 0; q < 2 * kOzMaxSlices; ++q) w[q] = 0;
+  for (int g = 0; g < 4; ++g) {
+    long long y[8];
 #pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    const int c = c0 + u;
-    oz_cut(ldexp((a < n && c < kx) ? xa[c] : 0.0, -e), s, w, u);
+    for (int u = 0; u < 8; ++u) {
+      const int c = 32 * ch + 8 * g + u;
+      y[u] = oz_fixed<S>((a < n && c < kx) ? X[(size_t)c * xld + a] : 0.0, sc);
+    }
+    oz_pack8<S>(y, w[g]);
   }
   const size_t slice = (size_t)ld * xs_row;
-  uint8_t* out = XS + (size_t)a * xs_row + col0 + c0;
-  for (int q = 0; q < s; ++q) *reinterpret_cast<uint2*>(out + q * slice) = make_uint2(w[2 * q], w[2 * q + 1]);
+  uint8_t* out = XS + oz_blk_off(a, col0 + 32 * ch, xs_row, 128);
+#pragma unroll
+  for (int q = 0; q < S; ++q) {
+    uint4* d = reinterpret_cast<uint4*>(out + q * slice);
+    d[0] = make_uint4(w[0][q].x, w[0][q].y, w[1][q].x, w[1][q].y);
+    d[1] = make_uint4(w[2][q].x, w[2][q].y, w[3][q].x, w[3][q].y);
+  }
 }
 
-// xmax[a] = bits of max_c |X[a][c]| (for the self-test, where X is given)
-__global__ void k_row_absmax(const double* __restrict__ X, int64_t xrow, int n, int kx,
+// xmax[a] = bits of max_c |X[c * xld + a]| (for the self-test, where X is given)
+__global__ void k_row_absmax(const double* __restrict__ X, int64_t xld, int n, int kx,
                              unsigned long long* __restrict__ xmax) {
   const int a = blockIdx.x;
   double m = 0.0;
   if (a < n)
-    for (int c = threadIdx.x; c < kx; c += blockDim.x) m = fmax(m, fabs(X[(size_t)a * xrow + c]));
+    for (int c = threadIdx.x; c < kx; c += blockDim.x) m = fmax(m, fabs(X[(size_t)c * xld + a]));
   m = warp_max(m);
   if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(xmax + a, (unsigned long long)__double_as_longlong(m));
 }
@@ -350,15 +467,17 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// 3D 8-bit tensor map over slices [s][rows][kx] (kx contiguous), boxes of
-// 32 bytes x box_rows x 1 slice, 32-byte swizzle.
-static bool make_slice_map(CUtensorMap* m, const uint8_t* base, int64_t kx, int64_t rows, int s, int box_rows) {
+// 8-bit tensor map over s blocked slices of a rows x kx matrix (layout of
+// oz_blk_off: tiles of br rows x 32 bytes, each contiguous), as a 5D tensor
+// (32 bytes, br rows, kx / 32 K steps, rows / br row tiles, s slices); a box
+// is one tile, placed in shared memory with the 32-byte swizzle.
+static bool make_slice_map(CUtensorMap* m, const uint8_t* base, int64_t kx, int64_t rows, int s, int br) {
   auto enc = tensor_map_encoder();
-  if (!enc || ((uintptr_t)base & 15) || kx % 32 || box_rows < 1 || box_rows > 256) return false;
-  cuuint64_t gdim[3] = {(cuuint64_t)kx, (cuuint64_t)rows, (cuuint64_t)s};
-  cuuint64_t gstr[2] = {(cuuint64_t)kx, (cuuint64_t)(kx * rows)};
-  cuuint32_t box[3] = {32u, (cuuint32_t)box_rows, 1u}, es[3] = {1, 1, 1};
-  return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void*)base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+  if (!enc || ((uintptr_t)base & 15) || kx % 32 || br < 8 || br > 256 || br % 8 || rows % br) return false;
+  cuuint64_t gdim[5] = {32u, (cuuint64_t)br, (cuuint64_t)(kx / 32), (cuuint64_t)(rows / br), (cuuint64_t)s};
+  cuuint64_t gstr[4] = {32u, (cuuint64_t)br * 32, (cuuint64_t)(kx * br), (cuuint64_t)(kx * rows)};
+  cuuint32_t box[5] = {32u, (cuuint32_t)br, 1u, 1u, 1u}, es[5] = {1, 1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, (void*)base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
              CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -401,17 +520,29 @@ static const short* oz_row_exponents(Handle* h, const int* inv, int ld, cudaStre
     const int64_t rows = (int64_t)nv * ld;
     k_oz_lexp<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(inv, n, nrs, L, nv, ld, e + (size_t)J0 * ld);
     g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (cudaGetLastError() != cudaSuccess) {
+      cudaFree(e);
+      return nullptr;
+    }
   }
   cho_set_lexp(c, e, ld);
   return e;
 }
 
-int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block, int s) {
+int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block, int s,
+             int sk) {
   ChoState* c = h->cho;
   const int64_t nrs = cho_nrs(c);
   const int M = cho_nvec(c);
   const int n = h->nbf;
-  if (s < 2 || s > kOzMaxSlices) { h->err = "mixed J/K: slices must be 2..8"; return MG_ERR_ARG; }
+  if (s < 2 || s > kOzMaxSlices || sk < 2 || sk > kOzMaxSlices) {
+    h->err = "mixed J/K: slices must be 2..8";
+    return MG_ERR_ARG;
+  }
+  if (const cudaError_t e = cudaGetLastError(); e != cudaSuccess) {
+    h->err = std::string("mixed J/K: error pending from earlier work: ") + cudaGetErrorString(e);
+    return MG_ERR_CUDA;
+  }
   const int ld = rup(n, 128);
   int nnt, Nt;
   oz_col_tiles(r, s, nnt, Nt);
@@ -433,35 +564,61 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   const int* d_rb = cho_rs_b_dev(c);
   const size_t nn = (size_t)n * n;
   const int64_t xs_row = (int64_t)G * kblk;
-  size_t need = 8 * (nrs + (size_t)nb + nn) + 4 * nn + (size_t)s * npad * ld + 4 * (size_t)npad +
-                (size_t)s * nb * ld * ld + 4 * (size_t)nb * ld + 8 * (size_t)n * kx + 8 * (size_t)ld +
-                (size_t)s * ld * xs_row + 4 * (size_t)G * ld + 8 * (size_t)nsm * 128 * 128 + 17 * 256;
+  const int ns = (int)h->sh.size();
+  // one term per take() below (each rounded up to 256 bytes: 15 takes)
+  size_t need = 8 * (nrs + (size_t)nb + nn) + 4 * nn + (size_t)s * npad * ld + 8 * (size_t)npad +
+                (size_t)s * nb * ld * ld + 4 * (size_t)nb * ld + 8 * (size_t)ld * kx + 8 * (size_t)ld +
+                (size_t)sk * ld * xs_row + 4 * (size_t)G * ld + 8 * (size_t)nsm * 128 * 128 + sizeof(int) +
+                4 * (size_t)(ns + 1 + n) + 15 * 256;
   char* ws = (char*)ws_get(h, need, st);
   if (!ws) { h->err = "jk workspace allocation failed"; return MG_ERR_MEMORY; }
+  char* const ws_end = ws + need;
   auto take = [&](size_t bytes) { char* p = ws; ws += (bytes + 255) & ~(size_t)255; return (void*)p; };
   double* jrs = (double*)take(8 * nrs);
   double* V = (double*)take(8 * (size_t)nb);
   double* D = (double*)take(8 * nn);
   int* inv = (int*)take(4 * nn);
   uint8_t* CS = (uint8_t*)take((size_t)s * npad * ld);
-  int* fC = (int*)take(4 * (size_t)npad);
+  double* fC = (double*)take(8 * (size_t)npad);
   uint8_t* LS = (uint8_t*)take((size_t)s * nb * ld * ld);
   int* eA = (int*)take(4 * (size_t)nb * ld);
-  double* Xf = (double*)take(8 * (size_t)n * kx);
+  double* Xf = (double*)take(8 * (size_t)ld * kx);  // column-major, ld rows
   unsigned long long* xmax = (unsigned long long*)take(8 * (size_t)ld);
-  uint8_t* XS = (uint8_t*)take((size_t)s * ld * xs_row);
+  uint8_t* XS = (uint8_t*)take((size_t)sk * ld * xs_row);
   int* eX = (int*)take(4 * (size_t)G * ld);
   double* P = (double*)take(8 * (size_t)nsm * 128 * 128);
   int* d_err = (int*)take(sizeof(int));
+  // every launch is checked at once, so that an error names its kernel
+  auto launched = [&](const char* what) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return true;
+    h->err = std::string("mixed J/K: ") + what + ": " + cudaGetErrorString(e);
+    return false;
+  };
+  int* sh_off = (int*)take(4 * (size_t)(ns + 1 + n));
+  int* ao_sh = sh_off + ns + 1;
+  if (ws > ws_end) { h->err = "mixed J/K: workspace layout exceeds its size"; return MG_ERR_CUDA; }
+  std::vector<int> hoff(ns + 1 + n);
+  for (int i = 0; i < ns; ++i) {
+    hoff[i] = h->sh[i].off;
+    for (int a = h->sh[i].off; a < h->sh[i].off + h->sh[i].nc * h->sh[i].ncomp; ++a) hoff[ns + 1 + a] = i;
+  }
+  hoff[ns] = n;
+  if (const cudaError_t e = cudaMemcpyAsync(sh_off, hoff.data(), 4 * (size_t)(ns + 1 + n), cudaMemcpyHostToDevice, st);
+      e != cudaSuccess) {
+    h->err = std::string("mixed J/K: shell table upload: ") + cudaGetErrorString(e);
+    return MG_ERR_CUDA;
+  }
   CUtensorMap map_l, map_c, map_x;
   if (!make_slice_map(&map_l, LS, ld, (int64_t)nb * ld, s, 128) || !make_slice_map(&map_c, CS, ld, npad, s, Nt) ||
-      !make_slice_map(&map_x, XS, xs_row, ld, s, 128)) {
+      !make_slice_map(&map_x, XS, xs_row, ld, sk, 128)) {
     h->err = "tensor maps for the exchange GEMMs could not be encoded";
     return MG_ERR_CUDA;
   }
   OzArgs ax{}, ak{};
   oz_plan(ax, s, Nt);
-  oz_plan(ak, s, 128);
+  oz_plan(ak, sk, 128);
   if (ax.stages < 2 || ak.stages < 2) { h->err = "mixed J/K: slice tiles do not fit in shared memory"; return MG_ERR_ARG; }
   if (!smem_attr_once((const void*)oz_gemm_kernel<false>, kOzSmemLimit) ||
       !smem_attr_once((const void*)oz_gemm_kernel<true>, kOzSmemLimit)) {
@@ -469,21 +626,33 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
     return MG_ERR_CUDA;
   }
   ax.err = ak.err = d_err;
-  ax.nrt = ld / 128; ax.nnt = nnt; ax.ld = ld; ax.n = n; ax.r = r; ax.eA = eA; ax.eB = fC; ax.X = Xf; ax.xrow = kx;
+  ax.nrt = ld / 128; ax.nnt = nnt; ax.ld = ld; ax.n = n; ax.r = r; ax.eA = eA; ax.fB = fC; ax.X = Xf; ax.xld = ld;
   ax.xmax = xmax;
   ak.ld = ld; ak.n = n; ak.ntile = ntile; ak.nsub = nsub; ak.kblk = kblk; ak.ksub = ksub; ak.eX = eX; ak.P = P;
   ak.K = d_K;
-  cudaMemsetAsync(d_err, 0, sizeof(int), st);
   const double one = 1.0, zero = 0.0;
-  cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, r, &one, d_C, n, d_C, n, &zero, D, n);
-  cudaMemsetAsync(jrs, 0, 8 * nrs, st);
-  cudaMemsetAsync(d_K, 0, 8 * nn, st);
+  if (cudaMemsetAsync(d_err, 0, sizeof(int), st) != cudaSuccess || cudaMemsetAsync(jrs, 0, 8 * nrs, st) != cudaSuccess ||
+      cudaMemsetAsync(d_K, 0, 8 * nn, st) != cudaSuccess) {
+    h->err = std::string("mixed J/K: clearing buffers: ") + cudaGetErrorString(cudaGetLastError());
+    return MG_ERR_CUDA;
+  }
+  if (const cublasStatus_t bs = cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, r, &one, d_C, n, d_C, n, &zero, D, n);
+      bs != CUBLAS_STATUS_SUCCESS) {
+    h->err = "mixed J/K: density product (cublasDgemm) failed, status " + std::to_string((int)bs);
+    return MG_ERR_CUDA;
+  }
+  if (const cudaError_t e = cudaGetLastError(); e != cudaSuccess) {
+    h->err = std::string("mixed J/K: after the density product: ") + cudaGetErrorString(e);
+    return MG_ERR_CUDA;
+  }
   k_rs_inverse<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, n, inv);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (!launched("k_rs_inverse")) return MG_ERR_CUDA;
   const short* eL = oz_row_exponents(h, inv, ld, st);
   if (!eL) { h->err = "mixed J/K: row exponents could not be stored"; return MG_ERR_MEMORY; }
-  k_oz_slice_c<<<(npad + 7) / 8, 256, 0, st>>>(d_C, n, r, npad, ld, s, CS, fC);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
+  oz_with_slices(s, [&](auto S) {
+    k_oz_slice_c<decltype(S)::value><<<(npad + 7) / 8, 256, 0, st>>>(d_C, n, r, npad, ld, Nt, CS, fC);
+  });
+  if (!launched("k_oz_slice_c")) return MG_ERR_CUDA;
   for (int g0 = 0; g0 < nblocks; g0 += G) {
     const int gn = std::min(G, nblocks - g0);
     for (int bi = 0; bi < gn; ++bi) {
@@ -492,40 +661,51 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
       const double* Lb = cho_vec_ptr(c, J0, nv, st, h);
       if (!Lb) { h->err = "vector block straddles storage blocks"; return MG_ERR_ARG; }
       // a short last block: clear the columns of the missing vectors
-      if (nv < nb) cudaMemsetAsync(Xf, 0, 8 * (size_t)n * kx, st);
+      if (nv < nb) cudaMemsetAsync(Xf, 0, 8 * (size_t)ld * kx, st);
       cudaMemsetAsync(V, 0, 8 * (size_t)nb, st);
       cudaMemsetAsync(xmax, 0, 8 * (size_t)ld, st);
-      const int64_t nthr = (int64_t)nv * ld * (ld / 8);
-      k_oz_slice_l<<<nb256(nthr), 256, 0, st>>>(inv, n, nrs, Lb, nv, ld, s, (int64_t)nb * ld * ld,
-                                               eL + (size_t)J0 * ld, D, LS, eA, V);
-      g_launches.fetch_add(1, std::memory_order_relaxed);
+      oz_with_slices(s, [&](auto S) {
+        k_oz_slice_l_blocks<decltype(S)::value>
+            <<<dim3((ld + kOzChunk - 1) / kOzChunk, (n + kOzRows - 1) / kOzRows, nv), kOzChunk, 0, st>>>(
+                cho_sp_first_dev(c), sh_off, ao_sh, n, nrs, Lb, ld, (int64_t)nb * ld * ld, eL + (size_t)J0 * ld, D,
+                LS, eA, V);
+      });
+      if (!launched("k_oz_slice_l_blocks")) return MG_ERR_CUDA;
       k_jacc64<<<nb256(nrs), 256, 0, st>>>(Lb, nrs, nv, V, jrs);
-      g_launches.fetch_add(1, std::memory_order_relaxed);
+      if (!launched("k_jacc64")) return MG_ERR_CUDA;
       // X_J = L_J C for the block (the slice map covers nb vectors; nv <= nb of them are used)
       ax.nJ = nv;
       ax.nitems = ax.nrt * nv * nnt;
       const int gx = std::min(ax.nitems, nsm);
       oz_gemm_kernel<false><<<gx, kOzThreads, ax.stages * ax.stage_bytes + 1024, st>>>(map_l, map_c, ax);
-      g_launches.fetch_add(1, std::memory_order_relaxed);
-      k_oz_slice_x<<<nb256((int64_t)ld * (kblk / 8)), 256, 0, st>>>(Xf, kx, n, kx, ld, kblk, s, xs_row,
-                                                                   (int64_t)bi * kblk, xmax, XS, eX + (size_t)bi * ld);
-      g_launches.fetch_add(1, std::memory_order_relaxed);
+      if (!launched("oz_gemm_kernel<false>")) return MG_ERR_CUDA;
+      oz_with_slices(sk, [&](auto S) {
+        k_oz_slice_x<decltype(S)::value><<<nb256((int64_t)ld * (kblk / 32)), 256, 0, st>>>(
+            Xf, ld, n, kx, ld, kblk, xs_row, (int64_t)bi * kblk, xmax, XS, eX + (size_t)bi * ld);
+      });
+      if (!launched("k_oz_slice_x")) return MG_ERR_CUDA;
     }
     // K += X X^T over the group (lower tiles)
     ak.nblk = gn;
     ak.nitems = ntile * gn * nsub;
     const int gk = std::min(ak.nitems, nsm);
     oz_gemm_kernel<true><<<gk, kOzThreads, ak.stages * ak.stage_bytes + 1024, st>>>(map_x, map_x, ak);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (!launched("oz_gemm_kernel<true>")) return MG_ERR_CUDA;
   }
   k_symmetrize_lower<<<nb256((int64_t)nn), 256, 0, st>>>(d_K, n);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (!launched("k_symmetrize_lower")) return MG_ERR_CUDA;
   k_unpack_sym<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, jrs, n, d_J);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
-  if (cudaGetLastError() != cudaSuccess) { h->err = "mixed J/K: launch failed"; return MG_ERR_CUDA; }
+  if (!launched("k_unpack_sym")) return MG_ERR_CUDA;
+  if (const cudaError_t e = cudaGetLastError(); e != cudaSuccess) {
+    h->err = std::string("mixed J/K: ") + cudaGetErrorString(e);
+    return MG_ERR_CUDA;
+  }
   int herr = 0;
   cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess) { h->err = "mixed J/K: device error"; return MG_ERR_CUDA; }
+  if (const cudaError_t e = cudaStreamSynchronize(st); e != cudaSuccess) {
+    h->err = std::string("mixed J/K: ") + cudaGetErrorString(e);
+    return MG_ERR_CUDA;
+  }
   if (herr) {
     h->err = "exchange GEMMs: a pipeline wait ran out (result incomplete)";
     return MG_ERR_CUDA;
@@ -534,8 +714,8 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
 }
 
 // The sliced engine on given dense matrices (verification of the kernels
-// used by jk_mixed): X = A B^T (A: ld x ld, B: r x ld, both row-major; X
-// row-major ld x r) and K = X X^T (lower triangle, column-major ld x ld).
+// used by jk_mixed): X = A B (A: ld x ld, B: ld x r, X: ld x r, all
+// column-major) and K = X X^T (lower triangle, column-major ld x ld).
 int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double* d_B, double* d_X, double* d_K,
                 uint8_t* d_slices, int* d_exps, cudaStream_t st) {
   if (ld < 128 || ld % 128 || r < 1 || s < 2 || s > kOzMaxSlices) return MG_ERR_ARG;
@@ -547,7 +727,7 @@ int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double
   const int ksub = rup((kblk + nsub - 1) / nsub, 32);
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
-  const size_t need = (size_t)s * ld * ld + 4 * (size_t)ld + (size_t)s * npad * ld + 4 * (size_t)npad +
+  const size_t need = (size_t)s * ld * ld + 4 * (size_t)ld + (size_t)s * npad * ld + 8 * (size_t)npad +
                       (size_t)s * ld * kblk + 4 * (size_t)ld + 16 * (size_t)ld + 8 * (size_t)nsm * 128 * 128 +
                       18 * 256;
   char* ws = (char*)ws_get(h, need, st);
@@ -556,7 +736,7 @@ int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double
   uint8_t* LS = (uint8_t*)take((size_t)s * ld * ld);
   int* eA = (int*)take(4 * (size_t)ld);
   uint8_t* CS = (uint8_t*)take((size_t)s * npad * ld);
-  int* fC = (int*)take(4 * (size_t)npad);
+  double* fC = (double*)take(8 * (size_t)npad);
   uint8_t* XS = (uint8_t*)take((size_t)s * ld * kblk);
   int* eX = (int*)take(4 * (size_t)ld);
   unsigned long long* amax = (unsigned long long*)take(8 * (size_t)ld);
@@ -574,7 +754,7 @@ int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double
       !smem_attr_once((const void*)oz_gemm_kernel<true>, kOzSmemLimit))
     return MG_ERR_CUDA;
   ax.err = ak.err = d_err;
-  ax.nrt = ld / 128; ax.nnt = nnt; ax.ld = ld; ax.n = ld; ax.r = r; ax.eA = eA; ax.eB = fC; ax.X = d_X; ax.xrow = r;
+  ax.nrt = ld / 128; ax.nnt = nnt; ax.ld = ld; ax.n = ld; ax.r = r; ax.eA = eA; ax.fB = fC; ax.X = d_X; ax.xld = ld;
   ax.xmax = xmax; ax.nJ = 1; ax.nitems = ax.nrt * nnt;
   ak.ld = ld; ak.n = ld; ak.ntile = (ld / 128) * (ld / 128 + 1) / 2; ak.nsub = nsub; ak.kblk = kblk; ak.ksub = ksub;
   ak.eX = eX; ak.P = P; ak.K = d_K; ak.nblk = 1; ak.nitems = ak.ntile * nsub;
@@ -583,13 +763,21 @@ int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double
   cudaMemsetAsync(amax, 0, 8 * (size_t)ld, st);
   cudaMemsetAsync(xmax, 0, 8 * (size_t)ld, st);
   k_row_absmax<<<ld, 256, 0, st>>>(d_A, ld, ld, ld, amax);
-  k_oz_slice_x<<<nb256((int64_t)ld * (ld / 8)), 256, 0, st>>>(d_A, ld, ld, ld, ld, ld, s, ld, 0, amax, LS, eA);
+  oz_with_slices(s, [&](auto S) {
+    k_oz_slice_x<decltype(S)::value><<<nb256((int64_t)ld * (ld / 32)), 256, 0, st>>>(d_A, ld, ld, ld, ld, ld, ld, 0,
+                                                                                    amax, LS, eA);
+  });
   if (d_slices) cudaMemcpyAsync(d_slices, LS, (size_t)s * ld * ld, cudaMemcpyDeviceToDevice, st);
   if (d_exps) cudaMemcpyAsync(d_exps, eA, 4 * (size_t)ld, cudaMemcpyDeviceToDevice, st);
-  k_oz_slice_c<<<(npad + 7) / 8, 256, 0, st>>>(d_B, ld, r, npad, ld, s, CS, fC);
+  oz_with_slices(s, [&](auto S) {
+    k_oz_slice_c<decltype(S)::value><<<(npad + 7) / 8, 256, 0, st>>>(d_B, ld, r, npad, ld, Nt, CS, fC);
+  });
   oz_gemm_kernel<false><<<std::min(ax.nitems, nsm), kOzThreads, ax.stages * ax.stage_bytes + 1024, st>>>(map_l, map_c,
                                                                                                        ax);
-  k_oz_slice_x<<<nb256((int64_t)ld * (kblk / 8)), 256, 0, st>>>(d_X, r, ld, r, ld, kblk, s, kblk, 0, xmax, XS, eX);
+  oz_with_slices(s, [&](auto S) {
+    k_oz_slice_x<decltype(S)::value><<<nb256((int64_t)ld * (kblk / 32)), 256, 0, st>>>(d_X, ld, ld, r, ld, kblk, kblk,
+                                                                                      0, xmax, XS, eX);
+  });
   oz_gemm_kernel<true><<<std::min(ak.nitems, nsm), kOzThreads, ak.stages * ak.stage_bytes + 1024, st>>>(map_x, map_x,
                                                                                                       ak);
   g_launches.fetch_add(6, std::memory_order_relaxed);

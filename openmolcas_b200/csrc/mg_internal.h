@@ -170,6 +170,8 @@ const int* cho_rs_a_dev(const ChoState* c);
 const int* cho_rs_b_dev(const ChoState* c);
 const double* cho_vec_ptr(const ChoState* c, int J0, int nb, cudaStream_t st, Handle* h);
 int cho_vec_block();
+// first rs index of every shell pair (pair_id order), device
+const int64_t* cho_sp_first_dev(const ChoState* c);
 // cached row exponents of the square Cholesky vectors (M x ld), owned by the state
 short* cho_lexp(const ChoState* c, int ld);
 void cho_set_lexp(ChoState* c, short* p, int ld);
@@ -177,7 +179,7 @@ int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double
                 uint8_t* d_slices, int* d_exps, cudaStream_t st);
 int fock_accumulate(double* F, const double* J, const double* K, double factxi, int64_t n, cudaStream_t st);
 int jk_fp64(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block);
-int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block, int s);
+int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block, int s, int sk);
 
 inline int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 inline int ncart_cum(int l) { return l <= 0 ? 0 : l * (l + 1) * (l + 2) / 6; }

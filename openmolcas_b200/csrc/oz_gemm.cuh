@@ -15,6 +15,14 @@
 // most kOzKChunk products per element (4096 * 6 * 255^2 < 2^31), so the only
 // roundings are the FP64 combination and the truncated tail.
 //
+// Operand layout in HBM (blocked): slice p of a matrix of R rows and K
+// 8-bit columns is stored as tiles of BR rows x 32 bytes (one MMA K step),
+// each tile contiguous (BR * 32 bytes), tiles ordered K step fastest, then
+// row tile:  byte (row, k) at ((row / BR) (K / 32) + k / 32) BR 32 +
+// (row % BR) 32 + k % 32  (oz_blk_off).  BR = 128 for A operands, Nt for the
+// B operand of the half-transform.  A TMA box is then one contiguous run of
+// memory (whole cache lines), not BR separate 32-byte pieces.
+//
 // One CTA of 192 threads per SM:
 //   warp 4 lane 0   TMA producer: per K step of 32, the slices 0..d1-1 of the
 //                   A tile (128 rows) and of the B tile (Nt rows), 32-byte
@@ -51,6 +59,25 @@ constexpr int kOzABytes = 128 * 32;
 // once per device to this size; stages are planned within it)
 constexpr int kOzSmemLimit = 221 * 1024;
 
+// 2^k for -1022 <= k <= 1023
+__device__ __forceinline__ double oz_pow2(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
+// 2^e for any int e (outside the normal range through ldexp)
+__device__ __forceinline__ double oz_pow2e(int e) { return (e >= -1022 && e <= 1023) ? oz_pow2(e) : ldexp(1.0, e); }
+
+// Exact int32 -> double on the FP64 adder: the double with high word
+// 0x43380000 and low word x + 2^31 is 1.5 2^52 + 2^31 + x; subtracting that
+// offset leaves x exactly.
+__device__ __forceinline__ double oz_i2d(uint32_t v) {
+  return __hiloint2double(0x43380000, (int)(v ^ 0x80000000u)) - 6755401588539392.0;
+}
+
+// byte offset of element (row, k) of one blocked slice (K columns, tiles of
+// br rows x 32 bytes)
+__host__ __device__ __forceinline__ size_t oz_blk_off(long long row, long long k, long long kdim, int br) {
+  return ((size_t)(row / br) * (size_t)(kdim >> 5) + (size_t)(k >> 5)) * (size_t)(br * 32) + (size_t)(row % br) * 32 +
+         (size_t)(k & 31);
+}
+
 struct OzArgs {
   int s;           // slices
   int nd;          // accumulators per pass
@@ -66,16 +93,16 @@ struct OzArgs {
   int n;           // valid rows / columns (nbf)
   int r;           // columns of C
   const int* eA;   // row exponents of the L slices, [J * ld + a]
-  const int* eB;   // column exponents of C, [k]
-  double* X;       // X[a * xrow + J * r + k] (FP64)
-  long long xrow;
+  const double* fB;  // column scale factors of C, 2^f_k
+  double* X;       // X[(J * r + k) * xld + a] (FP64, column-major)
+  int xld;
   unsigned long long* xmax;  // per row a: bits of the largest |X| written (atomicMax)
   // exchange product K += X X^T (SYRK == true): items (lower tile, block, sub-chunk)
   int ntile, nblk, nsub;
   int kblk;        // K extent of one block (multiple of 32)
   int ksub;        // K elements of a sub-chunk (multiple of 32)
   const int* eX;   // row exponents of the X slices, [blk * ld + a]
-  double* P;       // CTA-private FP64 tiles, 128 x 128 per CTA
+  double* P;       // CTA-private FP64 tiles, 128 x 128 per CTA (column-major)
   double* K;       // column-major n x n (lower triangle accumulated)
 };
 
@@ -123,11 +150,13 @@ __device__ __forceinline__ void oz_for_units(const OzArgs& a, F&& f) {
         }
     }
   } else {
-    const long long per = (long long)a.nitems;
-    const int i0 = (int)(per * blockIdx.x / gridDim.x), i1 = (int)(per * (blockIdx.x + 1) / gridDim.x);
-    const int per_tile = a.nblk * a.nsub;
-    for (int item = i0; item < i1; ++item) {
-      const int tile = item / per_tile, r1 = item - tile * per_tile, blk = r1 / a.nsub, sub = r1 - blk * a.nsub;
+    // items in (block, sub-chunk, tile) order, strided over the CTAs: the
+    // CTAs that run at the same time take the tiles of one or two K
+    // sub-chunks, whose slices stay in L2 while they are read; every item is
+    // a complete segment (its passes add into the CTA-private tile, then the
+    // tile is added into K)
+    for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
+      const int tile = item % a.ntile, r1 = item / a.ntile, sub = r1 % a.nsub, blk = r1 / a.nsub;
       int ti, tj;
       oz_tile_ij(tile, ti, tj);
       const int kb0 = sub * a.ksub;
@@ -136,8 +165,6 @@ __device__ __forceinline__ void oz_for_units(const OzArgs& a, F&& f) {
         if (threadIdx.x == 0) atomicExch(a.err, 2);
         return;
       }
-      const bool seg_first = item == i0 || r1 == 0;
-      const bool seg_last = item == i1 - 1 || r1 == per_tile - 1;
       for (int g = 0; g < npass; ++g) {
         OzUnit u;
         u.rowA = ti * 128;
@@ -148,8 +175,8 @@ __device__ __forceinline__ void oz_for_units(const OzArgs& a, F&& f) {
         u.d1 = min(a.s, u.d0 + a.nd);
         u.same = ti == tj;
         u.t0 = ti; u.t1 = tj; u.J = blk; u.nt = 0;
-        u.first = seg_first && g == 0;
-        u.last = seg_last && g == npass - 1;
+        u.first = g == 0;
+        u.last = g == npass - 1;
         if (!f(u)) return;
       }
     }
@@ -202,11 +229,14 @@ __global__ void __launch_bounds__(kOzThreads, 1)
           uint8_t* base = smem + (size_t)st * a.stage_bytes;
           const uint32_t fb = tc_smem_addr(&full_bar[st]);
           tc_mbar_expect_tx(fb, bytes);
-          const int kx = u.k0 + 32 * kk;
-          for (int p = 0; p < nsl; ++p) tc_tma_load3(tc_smem_addr(base + p * kOzABytes), &mapA, fb, kx, u.rowA, p);
+          // blocked operands: (32-byte K step, row tile) addresses one contiguous box
+          const int ks = (u.k0 >> 5) + kk;
+          for (int p = 0; p < nsl; ++p)
+            tc_tma_load5(tc_smem_addr(base + p * kOzABytes), &mapA, fb, 0, 0, ks, u.rowA >> 7, p);
           if (!u.same)
             for (int q = 0; q < nsl; ++q)
-              tc_tma_load3(tc_smem_addr(base + a.s * kOzABytes + q * a.b_bytes), &mapB, fb, kx, u.rowB, q);
+              tc_tma_load5(tc_smem_addr(base + a.s * kOzABytes + q * a.b_bytes), &mapB, fb, 0, 0, ks, u.rowB / a.Nt,
+                           q);
         }
         return true;
       });
@@ -264,40 +294,53 @@ __global__ void __launch_bounds__(kOzThreads, 1)
       if (ok) {
         const int ncol = SYRK ? 128 : a.Nt;
         double rmax = 0.0;
+        // row scale factor of this thread's output row (power of two)
+        const int arow = u.t0 * 128 + row;
+        const double fa = SYRK ? oz_pow2e(a.eX[u.J * a.ld + arow]) : (arow < a.n ? oz_pow2e(a.eA[u.J * a.ld + arow]) : 0.0);
         for (int c0 = 0; c0 < ncol; c0 += 16) {
           double sum[16];
 #pragma unroll
           for (int i = 0; i < 16; ++i) sum[i] = 0.0;
-          for (int d = u.d0; d < u.d1; ++d) {
-            uint32_t v[16];
-            tc_ld16(tl + (uint32_t)((d - u.d0) * a.acc_stride + c0), v);
-            const double w = ldexp(1.0, -14 - 8 * d);
+          {
+            // every accumulator's 16 columns in flight at once, one wait
+            uint32_t v[kOzMaxSlices][16];
+            const int nacc = u.d1 - u.d0;
 #pragma unroll
-            for (int i = 0; i < 16; ++i) sum[i] = fma((double)(int)v[i], w, sum[i]);
+            for (int j = 0; j < kOzMaxSlices; ++j)
+              if (j < nacc) tc_ld16_async(tl + (uint32_t)(j * a.acc_stride + c0), v[j]);
+            tc_ld_wait();
+#pragma unroll
+            for (int j = 0; j < kOzMaxSlices; ++j)
+              if (j < nacc) {
+                tc_ld_bind(v[j]);
+                const double w = oz_pow2(-14 - 8 * (u.d0 + j));
+#pragma unroll
+                for (int i = 0; i < 16; ++i) sum[i] = fma(oz_i2d(v[j][i]), w, sum[i]);
+              }
           }
+          // (the scaling by powers of two is exact; the warp's 32 rows of one
+          // column are consecutive in X and in the tile)
           if (!SYRK) {
-            const int arow = u.t0 * 128 + row;
             if (arow < a.n) {
-              const int ea = a.eA[u.J * a.ld + arow];
-              double* xr = a.X + (size_t)arow * a.xrow + (size_t)u.J * a.r;
+              double* xc = a.X + (size_t)u.J * a.r * a.xld + arow;
 #pragma unroll
               for (int i = 0; i < 16; ++i) {
                 const int k = u.nt * a.Nt + c0 + i;
                 if (k < a.r) {
-                  const double val = ldexp(sum[i], ea + a.eB[k]);
-                  xr[k] = u.first ? val : xr[k] + val;
+                  const double val = sum[i] * fa * a.fB[k];
+                  double* xp = xc + (size_t)k * a.xld;
+                  *xp = u.first ? val : *xp + val;
                   rmax = fmax(rmax, fabs(val));
                 }
               }
             }
           } else {
-            const int ea = a.eX[u.J * a.ld + u.t0 * 128 + row];
             const int* eb = a.eX + u.J * a.ld + u.t1 * 128 + c0;
-            double* pr = a.P + (size_t)blockIdx.x * 128 * 128 + (size_t)row * 128 + c0;
+            double* pc = a.P + (size_t)blockIdx.x * 128 * 128 + (size_t)c0 * 128 + row;
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
-              const double val = ldexp(sum[i], ea + eb[i]);
-              pr[i] = u.first ? val : pr[i] + val;
+              const double val = sum[i] * fa * oz_pow2e(eb[i]);
+              pc[i * 128] = u.first ? val : pc[i * 128] + val;
             }
           }
         }
@@ -305,12 +348,11 @@ __global__ void __launch_bounds__(kOzThreads, 1)
           atomicMax(a.xmax + u.t0 * 128 + row, (unsigned long long)__double_as_longlong(rmax));
         if (SYRK && u.last) {
           // this CTA's share of the tile is complete: add it into K
-          const int arow = u.t0 * 128 + row;
-          const double* pr = a.P + (size_t)blockIdx.x * 128 * 128 + (size_t)row * 128;
+          const double* pc = a.P + (size_t)blockIdx.x * 128 * 128 + row;
           if (arow < a.n)
             for (int c = 0; c < 128; ++c) {
               const int bcol = u.t1 * 128 + c;
-              if (bcol < a.n) atomicAdd(&a.K[(size_t)arow + (size_t)a.n * bcol], pr[c]);
+              if (bcol < a.n) atomicAdd(&a.K[(size_t)arow + (size_t)a.n * bcol], pc[c * 128]);
             }
         }
       }

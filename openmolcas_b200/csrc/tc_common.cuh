@@ -50,7 +50,7 @@ __device__ __forceinline__ bool tc_mbar_wait(uint32_t bar, uint32_t parity, vola
   return false;
 }
 
-// 2D and 3D tiled TMA loads into shared memory, completion on an mbarrier.
+// 2D and 5D tiled TMA loads into shared memory, completion on an mbarrier.
 __device__ __forceinline__ void tc_tma_load(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
@@ -58,11 +58,12 @@ __device__ __forceinline__ void tc_tma_load(uint32_t dst, const CUtensorMap* map
       "l"((uint64_t)map), "r"(bar), "r"(x), "r"(y)
       : "memory");
 }
-__device__ __forceinline__ void tc_tma_load3(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y, int z) {
+__device__ __forceinline__ void tc_tma_load5(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1, int c2,
+                                             int c3, int c4) {
   asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
-          dst),
-      "l"((uint64_t)map), "r"(bar), "r"(x), "r"(y), "r"(z)
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6, %7}], "
+      "[%2];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
       : "memory");
 }
 
@@ -132,6 +133,23 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// 16 consecutive 32-bit TMEM columns of this thread's lane, without waiting:
+// several loads may be in flight; tc_ld_wait() completes them and
+// tc_ld_bind() orders every later use of the registers after it.
+__device__ __forceinline__ void tc_ld16_async(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tc_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_ld_bind(uint32_t (&v)[16]) {
+#pragma unroll
+  for (int i = 0; i < 16; ++i) asm volatile("" : "+r"(v[i]));
 }
 
 // 16 consecutive 32-bit TMEM columns of this thread's lane.

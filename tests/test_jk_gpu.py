@@ -74,13 +74,13 @@ def _selftest(g, A, Bm, s):
     f = lib().mg_sliced_selftest
     f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 7
     ld, r = A.shape[0], Bm.shape[0]
-    dA = torch.from_numpy(A).cuda()
-    dB = torch.from_numpy(Bm).cuda()
-    X = torch.zeros(ld, r, dtype=torch.float64, device="cuda")
+    dA = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()  # column-major A
+    dB = torch.from_numpy(Bm).cuda()                          # column-major B = Bm^T (ld x r)
+    X = torch.zeros(r, ld, dtype=torch.float64, device="cuda")  # column-major ld x r
     K = torch.zeros(ld, ld, dtype=torch.float64, device="cuda")
     rc = f(g.h, ld, r, s, dA.data_ptr(), dB.data_ptr(), X.data_ptr(), K.data_ptr(), None, None, None)
     assert rc == 0
-    return X.cpu().numpy(), K.cpu().numpy().T
+    return X.cpu().numpy().T, K.cpu().numpy().T
 
 
 @pytest.mark.parametrize("ld,r", [(128, 6), (256, 208), (384, 300)])
@@ -173,6 +173,31 @@ def test_jk_mixed_many_vector_blocks():
     assert np.abs(Jm - J).max() < RELJ_BAR * np.abs(J).max()
     assert relK < RELK_BAR
     assert abs(Em - E) <= DE_BAR
+
+
+def test_jk_mixed_general_contraction():
+    """Generally contracted shells of every l (an ANO-like 9s5p4d -> 4s3p2d
+    set on one atom, narrower shells on two more), whose AO ranges straddle
+    the 16-row blocks in which the slicing kernel unpacks the rs-packed
+    vectors into squares, ThrCom 1e-6, rank-10 density: mixed against FP64
+    at the same bars."""
+    rng = np.random.default_rng(21)
+    coords = np.array([[0.0, 0.0, 0.0], [1.9, 0.4, -0.3], [-0.7, 2.1, 0.8]])
+    sh = [(0, 2, 4, 2), (0, 0, 9, 4), (0, 1, 5, 3), (1, 0, 6, 2), (1, 1, 3, 1), (2, 0, 3, 2), (2, 2, 2, 1)]
+    exps, coefs = [], []
+    for _, l, npr, nco in sh:
+        exps += list(0.1 * 2.7 ** np.arange(npr))
+        coefs += list(rng.standard_normal(npr * nco))
+    mol = B.molecule_from_arrays("general", coords, [6.0, 1.0, 1.0], [x[0] for x in sh], [x[1] for x in sh],
+                                 [x[2] for x in sh], [x[3] for x in sh], exps, coefs)
+    g = MolGpu(mol)
+    g.cho_drv(thrcom=1e-6)
+    Cn = B.density_factor(g.nbf, 10, 5)
+    J, K, Jm, Km = _jk_pair(g, torch.from_numpy(Cn))
+    D = Cn @ Cn.T
+    assert np.abs(Jm - J).max() < RELJ_BAR * np.abs(J).max()
+    assert np.abs(Km - K).max() < RELK_BAR * np.abs(K).max()
+    assert abs(_energy(D, Jm, Km) - _energy(D, J, K)) <= DE_BAR
 
 
 def test_c1_cluster_jk_energy():
