@@ -620,8 +620,10 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   oz_plan(ax, s, Nt);
   oz_plan(ak, sk, 128);
   if (ax.stages < 2 || ak.stages < 2) { h->err = "mixed J/K: slice tiles do not fit in shared memory"; return MG_ERR_ARG; }
-  if (!smem_attr_once((const void*)oz_gemm_kernel<false>, kOzSmemLimit) ||
-      !smem_attr_once((const void*)oz_gemm_kernel<true>, kOzSmemLimit)) {
+  bool attr = true;
+  oz_with_slices(s, [&](auto S) { attr &= smem_attr_once((const void*)oz_gemm_kernel<false, decltype(S)::value>, kOzSmemLimit); });
+  oz_with_slices(sk, [&](auto S) { attr &= smem_attr_once((const void*)oz_gemm_kernel<true, decltype(S)::value>, kOzSmemLimit); });
+  if (!attr) {
     h->err = "exchange GEMMs: shared-memory limit could not be raised";
     return MG_ERR_CUDA;
   }
@@ -677,7 +679,9 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
       ax.nJ = nv;
       ax.nitems = ax.nrt * nv * nnt;
       const int gx = std::min(ax.nitems, nsm);
-      oz_gemm_kernel<false><<<gx, kOzThreads, ax.stages * ax.stage_bytes + 1024, st>>>(map_l, map_c, ax);
+      oz_with_slices(s, [&](auto S) {
+        oz_gemm_kernel<false, decltype(S)::value><<<gx, kOzThreads, ax.stages * ax.stage_bytes + 1024, st>>>(map_l, map_c, ax);
+      });
       if (!launched("oz_gemm_kernel<false>")) return MG_ERR_CUDA;
       oz_with_slices(sk, [&](auto S) {
         k_oz_slice_x<decltype(S)::value><<<nb256((int64_t)ld * (kblk / 32)), 256, 0, st>>>(
@@ -689,7 +693,9 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
     ak.nblk = gn;
     ak.nitems = ntile * gn * nsub;
     const int gk = std::min(ak.nitems, nsm);
-    oz_gemm_kernel<true><<<gk, kOzThreads, ak.stages * ak.stage_bytes + 1024, st>>>(map_x, map_x, ak);
+    oz_with_slices(sk, [&](auto S) {
+      oz_gemm_kernel<true, decltype(S)::value><<<gk, kOzThreads, ak.stages * ak.stage_bytes + 1024, st>>>(map_x, map_x, ak);
+    });
     if (!launched("oz_gemm_kernel<true>")) return MG_ERR_CUDA;
   }
   k_symmetrize_lower<<<nb256((int64_t)nn), 256, 0, st>>>(d_K, n);
@@ -750,9 +756,12 @@ int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double
   OzArgs ax{}, ak{};
   oz_plan(ax, s, Nt);
   oz_plan(ak, s, 128);
-  if (!smem_attr_once((const void*)oz_gemm_kernel<false>, kOzSmemLimit) ||
-      !smem_attr_once((const void*)oz_gemm_kernel<true>, kOzSmemLimit))
-    return MG_ERR_CUDA;
+  bool attr = true;
+  oz_with_slices(s, [&](auto S) {
+    attr &= smem_attr_once((const void*)oz_gemm_kernel<false, decltype(S)::value>, kOzSmemLimit) &&
+            smem_attr_once((const void*)oz_gemm_kernel<true, decltype(S)::value>, kOzSmemLimit);
+  });
+  if (!attr) return MG_ERR_CUDA;
   ax.err = ak.err = d_err;
   ax.nrt = ld / 128; ax.nnt = nnt; ax.ld = ld; ax.n = ld; ax.r = r; ax.eA = eA; ax.fB = fC; ax.X = d_X; ax.xld = ld;
   ax.xmax = xmax; ax.nJ = 1; ax.nitems = ax.nrt * nnt;
@@ -772,14 +781,18 @@ int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double
   oz_with_slices(s, [&](auto S) {
     k_oz_slice_c<decltype(S)::value><<<(npad + 7) / 8, 256, 0, st>>>(d_B, ld, r, npad, ld, Nt, CS, fC);
   });
-  oz_gemm_kernel<false><<<std::min(ax.nitems, nsm), kOzThreads, ax.stages * ax.stage_bytes + 1024, st>>>(map_l, map_c,
-                                                                                                       ax);
+  oz_with_slices(s, [&](auto S) {
+    oz_gemm_kernel<false, decltype(S)::value>
+        <<<std::min(ax.nitems, nsm), kOzThreads, ax.stages * ax.stage_bytes + 1024, st>>>(map_l, map_c, ax);
+  });
   oz_with_slices(s, [&](auto S) {
     k_oz_slice_x<decltype(S)::value><<<nb256((int64_t)ld * (kblk / 32)), 256, 0, st>>>(d_X, ld, ld, r, ld, kblk, kblk,
                                                                                       0, xmax, XS, eX);
   });
-  oz_gemm_kernel<true><<<std::min(ak.nitems, nsm), kOzThreads, ak.stages * ak.stage_bytes + 1024, st>>>(map_x, map_x,
-                                                                                                      ak);
+  oz_with_slices(s, [&](auto S) {
+    oz_gemm_kernel<true, decltype(S)::value>
+        <<<std::min(ak.nitems, nsm), kOzThreads, ak.stages * ak.stage_bytes + 1024, st>>>(map_x, map_x, ak);
+  });
   g_launches.fetch_add(6, std::memory_order_relaxed);
   if (cudaGetLastError() != cudaSuccess) return MG_ERR_CUDA;
   int herr = 0;

@@ -183,10 +183,42 @@ __device__ __forceinline__ void oz_for_units(const OzArgs& a, F&& f) {
   }
 }
 
-template <bool SYRK>
+// The MMAs of diagonals [D0, D1) for one K step of 32, unrolled: the slice
+// p of A and q of B are descriptor offsets (p * 4096 and q * bst bytes, in
+// 16-byte units), id[] the four signedness variants of the instruction
+// descriptor, (p == 0 ? 2 : 0) + (q == 0 ? 1 : 0); the first product of
+// every accumulator overwrites it at the first K step of a unit.
+template <int D0, int D1>
+__device__ __forceinline__ void oz_issue(uint32_t tmem, int acc_stride, uint64_t da, uint64_t db, uint32_t bst,
+                                         const uint32_t (&id)[4], bool first) {
+#pragma unroll
+  for (int d = D0; d < D1; ++d) {
+    const uint32_t acc = tmem + (uint32_t)((d - D0) * acc_stride);
+#pragma unroll
+    for (int p = 0; p <= d; ++p) {
+      const int q = d - p;
+      tc_mma_i8(acc, da + (uint64_t)(p * (kOzABytes >> 4)), db + (uint64_t)q * bst,
+                id[(p == 0 ? 2 : 0) + (q == 0 ? 1 : 0)], (first && p == 0) ? 0u : 1u);
+    }
+  }
+}
+
+// Accumulators per pass: all NS diagonals for the half-transform (its column
+// tile is chosen so that they fit), 4 of 128 columns for the exchange product.
+template <bool SYRK, int NS>
+struct OzPass {
+  static constexpr int nd = SYRK ? (NS < 4 ? NS : 4) : NS;
+};
+
+template <bool SYRK, int NS>
 __global__ void __launch_bounds__(kOzThreads, 1)
     oz_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                    const OzArgs a) {
+  constexpr int ND = OzPass<SYRK, NS>::nd;
+  if (a.s != NS || a.nd != ND) {  // launched with another plan: nothing has started yet
+    if (threadIdx.x == 0) atomicExch(a.err, 3);
+    return;
+  }
   extern __shared__ uint8_t oz_smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kOzMaxStages], empty_bar[kOzMaxStages], accf_bar, acce_bar;
   __shared__ uint32_t tmem_base;
@@ -249,6 +281,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
   } else if (warp == 5) {
     if (lane == 0) {
       // ---- MMA issuer
+      const uint32_t id[4] = {tc_idesc_i8(a.Nt, false, false), tc_idesc_i8(a.Nt, false, true),
+                              tc_idesc_i8(a.Nt, true, false), tc_idesc_i8(a.Nt, true, true)};
       int it = 0, un = 0;
       oz_for_units<SYRK>(a, [&](const OzUnit& u) -> bool {
         // the accumulators must have been read out by the epilogue
@@ -263,16 +297,11 @@ __global__ void __launch_bounds__(kOzThreads, 1)
           uint8_t* base = smem + (size_t)st * a.stage_bytes;
           const uint32_t abase = tc_smem_addr(base);
           const uint32_t bbase = u.same ? abase : tc_smem_addr(base + a.s * kOzABytes);
-          const uint32_t bstep = u.same ? kOzABytes : a.b_bytes;
-          for (int d = u.d0; d < u.d1; ++d) {
-            const uint32_t acc = tmem + (uint32_t)((d - u.d0) * a.acc_stride);
-            for (int p = 0; p <= d; ++p) {
-              const int q = d - p;
-              const uint32_t idesc = tc_idesc_i8(a.Nt, p == 0, q == 0);
-              tc_mma_i8(acc, tc_desc_sw32(abase + p * kOzABytes), tc_desc_sw32(bbase + q * bstep), idesc,
-                        (kk > 0 || p > 0) ? 1u : 0u);
-            }
-          }
+          const uint32_t bst = (u.same ? kOzABytes : a.b_bytes) >> 4;
+          const uint64_t da = tc_desc_sw32(abase), db = tc_desc_sw32(bbase);
+          // at most two passes: diagonals [0, ND) and [ND, NS)
+          if (u.d0 == 0) oz_issue<0, ND>(tmem, a.acc_stride, da, db, bst, id, kk == 0);
+          else oz_issue<ND, NS>(tmem, a.acc_stride, da, db, bst, id, kk == 0);
           tc_commit(tc_smem_addr(&empty_bar[st]));
         }
         // accumulators complete (also after a failure, so the epilogue's wait drains the MMAs in flight)
@@ -303,14 +332,14 @@ __global__ void __launch_bounds__(kOzThreads, 1)
           for (int i = 0; i < 16; ++i) sum[i] = 0.0;
           {
             // every accumulator's 16 columns in flight at once, one wait
-            uint32_t v[kOzMaxSlices][16];
+            uint32_t v[ND][16];
             const int nacc = u.d1 - u.d0;
 #pragma unroll
-            for (int j = 0; j < kOzMaxSlices; ++j)
+            for (int j = 0; j < ND; ++j)
               if (j < nacc) tc_ld16_async(tl + (uint32_t)(j * a.acc_stride + c0), v[j]);
             tc_ld_wait();
 #pragma unroll
-            for (int j = 0; j < kOzMaxSlices; ++j)
+            for (int j = 0; j < ND; ++j)
               if (j < nacc) {
                 tc_ld_bind(v[j]);
                 const double w = oz_pow2(-14 - 8 * (u.d0 + j));
