@@ -304,12 +304,12 @@ __global__ void __launch_bounds__(kOzChunk) k_oz_slice_l_blocks(const int64_t* _
     for (int r = 0; r < kOzRows; ++r) {
       x[r] = 0.0;
       if (r < nr) {
+        // one load for every lane (the lanes of a warp may lie on either side of I)
         const int I = rI[r], la = rla[r];
-        int t;
-        if (Jp < I) t = (int)__ldg(sp_first + I * (I + 1) / 2 + Jp) + la + rnA[r] * lb;
-        else if (Jp > I) t = (int)__ldg(sp_first + trib + I) + lb + nB * la;
-        else t = (int)__ldg(sp_first + trib + I) + (la >= lb ? la * (la + 1) / 2 + lb : lb * (lb + 1) / 2 + la);
-        x[r] = __ldg(LJ + t);
+        const int pair = Jp < I ? I * (I + 1) / 2 + Jp : trib + I;
+        const int hi = la >= lb ? la : lb, lo = la >= lb ? lb : la;
+        const int off = Jp < I ? la + rnA[r] * lb : (Jp > I ? lb + nB * la : hi * (hi + 1) / 2 + lo);
+        x[r] = __ldg(LJ + (int)__ldg(sp_first + pair) + off);
       }
     }
   } else {

@@ -165,14 +165,16 @@ __device__ __forceinline__ void oz_for_units(const OzArgs& a, F&& f) {
         if (threadIdx.x == 0) atomicExch(a.err, 2);
         return;
       }
+      // the highest diagonals first: the later pass then needs only the
+      // slices of its own (low) diagonals
       for (int g = 0; g < npass; ++g) {
         OzUnit u;
         u.rowA = ti * 128;
         u.rowB = tj * 128;
         u.k0 = blk * a.kblk + kb0;
         u.nk = (kb1 - kb0) / 32;
-        u.d0 = g * a.nd;
-        u.d1 = min(a.s, u.d0 + a.nd);
+        u.d1 = a.s - g * a.nd;
+        u.d0 = max(0, u.d1 - a.nd);
         u.same = ti == tj;
         u.t0 = ti; u.t1 = tj; u.J = blk; u.nt = 0;
         u.first = g == 0;
@@ -299,9 +301,10 @@ __global__ void __launch_bounds__(kOzThreads, 1)
           const uint32_t bbase = u.same ? abase : tc_smem_addr(base + a.s * kOzABytes);
           const uint32_t bst = (u.same ? kOzABytes : a.b_bytes) >> 4;
           const uint64_t da = tc_desc_sw32(abase), db = tc_desc_sw32(bbase);
-          // at most two passes: diagonals [0, ND) and [ND, NS)
-          if (u.d0 == 0) oz_issue<0, ND>(tmem, a.acc_stride, da, db, bst, id, kk == 0);
-          else oz_issue<ND, NS>(tmem, a.acc_stride, da, db, bst, id, kk == 0);
+          // at most two passes: diagonals [NS - ND, NS), then [0, NS - ND)
+          constexpr int DH = NS - ND;
+          if (u.d1 == NS) oz_issue<DH, NS>(tmem, a.acc_stride, da, db, bst, id, kk == 0);
+          else oz_issue<0, DH>(tmem, a.acc_stride, da, db, bst, id, kk == 0);
           tc_commit(tc_smem_addr(&empty_bar[st]));
         }
         // accumulators complete (also after a failure, so the epilogue's wait drains the MMAs in flight)
