@@ -251,18 +251,20 @@ __global__ void k_oz_lexp(const int* __restrict__ inv, int n, int64_t nrs, const
   if (lane == 0) eL[row] = (short)max(-32000, oz_exponent(m));
 }
 
-// L slicing in blocks: one CTA per (column chunk of 256, block of 16 AO rows,
-// vector J).  Thread t owns column b = c0 + t and loads the 16 elements
-// L_J[a0..a0+16, b] straight from the rs-packed vector, the rs index worked
-// out from the shells of a and b (pair (I, J') with I > J' stores a-fastest,
-// I < J' the mirror, I = J' a triangle, plf_cho_diag.F90:60-72), all 16 loads
-// in flight at once; it cuts them with the cached row exponents into a byte
-// tile in shared memory (S x 16 rows x 256 columns), which the CTA then
-// writes out row by row in 16-byte pieces.  Columns b >= n are zero.
+// L slicing in blocks: one CTA per (256 AOs b, 16 AOs a0..a0+15, vector J).
+// Thread t owns b = c0 + t and loads L_J[a0..a0+16, b] straight from the
+// rs-packed vector, the rs index worked out from the shells of a and b (pair
+// (I, J') with I > J' stores a-fastest, I < J' the mirror, I = J' a
+// triangle, plf_cho_diag.F90:60-72), all 16 loads in flight at once.  L_J is
+// symmetric, so these are also row b, columns a0..a0+15: 16 consecutive K
+// bytes of row b of every slice, cut with row b's cached exponent, packed in
+// registers and written with one 16-byte store per slice (the blocked layout
+// of oz_blk_off).  The grid covers all ld columns a, so the K padding
+// a >= n is written as zeros (as are the rows b >= n).
 // sh_off[ns + 1]: first AO of every shell (sh_off[ns] = n); ao_sh[n]: the
 // shell of every AO.
-constexpr int kOzChunk = 256;   // columns per CTA (= threads)
-constexpr int kOzRows = 16;     // AO rows per CTA
+constexpr int kOzChunk = 256;   // AOs b per CTA (= threads)
+constexpr int kOzRows = 16;     // AOs a per CTA
 
 template <int S>
 __global__ void __launch_bounds__(kOzChunk) k_oz_slice_l_blocks(const int64_t* __restrict__ sp_first,
@@ -273,21 +275,14 @@ __global__ void __launch_bounds__(kOzChunk) k_oz_slice_l_blocks(const int64_t* _
                                                                 const double* __restrict__ D,
                                                                 uint8_t* __restrict__ LS, int* __restrict__ eA,
                                                                 double* __restrict__ V) {
-  __shared__ __align__(16) uint8_t Sb[S][kOzRows][kOzChunk];
-  __shared__ OzScale sc[kOzRows];
-  __shared__ int rI[kOzRows], rla[kOzRows], rnA[kOzRows];  // shell, index in it, its width
+  __shared__ int rI[kOzRows], rla[kOzRows], rnA[kOzRows];  // shell of a, index in it, its width
   __shared__ double red[kOzChunk / 32];
   const int c0 = blockIdx.x * kOzChunk;
   const int a0 = blockIdx.y * kOzRows;
   const int J = blockIdx.z;
-  const int nr = min(kOzRows, n - a0);
-  const int cw = min(kOzChunk, ld - c0);
+  const int nr = max(0, min(kOzRows, n - a0));
   if ((int)threadIdx.x < nr) {
     const int r = threadIdx.x, a = a0 + r;
-    const int64_t row = (int64_t)J * ld + a;
-    const int e = eL[row];
-    sc[r] = oz_scale<S>(e);
-    if (c0 == 0) eA[row] = e;
     const int I = ao_sh[a], aa = sh_off[I];
     rI[r] = I;
     rla[r] = a - aa;
@@ -316,26 +311,31 @@ __global__ void __launch_bounds__(kOzChunk) k_oz_slice_l_blocks(const int64_t* _
 #pragma unroll
     for (int r = 0; r < kOzRows; ++r) x[r] = 0.0;
   }
-  // cut (and the Coulomb contraction V_J += L_J[a, b] D[a, b])
+  // cut, and the Coulomb contraction V_J = sum_ab L_J[a, b] D[a, b] over the
+  // lower triangle (off-diagonal elements twice: L_J and D are symmetric)
   double v = 0.0;
+  if (b < ld) {
+    const int64_t row = (int64_t)J * ld + b;
+    const int e = eL[row];
+    if (blockIdx.y == 0) eA[row] = e;
+    const OzScale sc = oz_scale<S>(e);
+    uint32_t w[S][kOzRows / 4];
 #pragma unroll
-  for (int r = 0; r < kOzRows; ++r) {
-    if (r < nr) {
-      if (b < n) v = fma(x[r], __ldg(D + (size_t)(a0 + r) * n + b), v);
-      const long long y = oz_fixed<S>(x[r], sc[r]);
+    for (int p = 0; p < S; ++p)
 #pragma unroll
-      for (int p = 0; p < S; ++p) Sb[p][r][threadIdx.x] = (uint8_t)(y >> (8 * (S - 1 - p)));
+      for (int q = 0; q < kOzRows / 4; ++q) w[p][q] = 0;
+#pragma unroll
+    for (int r = 0; r < kOzRows; ++r) {
+      const int a = a0 + r;
+      if (r < nr && b <= a) v = fma(b < a ? 2.0 * x[r] : x[r], __ldg(D + (size_t)a * n + b), v);
+      const long long y = oz_fixed<S>(x[r], sc);
+#pragma unroll
+      for (int p = 0; p < S; ++p) w[p][r >> 2] |= (uint32_t)((y >> (8 * (S - 1 - p))) & 255) << (8 * (r & 3));
     }
-  }
-  __syncthreads();
-  // blocked layout (oz_blk_off, 128-row tiles): the nr rows of one 32-byte
-  // column chunk are nr * 32 consecutive bytes; a thread writes 16 of them
-  const int nch = cw / 32;  // cw is a multiple of 128
-  const int64_t row0 = (int64_t)J * ld + a0;
-  for (int o = threadIdx.x; o < S * nch * nr * 2; o += kOzChunk) {
-    const int half = o & 1, rest = o >> 1, rr = rest % nr, r2 = rest / nr, ch = r2 % nch, p = r2 / nch;
-    uint8_t* dst = LS + p * slice + oz_blk_off(row0, c0 + 32 * ch, ld, 128) + rr * 32 + half * 16;
-    *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(&Sb[p][rr][32 * ch + 16 * half]);
+    uint8_t* dst = LS + oz_blk_off(row, a0, ld, 128);  // a0 % 16 == 0: 16 bytes of one 32-byte chunk
+#pragma unroll
+    for (int p = 0; p < S; ++p)
+      *reinterpret_cast<uint4*>(dst + p * slice) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
   }
   v = warp_sum(v);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
@@ -668,7 +668,7 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
       cudaMemsetAsync(xmax, 0, 8 * (size_t)ld, st);
       oz_with_slices(s, [&](auto S) {
         k_oz_slice_l_blocks<decltype(S)::value>
-            <<<dim3((ld + kOzChunk - 1) / kOzChunk, (n + kOzRows - 1) / kOzRows, nv), kOzChunk, 0, st>>>(
+            <<<dim3((ld + kOzChunk - 1) / kOzChunk, ld / kOzRows, nv), kOzChunk, 0, st>>>(
                 cho_sp_first_dev(c), sh_off, ao_sh, n, nrs, Lb, ld, (int64_t)nb * ld * ld, eL + (size_t)J0 * ld, D,
                 LS, eA, V);
       });
