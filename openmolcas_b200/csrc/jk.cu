@@ -319,18 +319,28 @@ __global__ void __launch_bounds__(kOzChunk) k_oz_slice_l_blocks(const int64_t* _
     const int e = eL[row];
     if (blockIdx.y == 0) eA[row] = e;
     const OzScale sc = oz_scale<S>(e);
-    uint32_t w[S][kOzRows / 4];
+    uint32_t w[S][kOzRows / 4];  // slice p, rows 4 g .. 4 g + 3 (one byte each)
 #pragma unroll
-    for (int p = 0; p < S; ++p)
+    for (int g = 0; g < kOzRows / 4; ++g) {
+      uint32_t lo[4], hi[4];  // the two words of Y for the four rows
 #pragma unroll
-      for (int q = 0; q < kOzRows / 4; ++q) w[p][q] = 0;
+      for (int k = 0; k < 4; ++k) {
+        const int r = 4 * g + k, a = a0 + r;
+        if (r < nr && b <= a) v = fma(b < a ? 2.0 * x[r] : x[r], __ldg(D + (size_t)a * n + b), v);
+        const long long y = oz_fixed<S>(x[r], sc);
+        lo[k] = (uint32_t)y;
+        hi[k] = (uint32_t)((unsigned long long)y >> 32);
+      }
+      // byte S-1-p of the four Y into one word: two byte permutes take the
+      // byte from rows (0, 1) and (2, 3), a third joins the halves
 #pragma unroll
-    for (int r = 0; r < kOzRows; ++r) {
-      const int a = a0 + r;
-      if (r < nr && b <= a) v = fma(b < a ? 2.0 * x[r] : x[r], __ldg(D + (size_t)a * n + b), v);
-      const long long y = oz_fixed<S>(x[r], sc);
-#pragma unroll
-      for (int p = 0; p < S; ++p) w[p][r >> 2] |= (uint32_t)((y >> (8 * (S - 1 - p))) & 255) << (8 * (r & 3));
+      for (int p = 0; p < S; ++p) {
+        const int bi = S - 1 - p, kb = bi & 3;
+        const uint32_t sel = (uint32_t)(((4 + kb) << 4) | kb);
+        const uint32_t s01 = bi >= 4 ? __byte_perm(hi[0], hi[1], sel) : __byte_perm(lo[0], lo[1], sel);
+        const uint32_t s23 = bi >= 4 ? __byte_perm(hi[2], hi[3], sel) : __byte_perm(lo[2], lo[3], sel);
+        w[p][g] = __byte_perm(s01, s23, 0x5410);
+      }
     }
     uint8_t* dst = LS + oz_blk_off(row, a0, ld, 128);  // a0 % 16 == 0: 16 bytes of one 32-byte chunk
 #pragma unroll
