@@ -117,11 +117,17 @@ __global__ void k_sp_max(const double* __restrict__ diag, const unsigned char* _
                          double* __restrict__ diash) {
   int sp = blockIdx.x * blockDim.x + threadIdx.x;
   if (sp >= nsp) return;
-  double m = 0.0;
+  // diash[sp]: max(0, largest diagonal) over the pair's members in the
+  // reduced set, -1 when none is in it; diash[nsp + sp]: their largest |diagonal|
+  double m = -1.0, ma = 0.0;
   const int64_t f = sp_first[sp];
   for (int i = 0; i < sp_count[sp]; ++i)
-    if (inred[f + i]) m = fmax(m, diag[f + i]);
+    if (inred[f + i]) {
+      m = fmax(m, fmax(diag[f + i], 0.0));
+      ma = fmax(ma, fabs(diag[f + i]));
+    }
   diash[sp] = m;
+  diash[nsp + sp] = ma;
 }
 
 // Cho_CompVec for one pass, one thread per rs row (rows are independent:
@@ -365,7 +371,7 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
   dev_malloc(&c->d_diag0, sizeof(double) * nrs);
   dev_malloc(&c->d_inred, nrs);
   double* d_tmp = nullptr;
-  dev_malloc(&d_tmp, sizeof(double) * std::max<int64_t>(2 * 296, nsp));
+  dev_malloc(&d_tmp, sizeof(double) * std::max<int64_t>(2 * 296, 2 * (int64_t)nsp));
   double* buf = nullptr;
   size_t bufsz = 0;
   int rc = 0;
@@ -414,18 +420,20 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
   dev_malloc(&d_qrs, sizeof(int) * MQ);
   dev_malloc(&d_Q, sizeof(double) * MQ * MQ);
   dev_malloc(&d_lq, sizeof(double) * (size_t)MQ * kVecBlock);
-  std::vector<double> hdiash(nsp), hq;
+  std::vector<double> hdiash(2 * (size_t)nsp), hq;
   std::vector<int64_t> off_sp(nsp);
   auto Lcol = [&](int J) -> double* { return c->Lblk[J / kVecBlock] + (size_t)nrs * (J % kVecBlock); };
   for (int pass = 0; pass <= nrs; ++pass) {
-    // ---- Cho_SetPass
-    const double dgmax = red_max(c->d_diag, c->d_inred, nrs, d_tmp, 0, st);
-    if (dgmax < cfg.thrcom) break;
-    const double diamin = std::max(dgmax * cfg.span, cfg.thrcom);
+    // ---- Cho_SetPass: the largest reduced-set diagonal of every shell pair
+    // (-1: no member in the reduced set); their maximum is the pass's DGMax
     k_sp_max<<<nblk(nsp), 256, 0, st>>>(c->d_diag, c->d_inred, c->d_sp_first, c->d_sp_count, nsp, d_tmp);
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    cudaMemcpyAsync(hdiash.data(), d_tmp, sizeof(double) * nsp, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hdiash.data(), d_tmp, sizeof(double) * 2 * nsp, cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
+    double dgmax = 0.0;  // max |diagonal| over the reduced set
+    for (int sp = 0; sp < nsp; ++sp) dgmax = std::max(dgmax, hdiash[nsp + sp]);
+    if (dgmax < cfg.thrcom) break;
+    const double diamin = std::max(dgmax * cfg.span, cfg.thrcom);
     double smax = -1e9;
     int spab = -1;
     for (int sp = 0; sp < nsp; ++sp) {
@@ -447,15 +455,11 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
     const int nq = qual.size();
     if (nq == 0) { rc = MG_ERR_DECOMP; err = "empty qualification (Cho_GetInt 104)"; break; }
     // ---- integral columns (CD|AB) for every CD pair touching the reduced set
-    std::vector<unsigned char> hred(nrs);
-    cudaMemcpyAsync(hred.data(), c->d_inred, nrs, cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
+    // (the reduced set has not changed since the shell-pair maxima above)
     std::vector<int32_t> q4;
     std::vector<int> qsp;
     for (int sp = 0; sp < nsp; ++sp) {
-      bool any = false;
-      for (int t = 0; t < c->sp_count[sp] && !any; ++t) any = hred[c->sp_first[sp] + t];
-      if (!any) continue;
+      if (hdiash[sp] < 0.0) continue;
       q4.insert(q4.end(), {h->pairs[sp].i, h->pairs[sp].j, h->pairs[spab].i, h->pairs[spab].j});
       qsp.push_back(sp);
     }
