@@ -68,6 +68,8 @@ int build_eri_items(Handle* h, const int32_t* q4, int64_t nq, const int64_t* off
       cs.max_ne = std::max(cs.max_ne, P.ne);
       cs.max_nf = std::max(cs.max_nf, Q.ne);
       cs.max_nc = std::max(cs.max_nc, nij * nklc);
+      // primitive quartets x roots x (e0|f0) components, plus the contraction
+      cs.work += (double)P.np * Q.np * (nab + ncd + 2) / 2 * nef + (double)nij * nklc * nef;
     }
   }
   items.clear();
@@ -81,6 +83,7 @@ int build_eri_items(Handle* h, const int32_t* q4, int64_t nq, const int64_t* off
     c.begin = items.size();
     c.count = v.size();
     c.plan = eri_plan(c.nab, c.ncd, st[key]);
+    c.work = st[key].work;
     if (c.plan.PAB < 1) {
       h->err = "mg_eri_quartets: class does not fit in shared memory";
       return MG_ERR_ARG;
@@ -109,13 +112,18 @@ int run_eri_items(Handle* h, const std::vector<EriItem>& items, const std::vecto
   cudaMemcpyAsync(d_items, items.data(), sizeof(EriItem) * items.size(), cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(h->d_eri_counters, 0, sizeof(int) * 64, st);
   // The class kernels are independent (own counter, own output blocks): spread them over
-  // the handle's side streams so that the tail of one class overlaps the next class.
+  // the handle's side streams so that the tail of one class overlaps the next class,
+  // the largest classes first (the small ones fill in behind them).
   int rc = side_streams_fork(h, st);
   if (rc) return rc;
-  for (size_t ci = 0; ci < classes.size(); ++ci) {
+  std::vector<int> order(classes.size());
+  for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return classes[a].work > classes[b].work; });
+  for (size_t k = 0; k < order.size(); ++k) {
+    const int ci = order[k];
     const EriClass& c = classes[ci];
     if (eri_launch_class(h, d_items + c.begin, c.count, c.nab, c.ncd, c.plan, d_out, h->d_eri_counters + ci,
-                         h->eri_streams[ci % MG_ERI_STREAMS])) {
+                         h->eri_streams[k % MG_ERI_STREAMS])) {
       h->err = std::string("ERI kernel launch failed: ") + cudaGetErrorString(cudaGetLastError());
       return MG_ERR_CUDA;
     }

@@ -198,6 +198,11 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
     c.ncd1 = key % 8;
     c.begin = plan.items.size();
     c.count = v.size();
+    c.work = 0;
+    for (const GradItem& it : v) {  // primitive quartets x Cartesian components x roots
+      const DPair &P = h->pairs[it.p], &Q = h->pairs[it.q];
+      c.work += (double)P.np * Q.np * ncart(P.la) * ncart(P.lb) * ncart(Q.la) * ncart(Q.lb) * NRc;
+    }
     c.scr = 0;
     for (const GradItem& it : v)
       c.scr = std::max<long long>(c.scr, grad_item_scratch(h->pairs[it.p], h->pairs[it.q], it.i1 - it.i0, it.c1 - it.c0));
@@ -253,11 +258,18 @@ int grad_run(Handle* h, const GradPlan& plan, const double* d_D, const double* d
   // tail of one class overlaps the next.
   int rc = side_streams_fork(h, st);
   if (rc) return rc;
-  for (size_t ci = 0; ci < plan.classes.size(); ++ci) {
+  // largest classes first; the scratch region follows the stream (classes on one
+  // stream run one after another)
+  std::vector<int> order(plan.classes.size());
+  for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return plan.classes[a].work > plan.classes[b].work; });
+  for (size_t pos = 0; pos < order.size(); ++pos) {
+    const size_t ci = order[pos];
     const GradClass& c = plan.classes[ci];
     GradFn k = grad_kernel_m1(c.nab1, c.ncd1);
     if (!k) { h->err = "gradient class out of range"; return MG_ERR_ARG; }
-    const int sk = (int)(ci % MG_ERI_STREAMS);
+    const int sk = (int)(pos % MG_ERI_STREAMS);
     GradArgs a{plan.d_items + c.begin, c.count, h->d_pairs, h->d_prim, h->tot_np, h->d_coef, d_D, h->nbf,
                plan.d_tab, d_grad, plan.d_scratch + plan.scratch_stride * sk, c.scr, plan.d_counters + ci, c.tpq,
                c.gsm, c.pab, c.pcd, c.rw, d_DS, coulfac, 0.25 * exfac};

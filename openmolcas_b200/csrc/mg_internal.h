@@ -70,10 +70,12 @@ struct ClassPlan {
 struct ClassStats {
   int max_acc = 0, max_nef = 0, max_tmp = 0, max_nij = 0, max_npab = 0, max_npcd = 0, max_cab = 0, max_ccd = 0;
   int max_ne = 0, max_nf = 0, max_nc = 0;
+  double work = 0;  // estimated cost of the class's items (launch order only)
 };
 struct EriClass {
   int nab, ncd, begin, count;
   ClassPlan plan;
+  double work;  // estimated cost: classes launch largest first
 };
 
 struct ShellH {
@@ -129,6 +131,7 @@ struct GradClass {
   int minb;       // resident CTAs per SM the kernel variant is compiled for (1..3)
   long long scr;  // global scratch per group (doubles)
   long long grid; // persistent CTAs
+  double work;    // estimated cost: classes launch largest first
 };
 struct GradPlan {
   std::vector<GradItem> items;
