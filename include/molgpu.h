@@ -206,6 +206,26 @@ double mg_drvg1_flops(mg_handle* h, double cutint);
  */
 int mg_rys_roots(mg_handle* h, int nrys, int64_t n, const double* T, double* x, double* w);
 
+/* CD_InCore (cholesky_util/cd_incore.F90:14, cd_incore_1.F90): pivoted
+ * Cholesky vectors of a symmetric positive semidefinite n x n matrix X
+ * (column-major, device memory, overwritten): d_vec (n x maxvec,
+ * column-major) receives *numcho vectors with X ~ vec vec^T, stopping when
+ * the largest remaining diagonal is <= thr (thr < 0: 1e-6).  Returns
+ * CD_InCore's irc: 0; 101 a diagonal below -1e-8; 102 more than maxvec
+ * vectors needed; -1 maxvec < 1; or MG_ERR_ARG / MG_ERR_CUDA.  Synchronous. */
+int mg_cd_incore(mg_handle* h, double* d_X, int n, double thr, double* d_vec, int maxvec, int* numcho,
+                 void* stream);
+
+/* ChoSCF_Drv with a decomposed density (scf/choscf_drv.F90:99-135): the
+ * density D (nbf x nbf, device, symmetric PSD; not modified) is cut into its
+ * Cholesky vectors by CD_InCore at 1e-8 of its largest diagonal (held by the
+ * handle), which then drive CHO_LK_SCF: FLT += J[D] - FactXI K[D] as
+ * mg_cho_lk_scf.  *nvec (may be NULL) receives the number of vectors (the
+ * occupied count for an idempotent closed-shell density).  Returns 0,
+ * CD_InCore's irc 101/102, or MG_ERR_*.  Synchronous. */
+int mg_choscf_lk(mg_handle* h, const double* d_D, double factxi, double* d_FLT, int precision, int* nvec,
+                 void* stream);
+
 /* The 8-bit sliced tensor-core engine of MG_PREC_MIXED on given dense FP64
  * matrices (verification; no reference counterpart): X = A B with A
  * (ld x ld), B (ld x r) and X (ld x r) column-major, then K = X X^T into

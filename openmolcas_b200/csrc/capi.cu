@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <string>
 #include <vector>
 
 #include "../../include/molgpu.h"
@@ -197,6 +198,7 @@ int mg_destroy(mg_handle* H) {
   cudaFree(h->d_rys);
   cudaFree(h->d_eri_counters);
   cudaFree(h->d_lk);
+  cudaFree(h->d_dcd);
   for (int k = 0; k < MG_ERI_STREAMS; ++k) {
     if (h->eri_streams[k]) cudaStreamDestroy(h->eri_streams[k]);
     if (h->eri_events[k]) cudaEventDestroy(h->eri_events[k]);
@@ -550,6 +552,53 @@ int mg_cho_lk_scf(mg_handle* H, const double* d_C, int r, double factxi, double*
   int rc = mg_cho_jk(H, d_C, r, h->d_lk, h->d_lk + nn, precision, stream);
   if (rc) return rc;
   return fock_accumulate(d_FLT, h->d_lk, h->d_lk + nn, factxi, (int64_t)nn, (cudaStream_t)stream);
+}
+
+int mg_cd_incore(mg_handle* H, double* d_X, int n, double thr, double* d_vec, int maxvec, int* numcho,
+                 void* stream) {
+  if (!H || !numcho || (n > 0 && (!d_X || !d_vec))) return MG_ERR_ARG;
+  cudaSetDevice(H->h.device);
+  return cd_incore(&H->h, d_X, n, thr, d_vec, maxvec, numcho, (cudaStream_t)stream);
+}
+
+int mg_choscf_lk(mg_handle* H, const double* d_D, double factxi, double* d_FLT, int precision, int* nvec,
+                 void* stream) {
+  if (!H || !d_D || !d_FLT) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  if (!h->cho) { h->err = "mg_choscf_lk: no Cholesky vectors (call mg_cho_drv)"; return MG_ERR_ARG; }
+  cudaSetDevice(h->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = h->nbf;
+  const size_t nn = (size_t)n * n;
+  if (h->dcd_cap < nn) {
+    cudaFree(h->d_dcd);
+    h->d_dcd = nullptr;
+    h->dcd_cap = 0;
+    if (dev_malloc(&h->d_dcd, 2 * nn * sizeof(double)) != cudaSuccess) {
+      h->err = "mg_choscf_lk: allocation failed";
+      return MG_ERR_MEMORY;
+    }
+    h->dcd_cap = nn;
+  }
+  double* X = h->d_dcd;
+  double* Vec = h->d_dcd + nn;
+  // Thr = 1e-8 of the largest diagonal of D (choscf_drv.F90:110-115)
+  std::vector<double> dg(n);
+  cudaMemcpy2DAsync(dg.data(), sizeof(double), d_D, sizeof(double) * (n + 1), sizeof(double), n,
+                    cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(X, d_D, nn * sizeof(double), cudaMemcpyDeviceToDevice, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) { h->err = "mg_choscf_lk: copy failed"; return MG_ERR_CUDA; }
+  double ymax = 0.0;
+  for (double v : dg) ymax = std::max(ymax, v);
+  int numv = 0;
+  const int rc = cd_incore(h, X, n, 1.0e-8 * ymax, Vec, n, &numv, st);
+  if (nvec) *nvec = numv;
+  if (rc) {
+    if (rc > 100) h->err = "mg_choscf_lk: the density is not positive semidefinite (CD_InCore irc " + std::to_string(rc) + ")";
+    return rc;
+  }
+  if (numv == 0) return 0;  // D = 0: nothing to add
+  return mg_cho_lk_scf(H, Vec, numv, factxi, d_FLT, precision, stream);
 }
 
 int mg_sliced_selftest(mg_handle* H, int ld, int r, int slices, const double* d_A, const double* d_B, double* d_X,

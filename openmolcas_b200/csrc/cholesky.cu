@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "cho_qualify.h"
+#include "kern_common.cuh"
 #include "mg_internal.h"
 
 namespace mg {
@@ -599,6 +600,123 @@ void cho_set_lexp(ChoState* c, short* p, int ld) {
   cudaFree(c->d_lexp);
   c->d_lexp = p;
   c->lexp_ld = ld;
+}
+
+// ------------------------------------------------- in-core decomposition
+// CD_InCore (cholesky_util/cd_incore.F90:14 -> cd_incore_1.F90): pivoted
+// Cholesky factor of a symmetric positive semidefinite n x n matrix X, left
+// looking: each step takes the largest remaining diagonal (the first one,
+// in index order, that exceeds the running maximum by more than
+// Acc = min(1e-12, Thr/100)), updates only the pivot column against the
+// previous vectors, scales it into the new vector and subtracts its square
+// from the diagonal; diagonals below ThrNeg = -1e-13 are zeroed with their
+// row and column, below ThrFail = -1e-8 the decomposition fails (irc 101);
+// it stops when the largest diagonal is <= Thr.  One CTA: thread 0 scans the
+// diagonal (shared memory) in index order, as the tie rule needs; the column
+// update, the new vector and the diagonal update are row-parallel.
+// out[0] = NumCho, out[1] = irc (0, 101, 102).
+constexpr int kCdThreads = 1024;
+
+__global__ void __launch_bounds__(kCdThreads) k_cd_incore(double* __restrict__ X, int n, double* __restrict__ Vec,
+                                                          int maxvec, double thr, int* __restrict__ out) {
+  extern __shared__ double cd_dg[];  // the diagonal of X, then n ints of zeroed indices
+  int* zl = reinterpret_cast<int*>(cd_dg + n);
+  __shared__ int s_imax, s_stop, s_nz;
+  __shared__ double s_xmax;
+  const double thrneg = -1.0e-13, thrfail = -1.0e-8;
+  const double acc = fmin(1.0e-12, thr * 1.0e-2);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) cd_dg[i] = X[i + (size_t)n * i];
+  __syncthreads();
+  int numcho = 0, irc = 0;
+  for (int pass = 0; pass < n; ++pass) {
+    if (threadIdx.x == 0) {
+      int nz = 0, imax = -1, stop = 0;
+      double xmax = 0.0;
+      for (int i = 0; i < n; ++i) {
+        double d = cd_dg[i];
+        if (d < thrneg) {
+          if (d < thrfail) {
+            stop = 101;
+            break;
+          }
+          d = 0.0;
+          cd_dg[i] = 0.0;
+          zl[nz++] = i;
+        }
+        if (d > xmax + acc) {
+          xmax = d;
+          imax = i;
+        }
+      }
+      if (!stop && xmax <= thr) stop = 1;  // converged
+      if (!stop && numcho == maxvec) stop = 102;
+      s_imax = imax;
+      s_xmax = xmax;
+      s_stop = stop;
+      s_nz = nz;
+    }
+    __syncthreads();
+    if (s_stop) {
+      irc = s_stop == 1 ? 0 : s_stop;
+      break;
+    }
+    for (int z = 0; z < s_nz; ++z) {  // rows and columns of the zeroed diagonals
+      const int iz = zl[z];
+      for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        X[k + (size_t)n * iz] = 0.0;
+        X[iz + (size_t)n * k] = 0.0;
+      }
+    }
+    __syncthreads();
+    const int imax = s_imax;
+    const double xmax = s_xmax, xfac = 1.0 / sqrt(fabs(xmax));
+    double* vnew = Vec + (size_t)n * numcho;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      double x = X[i + (size_t)n * imax];
+      for (int j = 0; j < numcho; ++j) x -= Vec[imax + (size_t)n * j] * Vec[i + (size_t)n * j];
+      if (i == imax) x = xmax;
+      X[i + (size_t)n * imax] = x;
+      const double v = cd_dg[i] == 0.0 ? 0.0 : xfac * x;
+      vnew[i] = v;
+      cd_dg[i] -= v * v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) cd_dg[imax] = 0.0;
+    ++numcho;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = numcho;
+    out[1] = irc;
+  }
+}
+
+int cd_incore(Handle* h, double* d_X, int n, double thr, double* d_vec, int maxvec, int* numcho, cudaStream_t st) {
+  *numcho = 0;
+  if (n < 1) return 0;
+  if (maxvec < 1) return -1;
+  if (thr < 0.0) thr = 1.0e-6;  // CD_InCore's DefThr
+  const size_t smem = (size_t)n * (sizeof(double) + sizeof(int));
+  if (smem > 200 * 1024) {
+    h->err = "in-core decomposition: n above 17066";
+    return MG_ERR_ARG;
+  }
+  if (!smem_attr_once((const void*)k_cd_incore, 200 * 1024)) {
+    h->err = "in-core decomposition: shared-memory limit could not be raised";
+    return MG_ERR_CUDA;
+  }
+  int* d_out = (int*)ws_get(h, 2 * sizeof(int), st);
+  if (!d_out) { h->err = "workspace allocation failed"; return MG_ERR_MEMORY; }
+  k_cd_incore<<<1, kCdThreads, smem, st>>>(d_X, n, d_vec, maxvec, thr, d_out);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  int hout[2] = {0, 0};
+  cudaMemcpyAsync(hout, d_out, sizeof(hout), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    h->err = "in-core decomposition: CUDA error";
+    return MG_ERR_CUDA;
+  }
+  *numcho = hout[0];
+  return hout[1];
 }
 
 }  // namespace mg

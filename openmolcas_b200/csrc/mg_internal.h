@@ -118,6 +118,8 @@ struct Handle {
   cudaEvent_t eri_fork = nullptr;
   double* d_lk = nullptr;          // J and K of mg_cho_lk_scf (2 nbf^2)
   size_t lk_cap = 0;
+  double* d_dcd = nullptr;         // density copy and its Cholesky vectors of mg_choscf_lk (2 nbf^2)
+  size_t dcd_cap = 0;
 };
 
 struct GradItem {
@@ -180,6 +182,9 @@ short* cho_lexp(const ChoState* c, int ld);
 void cho_set_lexp(ChoState* c, short* p, int ld);
 int oz_selftest(Handle* h, int ld, int r, int s, const double* d_A, const double* d_B, double* d_X, double* d_K,
                 uint8_t* d_slices, int* d_exps, cudaStream_t st);
+// CD_InCore (cholesky_util/cd_incore.F90:14) on the device: returns irc
+// (0, 101, 102, -1) or MG_ERR_*; X (n x n, column-major) is overwritten.
+int cd_incore(Handle* h, double* d_X, int n, double thr, double* d_vec, int maxvec, int* numcho, cudaStream_t st);
 int fock_accumulate(double* F, const double* J, const double* K, double factxi, int64_t n, cudaStream_t st);
 int jk_fp64(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block);
 int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block, int s, int sk);

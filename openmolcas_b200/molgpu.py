@@ -59,6 +59,8 @@ def lib():
                              C.c_void_p]
     L.mg_cho_jk.argtypes = [vp, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     L.mg_rys_roots.argtypes = [vp, C.c_int, C.c_int64, d, d, d]
+    L.mg_cd_incore.argtypes = [vp, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_int, i, C.c_void_p]
+    L.mg_choscf_lk.argtypes = [vp, C.c_void_p, C.c_double, C.c_void_p, C.c_int, i, C.c_void_p]
     L.mg_eri_work.argtypes = [vp, i32, C.c_int64, d, d]
     _lib = L
     return L
@@ -235,6 +237,37 @@ class MolGpu:
         self._check(self.L.mg_cho_jk(self.h, C.c_void_p(Cc.data_ptr()), r, C.c_void_p(J.data_ptr()),
                                      C.c_void_p(K.data_ptr()), precision, _stream(self.device)), "mg_cho_jk")
         return J, K
+
+    def cd_incore(self, X: torch.Tensor, thr: float = 1e-6, maxvec: int | None = None):
+        """CD_InCore (cholesky_util/cd_incore.F90:14): pivoted Cholesky vectors of
+        a symmetric positive semidefinite matrix X (n x n; not modified).
+        Returns (Vec, irc): Vec (n x NumCho, X ~ Vec Vec^T to thr) and CD_InCore's
+        return code (0; 101 a diagonal below -1e-8; 102 more than maxvec vectors)."""
+        dev = f"cuda:{self.device}"
+        Xc = X.to(device=dev, dtype=torch.float64).t().contiguous()  # column-major copy (overwritten)
+        n = Xc.shape[0]
+        maxvec = n if maxvec is None else int(maxvec)
+        V = torch.zeros((max(maxvec, 1), n), dtype=torch.float64, device=dev)  # column-major n x maxvec
+        nc = C.c_int(0)
+        rc = self.L.mg_cd_incore(self.h, C.c_void_p(Xc.data_ptr()), n, thr, C.c_void_p(V.data_ptr()), maxvec,
+                                 C.byref(nc), _stream(self.device))
+        if rc not in (0, 101, 102):
+            self._check(rc, "mg_cd_incore")
+        return V[:nc.value].t(), rc
+
+    def choscf_lk(self, D: torch.Tensor, factxi: float, FLT: torch.Tensor, precision: int = 0) -> int:
+        """ChoSCF_Drv with the decomposed density (scf/choscf_drv.F90:99-135): D is
+        cut into Cholesky vectors (CD_InCore at 1e-8 of its largest diagonal) and
+        FLT += J[D] - factxi K[D] in place (FLT: nbf x nbf device tensor).
+        Returns the number of density vectors."""
+        dev = f"cuda:{self.device}"
+        Dc = D.to(device=dev, dtype=torch.float64).contiguous()  # symmetric: layout-agnostic
+        if FLT.dtype != torch.float64 or not FLT.is_contiguous() or FLT.device != torch.device(dev):
+            raise MolGpuError("FLT must be a contiguous float64 tensor on the handle's device")
+        nv = C.c_int(0)
+        self._check(self.L.mg_choscf_lk(self.h, C.c_void_p(Dc.data_ptr()), factxi, C.c_void_p(FLT.data_ptr()),
+                                        precision, C.byref(nv), _stream(self.device)), "mg_choscf_lk")
+        return nv.value
 
     # -------------------------------------------------------- gradient
     def drvg1(self, D: torch.Tensor, cutint: float = 1e-12, out: torch.Tensor | None = None,

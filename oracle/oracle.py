@@ -232,6 +232,47 @@ def cho_jk_blas(rs_a, rs_b, n, L, Cm, batch=16):
     return J, K
 
 
+def cd_incore(X, thr=1e-6, maxvec=None):
+    """CD_InCore restated (cholesky_util/cd_incore.F90:14-44 and
+    cd_incore_1.F90:14-100): left-looking pivoted Cholesky of a symmetric
+    positive semidefinite matrix with the reference's pivot rule (the first
+    diagonal, in index order, above the running maximum + Acc,
+    Acc = min(1e-12, Thr/100)), ThrNeg = -1e-13 (zero the row and column),
+    ThrFail = -1e-8 (irc 101), MxVec (irc 102).  Returns (Vec, irc)."""
+    X = np.array(X, dtype=np.float64, copy=True)
+    n = X.shape[0]
+    if thr < 0.0:
+        thr = 1e-6
+    maxvec = n if maxvec is None else maxvec
+    vec = np.zeros((n, maxvec))
+    acc = min(1e-12, thr * 1e-2)
+    numcho = 0
+    for _ in range(n):
+        xmax, imax = 0.0, -1
+        for i in range(n):
+            if X[i, i] < -1e-13:
+                if X[i, i] < -1e-8:
+                    return vec[:, :numcho], 101
+                X[:, i] = 0.0
+                X[i, :] = 0.0
+            if X[i, i] > xmax + acc:
+                xmax, imax = X[i, i], i
+        if xmax <= thr:
+            return vec[:, :numcho], 0
+        if numcho == maxvec:
+            return vec[:, :numcho], 102
+        xfac = 1.0 / np.sqrt(abs(xmax))
+        for j in range(numcho):
+            X[:, imax] -= vec[imax, j] * vec[:, j]
+        X[imax, imax] = xmax
+        d = np.diagonal(X).copy()
+        vec[:, numcho] = np.where(d == 0.0, 0.0, xfac * X[:, imax])
+        numcho += 1
+        X[np.arange(n), np.arange(n)] -= vec[:, numcho - 1] ** 2
+        X[imax, imax] = 0.0
+    return vec[:, :numcho], 0
+
+
 def num_threads():
     return lib().or_num_threads()
 

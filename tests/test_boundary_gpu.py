@@ -158,3 +158,58 @@ def test_torch_ops(small):
     assert abs(float(E) - float(0.5 * (D * J).sum() - 0.25 * (D * K).sum())) < 1e-10 * abs(float(E))
     assert float((Cg.grad - 2.0 * (J - 0.5 * K) @ Cn).abs().max()) < 1e-12 * float(Cg.grad.abs().max())
     torch_ops.unregister(h)
+
+
+@pytest.mark.parametrize("n,rank,case", [(120, 15, "plain"), (300, 40, "zeroed"), (64, 64, "full"),
+                                         (50, 10, "fail"), (50, 10, "maxvec")])
+def test_cd_incore_matches_oracle(small, n, rank, case):
+    """mg_cd_incore (CD_InCore, cholesky_util/cd_incore.F90:14) against the
+    oracle's restatement: the same number of vectors in the same pivot order
+    (vectors equal to FP64 rounding), the reconstruction, and the return codes
+    101 (a diagonal below -1e-8) and 102 (MxVec too small)."""
+    g = small[1]
+    rng = np.random.default_rng(n + rank)
+    C0 = rng.standard_normal((n, rank))
+    X = C0 @ C0.T
+    maxvec = None
+    if case == "zeroed":  # a diagonal just below zero: zeroed with its row and column
+        X[7, :] = 0.0
+        X[:, 7] = 0.0
+        X[7, 7] = -5e-12
+    elif case == "fail":
+        X[4, 4] = -1e-6
+    elif case == "maxvec":
+        maxvec = rank - 3
+    Vr, ircr = O.cd_incore(X, 1e-9, maxvec)
+    V, irc = g.cd_incore(torch.from_numpy(X), 1e-9, maxvec)
+    assert irc == ircr
+    V = V.cpu().numpy()
+    assert V.shape == Vr.shape
+    if V.size:
+        assert np.abs(V - Vr).max() < 1e-10 * np.abs(Vr).max()
+    if case in ("plain", "zeroed", "full"):
+        assert irc == 0 and V.shape[1] == rank
+        assert np.abs(V @ V.T - X).max() < 1e-9 * np.abs(X).max()
+
+
+def test_choscf_lk_decomposes_the_density(small):
+    """mg_choscf_lk (ChoSCF_Drv with a decomposed density, scf/choscf_drv.F90:
+    99-135): the density is cut into its Cholesky vectors (as many as its
+    rank) and FLT += J - FactXI K equals mg_cho_lk_scf with the factor the
+    density was made from, both precisions."""
+    mol, g, _ = small
+    g.cho_drv(thrcom=1e-8)
+    Cn = torch.from_numpy(B.density_factor(g.nbf, 5, 3)).cuda()
+    D = Cn @ Cn.t()
+    Cc = Cn.t().contiguous()
+    f = lib().mg_cho_lk_scf
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_void_p]
+    for prec in (MolGpu.PREC_FP64, MolGpu.PREC_MIXED):
+        F0 = torch.randn(g.nbf, g.nbf, dtype=torch.float64, device="cuda")
+        Fa = F0.clone()
+        nv = g.choscf_lk(D, 0.5, Fa, precision=prec)
+        Fb = F0.clone()
+        assert f(g.h, Cc.data_ptr(), 5, 0.5, Fb.data_ptr(), prec, None) == 0
+        torch.cuda.synchronize()
+        assert nv == 5
+        assert float((Fa - Fb).abs().max()) <= 1e-11 * float((Fb - F0).abs().max())

@@ -279,3 +279,26 @@ def test_cholesky_qualify_2_replaces_when_a_shell_pair_exceeds_maxqual():
         resid = diag - np.einsum("tj,tj->t", r["L"], r["L"])
         assert resid.max() <= 1e-6 and resid.min() > -1e-10
         assert len(set(r["piv"].tolist())) == r["M"]
+
+
+def test_cd_incore_restatement():
+    """CD_InCore (cholesky_util/cd_incore_1.F90) restated: a rank-7 PSD matrix
+    gives 7 vectors reproducing it, a slightly negative diagonal (above
+    ThrNeg's failure bound) is zeroed with its row and column, a diagonal below
+    -1e-8 fails with irc 101 and too small a MxVec with irc 102."""
+    rng = np.random.default_rng(1)
+    C0 = rng.standard_normal((40, 7))
+    X = C0 @ C0.T
+    V, irc = O.cd_incore(X, 1e-10)
+    assert irc == 0 and V.shape == (40, 7)
+    assert np.abs(V @ V.T - X).max() < 1e-12 * np.abs(X).max()
+    X2 = X.copy()
+    X2[3, :] = 0.0
+    X2[:, 3] = 0.0
+    X2[3, 3] = -5e-12
+    V2, irc2 = O.cd_incore(X2, 1e-10)
+    assert irc2 == 0 and np.all(V2[3] == 0.0)
+    X3 = X.copy()
+    X3[5, 5] = -1e-7
+    assert O.cd_incore(X3, 1e-10)[1] == 101
+    assert O.cd_incore(X, 1e-10, maxvec=3)[1] == 102
