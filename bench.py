@@ -275,7 +275,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="molgpu", choices=["molgpu", "reference"])
-    ap.add_argument("--leg", default=None, choices=["eri", "grad", "jk"],
+    ap.add_argument("--leg", default=None, choices=["eri", "grad", "jk", "c5"],
                     help="run one leg alone (timing / profiling driver), no JSON line")
     ap.add_argument("--cfg", default=None, help="--leg eri/grad: configuration (c2, c4, small, medium)")
     ap.add_argument("--quartets", type=int, default=20000, help="--leg eri: sample size")
@@ -555,7 +555,8 @@ def run_leg(args):
     --nvtx-include "<leg>/" selects its kernels), timed with CUDA events:
       --leg eri  --cfg c2 --quartets N   seeded sample of the screened unique quartets
       --leg grad --cfg c4|small|medium   two-electron gradient (small/medium: 4/8 atoms of 4s3p2d)
-      --leg jk   --natom N               Cholesky (ThrCom 1e-6) + J/K, N atoms of the 1500-bf mix"""
+      --leg jk   --natom N               Cholesky (ThrCom 1e-6) + J/K, N atoms of the 1500-bf mix
+      --leg c5                           C5: Cholesky + mixed/FP64 J/K of 8 densities, CPU J/K sample"""
     import torch
     from openmolcas_b200 import basis as B
     from openmolcas_b200.molgpu import MolGpu, unique_quartets
@@ -596,6 +597,8 @@ def run_leg(args):
         D = torch.from_numpy(Cn @ Cn.T).cuda()
         grad, ms = timed(lambda: g.drvg1(D, cutint=CUTINT))
         print(f"grad {cfg}: nbf {m.nbf}, last {ms[-1]:.1f} ms, |sum F| = {float(grad.sum(0).abs().max()):.2e}")
+    elif args.leg == "c5":
+        run_c5(timed)
     else:
         c3 = B.CONFIGS[JK_CFG]
         natom = args.natom
@@ -623,6 +626,63 @@ def run_leg(args):
             line += f", {name} {ms:.2f} ms (E {E:.10f})"
         print(line)
     return 0
+
+
+def run_c5(timed):
+    """The full-scale system (250 seeded atoms, 2s1p / 3s2p1d / 4s3p2d1f, 1815
+    functions): the ERI Cholesky decomposition at ThrCom 1e-6, then J/K of 8
+    random densities of uneven rank (50..300) through the mixed and the FP64
+    path, each with its energy difference; the CPU restatement of the J/K
+    (CHO_LK_SCF through BLAS) timed on a sample of the vectors for every
+    density and scaled to all of them.  The gradient of this system is not
+    run (about 10^3 s per density at the measured C4 rate).  One JSON line."""
+    import torch
+    from openmolcas_b200 import basis as B
+    from openmolcas_b200.molgpu import MolGpu
+    m = B.config_molecule("c5")
+    g = MolGpu(m)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    info = g.cho_drv(thrcom=THRCOM)
+    torch.cuda.synchronize()
+    t_cd = time.time() - t0
+    ranks = [int(round(r)) for r in np.linspace(50, 300, 8)]
+    dens = []
+    for k, rk in enumerate(ranks):
+        Cd = torch.from_numpy(B.density_factor(m.nbf, rk, 5 + k)).cuda()
+        D = Cd @ Cd.t()
+        row = {"rank": rk}
+        for name, prec in (("mixed", MolGpu.PREC_MIXED), ("fp64", MolGpu.PREC_FP64)):
+            g.cho_jk(Cd, precision=prec)  # untimed first call (row exponents, workspace)
+            torch.cuda.synchronize()
+            (J, K), ms = timed(lambda: g.cho_jk(Cd, precision=prec))
+            row[name + "_s"] = ms[-1] / 1e3
+            row["E_" + name] = float(0.5 * (D * J).sum() - 0.25 * (D * K).sum())
+        row["dE"] = row["E_mixed"] - row["E_fp64"]
+        dens.append(row)
+    del g
+    torch.cuda.empty_cache()
+    # CPU restatement on a sample of the vectors (the cost does not depend on their values)
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    rs_a, rs_b, _ = O.Oracle(m).rs_list()
+    nv = 8 * threads
+    L = np.random.default_rng(0).standard_normal((rs_a.size, nv)) * 1e-3
+    cpu = 0.0
+    for k, rk in enumerate(ranks):
+        Cm = B.density_factor(m.nbf, rk, 5 + k)
+        t0 = time.time()
+        O.cho_jk_blas(rs_a, rs_b, m.nbf, L, Cm)
+        cpu += (time.time() - t0) * info["M"] / nv
+    mixed = sum(r["mixed_s"] for r in dens)
+    fp64 = sum(r["fp64_s"] for r in dens)
+    print(json.dumps({"workload": f"c5: 250 atoms, {m.nbf} bf, ThrCom {THRCOM}, 8 densities of rank {ranks}",
+                      "cholesky": {"seconds": t_cd, "M": info["M"], "npass": info["npass"]},
+                      "jk_mixed_s": mixed, "jk_fp64_s": fp64, "speedup": fp64 / mixed,
+                      "max_abs_dE": max(abs(r["dE"]) for r in dens), "densities": dens,
+                      "cpu_baseline": {"jk_s": cpu, "cores": threads, "kind": "port",
+                                       "sample": f"CHO_LK_SCF through BLAS over {nv} of {info['M']} vectors per "
+                                                 f"density, x{info['M'] / nv:.1f}"}}))
 
 
 def run_reference(args):
