@@ -513,7 +513,9 @@ class CpuRef:
         m3 = B.config_molecule(JK_CFG)
         self.M = int(M or C3_NVEC)
         self.n = m3.nbf
-        self.rs_a, self.rs_b, _ = O.Oracle(m3).rs_list()
+        o3 = O.Oracle(m3)
+        o3.rs_compact(THRCOM)  # the AO pairs the vectors are stored over
+        self.rs_a, self.rs_b, _ = o3.rs_list()
         nrs = self.rs_a.size
         self.nv = max(8 * self.threads, -(-self.M // CPU_SAMPLE_FACTOR))
         self.L = np.random.default_rng(0).standard_normal((nrs, self.nv)) * 1e-3
@@ -665,7 +667,9 @@ def run_c5(timed):
     # CPU restatement on a sample of the vectors (the cost does not depend on their values)
     from oracle import oracle as O
     threads = os.cpu_count() or 1
-    rs_a, rs_b, _ = O.Oracle(m).rs_list()
+    o5 = O.Oracle(m)
+    o5.rs_compact(THRCOM)  # the AO pairs the vectors are stored over
+    rs_a, rs_b, _ = o5.rs_list()
     nv = 8 * threads
     L = np.random.default_rng(0).standard_normal((rs_a.size, nv)) * 1e-3
     cpu = 0.0

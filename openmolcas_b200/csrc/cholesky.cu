@@ -230,13 +230,22 @@ void cho_free(ChoState* c) {
   delete c;
 }
 
-// AO-pair list in reduced-set order (plf_cho_diag.F90:60-72 conventions)
-static void make_rs(Handle* h, ChoState* c) {
+// AO-pair list in reduced-set order (plf_cho_diag.F90:60-72 conventions):
+// every shell pair (keep == nullptr) or the shell pairs with keep[sp] set
+// (the others get sp_first = -1 and no rows).  Replaces a previous list.
+static void make_rs(Handle* h, ChoState* c, const std::vector<char>* keep = nullptr) {
+  cudaFree(c->d_rs_a); cudaFree(c->d_rs_b); cudaFree(c->d_rs); cudaFree(c->d_sp_first); cudaFree(c->d_sp_count);
+  c->rs_a.clear(); c->rs_b.clear(); c->rs_sp.clear(); c->sp_first.clear(); c->sp_count.clear();
   const int ns = h->sh.size();
   std::vector<RsDev> rsd;
   for (int i = 0; i < ns; ++i)
     for (int j = 0; j <= i; ++j) {
       const int sp = pair_id(i, j);
+      if (keep && !(*keep)[sp]) {
+        c->sp_first.push_back(-1);
+        c->sp_count.push_back(0);
+        continue;
+      }
       const ShellH &A = h->sh[i], &B = h->sh[j];
       const int nA = A.nc * A.ncomp, nB = B.nc * B.ncomp;
       c->sp_first.push_back(c->rs_a.size());
@@ -363,20 +372,21 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
   ChoState* c = new ChoState;
   out = c;
   make_rs(h, c);
-  const int64_t nrs = c->nrs;
   const int nsp = c->sp_count.size();
   const double damp = cho_default_damp(cfg.thrcom);
   if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS) { err = "cublasCreate failed"; return MG_ERR_CUDA; }
   cublasSetStream(c->cublas, st);
-  dev_malloc(&c->d_diag, sizeof(double) * nrs);
-  dev_malloc(&c->d_diag0, sizeof(double) * nrs);
-  dev_malloc(&c->d_inred, nrs);
   double* d_tmp = nullptr;
   dev_malloc(&d_tmp, sizeof(double) * std::max<int64_t>(2 * 296, 2 * (int64_t)nsp));
   double* buf = nullptr;
   size_t bufsz = 0;
   int rc = 0;
-  // ---- diagonal (CHO_GETDIAG): (AB|AB) for every shell pair
+  // ---- diagonal (CHO_GETDIAG): (AB|AB) for every shell pair, then the initial
+  // screening (cho_calcdiag.F90:255-300): elements below
+  // ScrMax = ThrCom^2 / (Damp DiaMax) leave the reduced set.  The vectors are
+  // stored over the shell pairs that keep at least one element (their rows
+  // outside a pass's reduced set are zero), so the rs list is rebuilt over them.
+  double scrmax = 1e15;
   {
     std::vector<int32_t> q4;
     for (int sp = 0; sp < nsp; ++sp) {
@@ -389,22 +399,36 @@ int cho_decompose(Handle* h, const ChoCfgH& cfg, ChoState*& out, cudaStream_t st
     int64_t* d_off = nullptr;
     dev_malloc(&d_off, sizeof(int64_t) * nsp);
     cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * nsp, cudaMemcpyHostToDevice, st);
-    k_extract_diag<<<nblk(nrs), 256, 0, st>>>(c->d_rs, nrs, h->d_pairs, d_off, buf, c->d_diag0);
+    // full diagonal, every shell pair
+    double* d_full = nullptr;
+    dev_malloc(&d_full, sizeof(double) * c->nrs);
+    k_extract_diag<<<nblk(c->nrs), 256, 0, st>>>(c->d_rs, c->nrs, h->d_pairs, d_off, buf, d_full);
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    cudaMemcpyAsync(c->d_diag, c->d_diag0, sizeof(double) * nrs, cudaMemcpyDeviceToDevice, st);
+    std::vector<double> hd(c->nrs);
+    cudaMemcpyAsync(hd.data(), d_full, sizeof(double) * c->nrs, cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    cudaFree(d_full);
+    double dm = 0;
+    for (double v : hd) dm = std::max(dm, std::fabs(v));
+    if (dm > 0) scrmax = cfg.thrcom * cfg.thrcom / damp / dm;
+    std::vector<char> keep(nsp, 0);
+    for (int64_t t = 0; t < c->nrs; ++t)
+      if (!(hd[t] < scrmax)) keep[c->rs_sp[t]] = 1;
+    make_rs(h, c, &keep);
+    // the diagonal over the kept shell pairs, from the same integral blocks
+    dev_malloc(&c->d_diag, sizeof(double) * std::max<int64_t>(c->nrs, 1));
+    dev_malloc(&c->d_diag0, sizeof(double) * std::max<int64_t>(c->nrs, 1));
+    dev_malloc(&c->d_inred, std::max<int64_t>(c->nrs, 1));
+    k_extract_diag<<<nblk(std::max<int64_t>(c->nrs, 1)), 256, 0, st>>>(c->d_rs, c->nrs, h->d_pairs, d_off, buf,
+                                                                        c->d_diag0);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    cudaMemcpyAsync(c->d_diag, c->d_diag0, sizeof(double) * c->nrs, cudaMemcpyDeviceToDevice, st);
     cudaStreamSynchronize(st);
     cudaFree(d_off);
   }
-  // ---- initial screening (cho_calcdiag.F90:255-300)
-  {
-    std::vector<double> hd(nrs);
-    cudaMemcpy(hd.data(), c->d_diag, sizeof(double) * nrs, cudaMemcpyDeviceToHost);
-    double dm = 0;
-    for (double v : hd) dm = std::max(dm, std::fabs(v));
-    const double scrmax = dm > 0 ? cfg.thrcom * cfg.thrcom / damp / dm : 1e15;
-    k_init_red<<<nblk(nrs), 256, 0, st>>>(c->d_diag, c->d_inred, nrs, scrmax);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-  }
+  const int64_t nrs = c->nrs;
+  k_init_red<<<nblk(std::max<int64_t>(nrs, 1)), 256, 0, st>>>(c->d_diag, c->d_inred, nrs, scrmax);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   int* d_flags = nullptr;
   dev_malloc(&d_flags, sizeof(int));
   cudaMemsetAsync(d_flags, 0, sizeof(int), st);

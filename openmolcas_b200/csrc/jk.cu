@@ -127,6 +127,9 @@ int jk_fp64(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaS
   g_launches.fetch_add(1, std::memory_order_relaxed);
   cudaMemsetAsync(jrs, 0, sizeof(double) * nrs, st);
   cudaMemsetAsync(d_K, 0, sizeof(double) * n * n, st);
+  // AO pairs without rows (screened-out shell pairs) stay zero in every square
+  cudaMemsetAsync(Lsq, 0, sizeof(double) * block * n * n, st);
+  cudaMemsetAsync(d_J, 0, sizeof(double) * n * n, st);
   for (int J0 = 0; J0 < M; J0 += block) {
     const int nb = std::min(block, M - J0);
     // vectors J0.. may straddle storage blocks: gather into a contiguous view
@@ -246,7 +249,10 @@ __global__ void k_oz_lexp(const int* __restrict__ inv, int n, int64_t nrs, const
   const double* LJ = L + nrs * J;
   double m = 0.0;
   if (a < n)
-    for (int b = lane; b < n; b += 32) m = fmax(m, fabs(LJ[inv[(size_t)a * n + b]]));
+    for (int b = lane; b < n; b += 32) {
+      const int t = inv[(size_t)a * n + b];  // -1: not stored (zero)
+      if (t >= 0) m = fmax(m, fabs(LJ[t]));
+    }
   m = warp_max(m);
   if (lane == 0) eL[row] = (short)max(-32000, oz_exponent(m));
 }
@@ -304,7 +310,8 @@ __global__ void __launch_bounds__(kOzChunk) k_oz_slice_l_blocks(const int64_t* _
         const int pair = Jp < I ? I * (I + 1) / 2 + Jp : trib + I;
         const int hi = la >= lb ? la : lb, lo = la >= lb ? lb : la;
         const int off = Jp < I ? la + rnA[r] * lb : (Jp > I ? lb + nB * la : hi * (hi + 1) / 2 + lo);
-        x[r] = __ldg(LJ + (int)__ldg(sp_first + pair) + off);
+        const int base = (int)__ldg(sp_first + pair);  // -1: a shell pair without rows (screened out)
+        x[r] = base >= 0 ? __ldg(LJ + base + off) : 0.0;
       }
     }
   } else {
@@ -452,7 +459,8 @@ __global__ void k_jacc64(const double* __restrict__ L, int64_t nrs, int nb, cons
   jrs[t] += s;
 }
 
-// inv[a*n + b] = inv[b*n + a] = t for every rs pair t
+// inv[a*n + b] = inv[b*n + a] = t for every rs pair t (the caller fills inv
+// with -1 first: AO pairs of shell pairs without rows keep it)
 __global__ void k_rs_inverse(const int* __restrict__ rs_a, const int* __restrict__ rs_b, int64_t nrs, int n,
                              int* __restrict__ inv) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -657,6 +665,7 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
     h->err = std::string("mixed J/K: after the density product: ") + cudaGetErrorString(e);
     return MG_ERR_CUDA;
   }
+  cudaMemsetAsync(inv, 0xFF, 4 * nn, st);
   k_rs_inverse<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, n, inv);
   if (!launched("k_rs_inverse")) return MG_ERR_CUDA;
   const short* eL = oz_row_exponents(h, inv, ld, st);
@@ -710,6 +719,7 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   }
   k_symmetrize_lower<<<nb256((int64_t)nn), 256, 0, st>>>(d_K, n);
   if (!launched("k_symmetrize_lower")) return MG_ERR_CUDA;
+  cudaMemsetAsync(d_J, 0, 8 * nn, st);  // AO pairs without rows
   k_unpack_sym<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, jrs, n, d_J);
   if (!launched("k_unpack_sym")) return MG_ERR_CUDA;
   if (const cudaError_t e = cudaGetLastError(); e != cudaSuccess) {

@@ -46,6 +46,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <memory>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -463,8 +464,10 @@ void eri_quartet(const Basis& bs, int iS, int jS, int kS, int lS, double* out, b
 // the reference: for each component the nBas contracted functions follow).
 inline int ao_index(const Shell& s, int k, int m) { return s.off + m * s.nc + k; }
 
+struct RSList;
 struct Handle {
   Basis bs;
+  std::shared_ptr<RSList> rs;  // the rs list of the last decomposition (or of rs_compact); null: every pair
 };
 
 std::vector<int> quartet_dims(const Basis& bs, int i, int j, int k, int l) {
@@ -544,7 +547,9 @@ struct RSList {
   std::vector<int> sp_i, sp_j;    // shells of each pair
   std::vector<int> sp_first, sp_count;
 };
-RSList make_rs(const Basis& bs) {
+// keep: the shell pairs that carry rows (null: all); the others keep their
+// pair id with sp_first = -1 and no rows.
+RSList make_rs(const Basis& bs, const std::vector<char>* keep = nullptr) {
   RSList R;
   int ns = bs.sh.size();
   for (int i = 0; i < ns; ++i)
@@ -552,6 +557,11 @@ RSList make_rs(const Basis& bs) {
       int id = R.sp_i.size();
       R.sp_i.push_back(i);
       R.sp_j.push_back(j);
+      if (keep && !(*keep)[id]) {
+        R.sp_first.push_back(-1);
+        R.sp_count.push_back(0);
+        continue;
+      }
       R.sp_first.push_back(R.a.size());
       const Shell &A = bs.sh[i], &B = bs.sh[j];
       int nA = A.nc * nsph(A.l), nB = B.nc * nsph(B.l);
@@ -690,9 +700,8 @@ struct ChoResult {
   int irc = 0;
 };
 
-ChoResult cho_decompose(const Basis& bs, const ChoCfg& cfg, const std::vector<double>& diag0) {
+ChoResult cho_decompose(const Basis& bs, const ChoCfg& cfg, const std::vector<double>& diag0, const RSList& R) {
   ChoResult res;
-  RSList R = make_rs(bs);
   size_t nrs = R.a.size();
   std::vector<double> diag = diag0;
   // initial screening (cho_calcdiag.F90:255-300)
@@ -868,6 +877,7 @@ std::vector<double> eri_diag(const Basis& bs, const RSList& R) {
   int nsp = R.sp_i.size();
 #pragma omp parallel for schedule(dynamic)
   for (int sp = 0; sp < nsp; ++sp) {
+    if (R.sp_count[sp] == 0) continue;  // a screened-out pair: no rows
     int i = R.sp_i[sp], j = R.sp_j[sp];
     std::vector<double> blk(quartet_size(bs, i, j, i, j));
     eri_quartet(bs, i, j, i, j, blk.data());
@@ -1102,18 +1112,49 @@ int or_eri_full(void* h, double cutint, double* full) {
   return 0;
 }
 
+// The rs list in use: the one of the handle's last decomposition (or of
+// or_rs_compact), else every AO pair.
+static RSList cur_rs(Handle* h) { return h->rs ? *h->rs : make_rs(h->bs); }
+
+// Initial screening of the decomposition (cho_calcdiag.F90:255-300): elements
+// with diag < ScrMax = ThrCom^2 / (Damp DiaMax) leave the reduced set; the
+// vectors are stored over the shell pairs that keep at least one element.
+static RSList screened_rs(const Basis& bs, double thrcom, double damp, std::vector<double>* diag_out) {
+  RSList F = make_rs(bs);
+  std::vector<double> d = eri_diag(bs, F);
+  double dm = 0.0;
+  for (double v : d) dm = std::max(dm, std::fabs(v));
+  const double scrmax = dm > 0 ? thrcom * thrcom / damp / dm : 1e15;
+  std::vector<char> keep(F.sp_i.size(), 0);
+  for (size_t t = 0; t < d.size(); ++t)
+    if (!(d[t] < scrmax)) keep[F.sp[t]] = 1;
+  RSList R = make_rs(bs, &keep);
+  if (diag_out) {
+    diag_out->clear();
+    for (size_t t = 0; t < d.size(); ++t)
+      if (keep[F.sp[t]]) diag_out->push_back(d[t]);
+  }
+  return R;
+}
+
 // ERI diagonal over the rs list; returns nrs (fills a,b,sp if non-null)
-int64_t or_rs_count(void* h) { return make_rs(((Handle*)h)->bs).a.size(); }
+int64_t or_rs_count(void* h) { return cur_rs((Handle*)h).a.size(); }
 int or_rs_list(void* h, int* a, int* b, int* sp) {
-  RSList R = make_rs(((Handle*)h)->bs);
+  RSList R = cur_rs((Handle*)h);
   for (size_t t = 0; t < R.a.size(); ++t) { a[t] = R.a[t]; b[t] = R.b[t]; sp[t] = R.sp[t]; }
   return 0;
 }
 int or_eri_diag(void* h, double* d) {
   Basis& bs = ((Handle*)h)->bs;
-  RSList R = make_rs(bs);
+  RSList R = cur_rs((Handle*)h);
   auto v = eri_diag(bs, R);
   std::copy(v.begin(), v.end(), d);
+  return 0;
+}
+// the rs list a decomposition at thrcom would store its vectors over (no decomposition)
+int or_rs_compact(void* h, double thrcom) {
+  Handle* H = (Handle*)h;
+  H->rs = std::make_shared<RSList>(screened_rs(H->bs, thrcom, cho_default_damp(thrcom), nullptr));
   return 0;
 }
 
@@ -1135,9 +1176,10 @@ int or_cholesky_x(void* h, double thrcom, double span, int minqual, int maxqual,
   cfg.ialqua = ialqua;
   cfg.damp1 = cfg.damp2 = cho_default_damp(thrcom);
   cfg.thrneg = -1e-40; cfg.warneg = -1e-10; cfg.tooneg = -1e-8;
-  RSList R = make_rs(bs);
-  auto d = eri_diag(bs, R);
-  ChoResult res = cho_decompose(bs, cfg, d);
+  std::vector<double> d;
+  RSList R = screened_rs(bs, thrcom, cfg.damp1, &d);
+  ((Handle*)h)->rs = std::make_shared<RSList>(R);
+  ChoResult res = cho_decompose(bs, cfg, d, R);
   if (res.irc) return res.irc;
   if (res.M > maxvec) return 102;
   *M_out = res.M;
@@ -1166,7 +1208,7 @@ static inline double dot_simd(const double* __restrict__ x, const double* __rest
 
 int or_cho_jk(void* h, const double* L, int M, const double* C, int r, double* J, double* K) {
   Basis& bs = ((Handle*)h)->bs;
-  RSList R = make_rs(bs);
+  RSList R = cur_rs((Handle*)h);
   const size_t nrs = R.a.size();
   const int n = bs.nbf;
   std::vector<double> D((size_t)n * n, 0.0), Ct((size_t)n * r);

@@ -45,6 +45,7 @@ def lib():
         L.or_rs_count.restype = C.c_int64
         L.or_rs_count.argtypes = [vp]
         L.or_rs_list.argtypes = [vp, i, i, i]
+        L.or_rs_compact.argtypes = [vp, C.c_double]
         L.or_eri_diag.argtypes = [vp, d]
         L.or_cholesky.argtypes = [vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, i, i, i, d, i]
         L.or_cholesky_x.argtypes = [vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, i, i, i,
@@ -130,7 +131,15 @@ class Oracle:
         lib().or_eri_full(self.h, cutint, _p(out))
         return out.reshape(n, n, n, n)
 
+    def rs_compact(self, thrcom):
+        """Make the rs list the one a decomposition at thrcom stores its vectors
+        over (the shell pairs that survive the initial screening), without
+        decomposing.  A decomposition sets it as well; before either, the rs
+        list holds every AO pair."""
+        lib().or_rs_compact(self.h, thrcom)
+
     def rs_list(self):
+        """The rs list in use (AO indices a >= b within each shell pair, shell-pair id)."""
         n = lib().or_rs_count(self.h)
         a = np.empty(n, np.int32)
         b = np.empty(n, np.int32)
