@@ -113,7 +113,11 @@ int mg_eri_quartets_noalloc(mg_handle* h, const int32_t* quartets, int64_t nq, c
  * cho_drv_inner.F90:14, cho_decom_a4.F90:12).  Vectors stay on the device
  * inside the handle, FP64, in reduced-set layout: AO pairs a>=b grouped by
  * shell pair (i>=j in iTri order); inside a pair a fastest (i>j) or iTri
- * (i==j) (cholesky_util/plf_cho_diag.F90:60-72).
+ * (i==j) (cholesky_util/plf_cho_diag.F90:60-72).  Only the shell pairs with
+ * at least one element that survives the initial screening of the diagonal
+ * (diag >= ThrCom^2 / (Damp DiaMax), cho_calcdiag.F90:255-300) have rows
+ * (their count is nrs of mg_cho_info; mg_cho_rs_list lists them); the
+ * vectors are zero on the other AO pairs.
  */
 typedef struct mg_cho_cfg {
   double thrcom; /* decomposition threshold ThrCom (cholesky.F90:128, 1e-4) */

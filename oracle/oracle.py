@@ -157,7 +157,7 @@ class Oracle:
         """Pivoted Cholesky decomposition.  mxshpr/ialqua: shell pairs per pass
         and qualification algorithm; (1, 2) is the reference's default for
         algorithm 4 and what the device decomposition implements."""
-        nrs = lib().or_rs_count(self.h)
+        nrs = self.nbf * (self.nbf + 1) // 2  # every AO pair: the bound of the decomposition's rs list
         if maxvec is None:
             maxvec = min(nrs, 20 * self.nbf)
         L = np.zeros(nrs * maxvec)
@@ -170,6 +170,7 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(f"oracle cholesky failed rc={rc}")
         m = M.value
+        nrs = lib().or_rs_count(self.h)  # the decomposition's rs list (screened shell pairs have no rows)
         return dict(L=L[: nrs * m].reshape(m, nrs).T.copy(), piv=piv[:m].copy(), pass_of=pas[:m].copy(),
                     M=m, npass=npass.value)
 

@@ -7,8 +7,9 @@ tens of minutes, which is why it is stored).
 
 Workload: the 40-atom slice of the 1500-function mix that the J/K tests and
 `bench.py --leg jk --natom 40` use (3s2p1d and 2s1p atoms, seed 3).  Stored:
-the pivots (rs index of each vector's pivot), the pass of each vector, the
-vector and pass counts, and every vector's sum of squares.
+the pivots as AO index pairs (a >= b; independent of the rs numbering), the
+pass of each vector, the vector and pass counts, and every vector's sum of
+squares.
 
     python tests/golden/make_cho_jk40_golden.py
 """
@@ -43,9 +44,11 @@ def main():
     t0 = time.time()
     ref = o.cholesky(thrcom=THRCOM, maxvec=4000)
     L = ref["L"]
+    a, b, _ = o.rs_list()  # the rs list of this decomposition
     print(f"oracle Cholesky of jk40 ({mol.nbf} functions) at ThrCom {THRCOM}: M = {ref['M']}, "
           f"{ref['npass']} passes, {time.time() - t0:.1f} s on {O.num_threads()} threads")
-    np.savez(os.path.join(HERE, "cho_jk40_oracle.npz"), thrcom=THRCOM, nbf=mol.nbf, piv=ref["piv"],
+    np.savez(os.path.join(HERE, "cho_jk40_oracle.npz"), thrcom=THRCOM, nbf=mol.nbf, piv_a=a[ref["piv"]],
+             piv_b=b[ref["piv"]],
              pass_of=ref["pass_of"], M=ref["M"], npass=ref["npass"], norm2=(L * L).sum(0))
 
 
