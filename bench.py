@@ -633,8 +633,9 @@ def run_leg(args):
 def run_c5(timed):
     """The full-scale system (250 seeded atoms, 2s1p / 3s2p1d / 4s3p2d1f, 1815
     functions): the ERI Cholesky decomposition at ThrCom 1e-6, then J/K of 8
-    random densities of uneven rank (50..300) through the mixed and the FP64
-    path, each with its energy difference; the CPU restatement of the J/K
+    random densities of uneven rank (50..300) in one batch through the mixed
+    and the FP64 path, each density with its energy difference; the CPU
+    restatement of the J/K
     (CHO_LK_SCF through BLAS) timed on a sample of the vectors for every
     density and scaled to all of them.  The gradient of this system is not
     run (about 10^3 s per density at the measured C4 rate).  One JSON line."""
@@ -649,19 +650,21 @@ def run_c5(timed):
     torch.cuda.synchronize()
     t_cd = time.time() - t0
     ranks = [int(round(r)) for r in np.linspace(50, 300, 8)]
-    dens = []
-    for k, rk in enumerate(ranks):
-        Cd = torch.from_numpy(B.density_factor(m.nbf, rk, 5 + k)).cuda()
-        D = Cd @ Cd.t()
-        row = {"rank": rk}
-        for name, prec in (("mixed", MolGpu.PREC_MIXED), ("fp64", MolGpu.PREC_FP64)):
-            g.cho_jk(Cd, precision=prec)  # untimed first call (row exponents, workspace)
-            torch.cuda.synchronize()
-            (J, K), ms = timed(lambda: g.cho_jk(Cd, precision=prec))
-            row[name + "_s"] = ms[-1] / 1e3
+    Cds = [torch.from_numpy(B.density_factor(m.nbf, rk, 5 + k)).cuda() for k, rk in enumerate(ranks)]
+    dens = [{"rank": rk} for rk in ranks]
+    times = {}
+    for name, prec in (("mixed", MolGpu.PREC_MIXED), ("fp64", MolGpu.PREC_FP64)):
+        # the 8 densities in one batch (every block of vectors unpacked once), after an untimed call
+        g.cho_jk_batch(Cds, precision=prec)
+        torch.cuda.synchronize()
+        res, ms = timed(lambda: g.cho_jk_batch(Cds, precision=prec))
+        times[name] = ms[-1] / 1e3
+        for row, Cd, (J, K) in zip(dens, Cds, res):
+            D = Cd @ Cd.t()
             row["E_" + name] = float(0.5 * (D * J).sum() - 0.25 * (D * K).sum())
+        del res
+    for row in dens:
         row["dE"] = row["E_mixed"] - row["E_fp64"]
-        dens.append(row)
     del g
     torch.cuda.empty_cache()
     # CPU restatement on a sample of the vectors (the cost does not depend on their values)
@@ -678,8 +681,7 @@ def run_c5(timed):
         t0 = time.time()
         O.cho_jk_blas(rs_a, rs_b, m.nbf, L, Cm)
         cpu += (time.time() - t0) * info["M"] / nv
-    mixed = sum(r["mixed_s"] for r in dens)
-    fp64 = sum(r["fp64_s"] for r in dens)
+    mixed, fp64 = times["mixed"], times["fp64"]
     print(json.dumps({"workload": f"c5: 250 atoms, {m.nbf} bf, ThrCom {THRCOM}, 8 densities of rank {ranks}",
                       "cholesky": {"seconds": t_cd, "M": info["M"], "npass": info["npass"]},
                       "jk_mixed_s": mixed, "jk_fp64_s": fp64, "speedup": fp64 / mixed,

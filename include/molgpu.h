@@ -210,6 +210,15 @@ double mg_drvg1_flops(mg_handle* h, double cutint);
  */
 int mg_rys_roots(mg_handle* h, int nrys, int64_t n, const double* T, double* x, double* w);
 
+/* CHO_LK_SCF for ndens (1..8) densities at once (the several densities of
+ * choscf_drv.F90's calls, e.g. alpha and beta, or a batch of states): the
+ * same as ndens calls of mg_cho_jk, but every block of vectors is unpacked
+ * once for all of them.  d_C[i] (nbf x r[i]), d_J[i], d_K[i]: device
+ * pointers, in host arrays of length ndens.  Synchronous (mixed) or queued
+ * on the stream (FP64), as mg_cho_jk. */
+int mg_cho_jk_batch(mg_handle* h, int ndens, const double* const* d_C, const int* r, double* const* d_J,
+                    double* const* d_K, int precision, void* stream);
+
 /* CD_InCore (cholesky_util/cd_incore.F90:14, cd_incore_1.F90): pivoted
  * Cholesky vectors of a symmetric positive semidefinite n x n matrix X
  * (column-major, device memory, overwritten): d_vec (n x maxvec,

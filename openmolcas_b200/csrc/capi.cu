@@ -532,6 +532,21 @@ int mg_cho_jk(mg_handle* H, const double* d_C, int r, double* d_J, double* d_K, 
   return MG_ERR_ARG;
 }
 
+int mg_cho_jk_batch(mg_handle* H, int ndens, const double* const* d_C, const int* r, double* const* d_J,
+                    double* const* d_K, int precision, void* stream) {
+  if (!H || ndens < 1 || ndens > 8 || !d_C || !r || !d_J || !d_K) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  if (!h->cho) { h->err = "mg_cho_jk_batch: no Cholesky vectors (call mg_cho_drv)"; return MG_ERR_ARG; }
+  cudaSetDevice(h->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == MG_PREC_FP64) return jk_fp64_batch(h, ndens, d_C, r, d_J, d_K, st, 32);
+  if (precision == MG_PREC_MIXED) return jk_mixed_batch(h, ndens, d_C, r, d_J, d_K, st, 64, MG_JK_SLICES, MG_JK_SLICES_K);
+  if (precision > 100 && precision <= 108)
+    return jk_mixed_batch(h, ndens, d_C, r, d_J, d_K, st, 64, precision - 100, precision - 100);
+  h->err = "mg_cho_jk_batch: unsupported precision";
+  return MG_ERR_ARG;
+}
+
 int mg_cho_lk_scf(mg_handle* H, const double* d_C, int r, double factxi, double* d_FLT, int precision,
                   void* stream) {
   if (!H || !d_C || !d_FLT || r < 1) return MG_ERR_ARG;

@@ -101,54 +101,73 @@ struct JkWork {
 };
 
 int jk_fp64(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block) {
+  return jk_fp64_batch(h, 1, &d_C, &r, &d_J, &d_K, st, block);
+}
+
+// FP64 J/K of k densities: every block of vectors is unpacked once, each
+// density runs its DGEMVs, half-transform and DSYRK on the squares.
+int jk_fp64_batch(Handle* h, int k, const double* const* Cs, const int* rs_, double* const* Js, double* const* Ks,
+                  cudaStream_t st, int block) {
   ChoState* c = h->cho;
   const int64_t nrs = cho_nrs(c);
   const int M = cho_nvec(c);
   const int n = h->nbf;
+  if (k < 1) { h->err = "FP64 J/K: no density"; return MG_ERR_ARG; }
+  int rmax = 0;
+  for (int d = 0; d < k; ++d) {
+    if (!Cs[d] || !Js[d] || !Ks[d] || rs_[d] < 1) { h->err = "FP64 J/K: a density of the batch has no factor or outputs"; return MG_ERR_ARG; }
+    rmax = std::max(rmax, rs_[d]);
+  }
   cublasHandle_t cb = cho_cublas(c);
   cublasSetStream(cb, st);
   const int* d_ra = cho_rs_a_dev(c);
   const int* d_rb = cho_rs_b_dev(c);
-  // scratch: dw (nrs), V (block), jrs (nrs), D (n*n), Lsq (block*n*n), X (n * block * r)
-  const size_t need = sizeof(double) * ((size_t)nrs * 2 + block + (size_t)n * n + (size_t)block * n * n +
-                                        (size_t)n * block * r);
+  // scratch: dw (k nrs), jrs (k nrs), V (block), D (n*n), Lsq (block*n*n), X (n * block * rmax)
+  const size_t need = sizeof(double) * ((size_t)nrs * 2 * k + block + (size_t)n * n + (size_t)block * n * n +
+                                        (size_t)n * block * rmax);
   double* ws = (double*)ws_get(h, need, st);
   if (!ws) { h->err = "jk workspace allocation failed"; return MG_ERR_MEMORY; }
   double* dw = ws;
-  double* jrs = dw + nrs;
-  double* V = jrs + nrs;
+  double* jrs = dw + (size_t)nrs * k;
+  double* V = jrs + (size_t)nrs * k;
   double* D = V + block;
   double* Lsq = D + (size_t)n * n;
   double* X = Lsq + (size_t)block * n * n;
   const double one = 1.0, zero = 0.0;
-  // D = C C^T  (C column-major n x r); D symmetric so layout-agnostic
-  cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, r, &one, d_C, n, d_C, n, &zero, D, n);
-  k_pack_density<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, D, n, dw);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
-  cudaMemsetAsync(jrs, 0, sizeof(double) * nrs, st);
-  cudaMemsetAsync(d_K, 0, sizeof(double) * n * n, st);
+  for (int d = 0; d < k; ++d) {
+    // D = C C^T  (C column-major n x r); D symmetric so layout-agnostic
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, rs_[d], &one, Cs[d], n, Cs[d], n, &zero, D, n);
+    k_pack_density<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, D, n, dw + (size_t)d * nrs);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    cudaMemsetAsync(Ks[d], 0, sizeof(double) * n * n, st);
+    cudaMemsetAsync(Js[d], 0, sizeof(double) * n * n, st);  // AO pairs without rows stay zero
+  }
+  cudaMemsetAsync(jrs, 0, sizeof(double) * nrs * k, st);
   // AO pairs without rows (screened-out shell pairs) stay zero in every square
   cudaMemsetAsync(Lsq, 0, sizeof(double) * block * n * n, st);
-  cudaMemsetAsync(d_J, 0, sizeof(double) * n * n, st);
   for (int J0 = 0; J0 < M; J0 += block) {
     const int nb = std::min(block, M - J0);
     // vectors J0.. may straddle storage blocks: gather into a contiguous view
     const double* Lb = cho_vec_ptr(c, J0, nb, st, h);
     if (!Lb) { h->err = "vector block gather failed"; return MG_ERR_MEMORY; }
-    // Coulomb: V = L_b^T dw ; jrs += L_b V
-    cublasDgemv(cb, CUBLAS_OP_T, (int)nrs, nb, &one, Lb, (int)nrs, dw, 1, &zero, V, 1);
-    cublasDgemv(cb, CUBLAS_OP_N, (int)nrs, nb, &one, Lb, (int)nrs, V, 1, &one, jrs, 1);
-    // Exchange: X_J = Lsq_J C (n x r each), K += X X^T
     k_unpack_block<<<nb256(nrs * nb), 256, 0, st>>>(d_ra, d_rb, nrs, Lb, nb, n, Lsq);
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    cublasDgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_N, n, r, n, &one, Lsq, n, (long long)n * n, d_C, n, 0, &zero,
-                              X, n, (long long)n * r, nb);
-    cublasDsyrk(cb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, nb * r, &one, X, n, &one, d_K, n);
+    for (int d = 0; d < k; ++d) {
+      // Coulomb: V = L_b^T dw ; jrs += L_b V
+      cublasDgemv(cb, CUBLAS_OP_T, (int)nrs, nb, &one, Lb, (int)nrs, dw + (size_t)d * nrs, 1, &zero, V, 1);
+      cublasDgemv(cb, CUBLAS_OP_N, (int)nrs, nb, &one, Lb, (int)nrs, V, 1, &one, jrs + (size_t)d * nrs, 1);
+      // Exchange: X_J = Lsq_J C (n x r each), K += X X^T
+      cublasDgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_N, n, rs_[d], n, &one, Lsq, n, (long long)n * n, Cs[d], n,
+                                0, &zero, X, n, (long long)n * rs_[d], nb);
+      cublasDsyrk(cb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, nb * rs_[d], &one, X, n, &one, Ks[d], n);
+    }
   }
-  k_unpack_sym<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, jrs, n, d_J);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_symmetrize_lower<<<nb256((int64_t)n * n), 256, 0, st>>>(d_K, n);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
+  for (int d = 0; d < k; ++d) {
+    k_unpack_sym<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, jrs + (size_t)d * nrs, n, Js[d]);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    k_symmetrize_lower<<<nb256((int64_t)n * n), 256, 0, st>>>(Ks[d], n);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : MG_ERR_CUDA;
 }
 
@@ -459,6 +478,59 @@ __global__ void k_jacc64(const double* __restrict__ L, int64_t nrs, int nb, cons
   jrs[t] += s;
 }
 
+// Coulomb contractions of a batch's further densities (the first one's are
+// formed by the L unpacking): V[d nb + J] = sum_t L[t, J] dw_d[t] for
+// d = 1 .. kd, dw_d = dws + (d - 1) nrs the packed weighted density
+// (k_pack_density).  One CTA per vector J, each vector element read once.
+constexpr int kJkMaxDens = 8;
+
+__global__ void __launch_bounds__(256) k_vmulti(const double* __restrict__ L, int64_t nrs, int nb, int kd,
+                                                const double* __restrict__ dws, double* __restrict__ V) {
+  __shared__ double red[kJkMaxDens][8];
+  const int J = blockIdx.x;
+  const double* LJ = L + nrs * J;
+  double acc[kJkMaxDens - 1];
+#pragma unroll
+  for (int d = 0; d < kJkMaxDens - 1; ++d) acc[d] = 0.0;
+  for (int64_t t = threadIdx.x; t < nrs; t += blockDim.x) {
+    const double x = __ldg(LJ + t);
+#pragma unroll
+    for (int d = 0; d < kJkMaxDens - 1; ++d)
+      if (d < kd) acc[d] = fma(x, __ldg(dws + (size_t)d * nrs + t), acc[d]);
+  }
+#pragma unroll
+  for (int d = 0; d < kJkMaxDens - 1; ++d) {
+    const double v = warp_sum(acc[d]);
+    if ((threadIdx.x & 31) == 0) red[d][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < kd) {
+    double v = 0.0;
+    for (int w = 0; w < 8; ++w) v += red[threadIdx.x][w];
+    V[(size_t)(threadIdx.x + 1) * nb + J] = v;
+  }
+}
+
+// jrs_d[t] += sum_J L[t, J] V[d nb + J] for the k densities of a batch,
+// each vector element read once (k_jacc64 for one density)
+__global__ void k_jacc_multi(const double* __restrict__ L, int64_t nrs, int nv, int nb, int k,
+                             const double* __restrict__ V, double* __restrict__ jrs) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nrs) return;
+  double acc[kJkMaxDens];
+#pragma unroll
+  for (int d = 0; d < kJkMaxDens; ++d) acc[d] = 0.0;
+  for (int J = 0; J < nv; ++J) {
+    const double x = L[t + nrs * J];
+#pragma unroll
+    for (int d = 0; d < kJkMaxDens; ++d)
+      if (d < k) acc[d] = fma(x, V[(size_t)d * nb + J], acc[d]);
+  }
+#pragma unroll
+  for (int d = 0; d < kJkMaxDens; ++d)
+    if (d < k) jrs[(size_t)d * nrs + t] += acc[d];
+}
+
 // inv[a*n + b] = inv[b*n + a] = t for every rs pair t (the caller fills inv
 // with -1 first: AO pairs of shell pairs without rows keep it)
 __global__ void k_rs_inverse(const int* __restrict__ rs_a, const int* __restrict__ rs_b, int64_t nrs, int n,
@@ -547,8 +619,37 @@ static const short* oz_row_exponents(Handle* h, const int* inv, int ld, cudaStre
   return e;
 }
 
+// Per-density state of a mixed J/K batch.
+struct OzDens {
+  const double* C;
+  int r;
+  double* J;
+  double* K;
+  int nnt, Nt, npad, kx, kblk, nsub, ksub;
+  int64_t xs_row;
+  double* jrs;           // Coulomb in rs layout
+  double* dw;            // packed weighted density (densities after the first)
+  uint8_t* CS;           // slices of C
+  double* fC;            // column scale factors of C
+  uint8_t* XS;           // slices of X for one group of blocks
+  int* eX;               // their row exponents
+  CUtensorMap map_c, map_x;
+  OzArgs ax, ak;
+};
+
 int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block, int s,
              int sk) {
+  return jk_mixed_batch(h, 1, &d_C, &r, &d_J, &d_K, st, block, s, sk);
+}
+
+// J/K of k densities over one pass of the vectors: every block of vectors is
+// unpacked and sliced once (with the first density's Coulomb contraction
+// fused), the further densities' contractions take one more read of the
+// block (k_vmulti), J accumulates for all densities in one read
+// (k_jacc_multi), and each density runs its half-transform, X slicing and
+// exchange product on the shared slices.
+int jk_mixed_batch(Handle* h, int k, const double* const* Cs, const int* rs_, double* const* Js, double* const* Ks,
+                   cudaStream_t st, int block, int s, int sk) {
   ChoState* c = h->cho;
   const int64_t nrs = cho_nrs(c);
   const int M = cho_nvec(c);
@@ -557,23 +658,41 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
     h->err = "mixed J/K: slices must be 2..8";
     return MG_ERR_ARG;
   }
+  if (k < 1 || k > kJkMaxDens) {
+    h->err = "mixed J/K: 1..8 densities per batch";
+    return MG_ERR_ARG;
+  }
   if (const cudaError_t e = cudaGetLastError(); e != cudaSuccess) {
     h->err = std::string("mixed J/K: error pending from earlier work: ") + cudaGetErrorString(e);
     return MG_ERR_CUDA;
   }
   const int ld = rup(n, 128);
-  int nnt, Nt;
-  oz_col_tiles(r, s, nnt, Nt);
-  const int npad = nnt * Nt;
   // vectors per block: one block's K extent of the exchange product, nb r
   const int nb = std::min(block, M);
-  const int kx = nb * r;
-  const int kblk = rup(kx, 32);
-  const int nsub = (kblk + kOzKChunk - 1) / kOzKChunk;
-  const int ksub = rup((kblk + nsub - 1) / nsub, 32);
   const int nblocks = (M + nb - 1) / nb;
   const int G = std::min(16, nblocks);  // blocks per exchange-product group
   const int ntile = (ld / 128) * (ld / 128 + 1) / 2;
+  std::vector<OzDens> dd(k);
+  int kxmax = 0;
+  for (int d = 0; d < k; ++d) {
+    OzDens& q = dd[d];
+    q.C = Cs[d];
+    q.r = rs_[d];
+    q.J = Js[d];
+    q.K = Ks[d];
+    if (!q.C || !q.J || !q.K || q.r < 1) {
+      h->err = "mixed J/K: a density of the batch has no factor or outputs";
+      return MG_ERR_ARG;
+    }
+    oz_col_tiles(q.r, s, q.nnt, q.Nt);
+    q.npad = q.nnt * q.Nt;
+    q.kx = nb * q.r;
+    q.kblk = rup(q.kx, 32);
+    q.nsub = (q.kblk + kOzKChunk - 1) / kOzKChunk;
+    q.ksub = rup((q.kblk + q.nsub - 1) / q.nsub, 32);
+    q.xs_row = (int64_t)G * q.kblk;
+    kxmax = std::max(kxmax, q.kx);
+  }
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
   cublasHandle_t cb = cho_cublas(c);
@@ -581,31 +700,42 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   const int* d_ra = cho_rs_a_dev(c);
   const int* d_rb = cho_rs_b_dev(c);
   const size_t nn = (size_t)n * n;
-  const int64_t xs_row = (int64_t)G * kblk;
   const int ns = (int)h->sh.size();
-  // one term per take() below (each rounded up to 256 bytes: 15 takes)
-  size_t need = 8 * (nrs + (size_t)nb + nn) + 4 * nn + (size_t)s * npad * ld + 8 * (size_t)npad +
-                (size_t)s * nb * ld * ld + 4 * (size_t)nb * ld + 8 * (size_t)ld * kx + 8 * (size_t)ld +
-                (size_t)sk * ld * xs_row + 4 * (size_t)G * ld + 8 * (size_t)nsm * 128 * 128 + sizeof(int) +
-                4 * (size_t)(ns + 1 + n) + 15 * 256;
+  // one term per take() below (each rounded up to 256 bytes)
+  size_t need = 8 * ((size_t)nb * k + 2 * nn) + 4 * nn + (size_t)s * nb * ld * ld + 4 * (size_t)nb * ld +
+                8 * (size_t)ld * kxmax + 8 * (size_t)ld + 8 * (size_t)nsm * 128 * 128 + sizeof(int) +
+                4 * (size_t)(ns + 1 + n) + 11 * 256;
+  for (const OzDens& q : dd)
+    need += 16 * (size_t)nrs + (size_t)s * q.npad * ld + 8 * (size_t)q.npad + (size_t)sk * ld * q.xs_row +
+            4 * (size_t)G * ld + 6 * 256;
   char* ws = (char*)ws_get(h, need, st);
   if (!ws) { h->err = "jk workspace allocation failed"; return MG_ERR_MEMORY; }
   char* const ws_end = ws + need;
   auto take = [&](size_t bytes) { char* p = ws; ws += (bytes + 255) & ~(size_t)255; return (void*)p; };
-  double* jrs = (double*)take(8 * nrs);
-  double* V = (double*)take(8 * (size_t)nb);
-  double* D = (double*)take(8 * nn);
+  double* V = (double*)take(8 * (size_t)nb * k);  // V[d nb + J]
+  double* D = (double*)take(8 * nn);               // D of the first density (its contraction is fused)
+  double* Dt = (double*)take(8 * nn);              // D of a further density, while it is packed
   int* inv = (int*)take(4 * nn);
-  uint8_t* CS = (uint8_t*)take((size_t)s * npad * ld);
-  double* fC = (double*)take(8 * (size_t)npad);
   uint8_t* LS = (uint8_t*)take((size_t)s * nb * ld * ld);
   int* eA = (int*)take(4 * (size_t)nb * ld);
-  double* Xf = (double*)take(8 * (size_t)ld * kx);  // column-major, ld rows
+  double* Xf = (double*)take(8 * (size_t)ld * kxmax);  // column-major, ld rows
   unsigned long long* xmax = (unsigned long long*)take(8 * (size_t)ld);
-  uint8_t* XS = (uint8_t*)take((size_t)sk * ld * xs_row);
-  int* eX = (int*)take(4 * (size_t)G * ld);
   double* P = (double*)take(8 * (size_t)nsm * 128 * 128);
   int* d_err = (int*)take(sizeof(int));
+  int* sh_off = (int*)take(4 * (size_t)(ns + 1 + n));
+  int* ao_sh = sh_off + ns + 1;
+  double* jrs_all = (double*)take(8 * (size_t)nrs * k);  // jrs of density d at d nrs
+  double* dws = (double*)take(8 * (size_t)nrs * std::max(1, k - 1));
+  for (int d = 0; d < k; ++d) {
+    OzDens& q = dd[d];
+    q.jrs = jrs_all + (size_t)d * nrs;
+    q.dw = d > 0 ? dws + (size_t)(d - 1) * nrs : nullptr;
+    q.CS = (uint8_t*)take((size_t)s * q.npad * ld);
+    q.fC = (double*)take(8 * (size_t)q.npad);
+    q.XS = (uint8_t*)take((size_t)sk * ld * q.xs_row);
+    q.eX = (int*)take(4 * (size_t)G * ld);
+  }
+  if (ws > ws_end) { h->err = "mixed J/K: workspace layout exceeds its size"; return MG_ERR_CUDA; }
   // every launch is checked at once, so that an error names its kernel
   auto launched = [&](const char* what) {
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -614,9 +744,6 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
     h->err = std::string("mixed J/K: ") + what + ": " + cudaGetErrorString(e);
     return false;
   };
-  int* sh_off = (int*)take(4 * (size_t)(ns + 1 + n));
-  int* ao_sh = sh_off + ns + 1;
-  if (ws > ws_end) { h->err = "mixed J/K: workspace layout exceeds its size"; return MG_ERR_CUDA; }
   std::vector<int> hoff(ns + 1 + n);
   for (int i = 0; i < ns; ++i) {
     hoff[i] = h->sh[i].off;
@@ -628,16 +755,16 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
     h->err = std::string("mixed J/K: shell table upload: ") + cudaGetErrorString(e);
     return MG_ERR_CUDA;
   }
-  CUtensorMap map_l, map_c, map_x;
-  if (!make_slice_map(&map_l, LS, ld, (int64_t)nb * ld, s, 128) || !make_slice_map(&map_c, CS, ld, npad, s, Nt) ||
-      !make_slice_map(&map_x, XS, xs_row, ld, sk, 128)) {
+  CUtensorMap map_l;
+  if (!make_slice_map(&map_l, LS, ld, (int64_t)nb * ld, s, 128)) {
     h->err = "tensor maps for the exchange GEMMs could not be encoded";
     return MG_ERR_CUDA;
   }
-  OzArgs ax{}, ak{};
-  oz_plan(ax, s, Nt);
-  oz_plan(ak, sk, 128);
-  if (ax.stages < 2 || ak.stages < 2) { h->err = "mixed J/K: slice tiles do not fit in shared memory"; return MG_ERR_ARG; }
+  for (OzDens& q : dd)
+    if (!make_slice_map(&q.map_c, q.CS, ld, q.npad, s, q.Nt) || !make_slice_map(&q.map_x, q.XS, q.xs_row, ld, sk, 128)) {
+      h->err = "tensor maps for the exchange GEMMs could not be encoded";
+      return MG_ERR_CUDA;
+    }
   bool attr = true;
   oz_with_slices(s, [&](auto S) { attr &= smem_attr_once((const void*)oz_gemm_kernel<false, decltype(S)::value>, kOzSmemLimit); });
   oz_with_slices(sk, [&](auto S) { attr &= smem_attr_once((const void*)oz_gemm_kernel<true, decltype(S)::value>, kOzSmemLimit); });
@@ -645,24 +772,46 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
     h->err = "exchange GEMMs: shared-memory limit could not be raised";
     return MG_ERR_CUDA;
   }
-  ax.err = ak.err = d_err;
-  ax.nrt = ld / 128; ax.nnt = nnt; ax.ld = ld; ax.n = n; ax.r = r; ax.eA = eA; ax.fB = fC; ax.X = Xf; ax.xld = ld;
-  ax.xmax = xmax;
-  ak.ld = ld; ak.n = n; ak.ntile = ntile; ak.nsub = nsub; ak.kblk = kblk; ak.ksub = ksub; ak.eX = eX; ak.P = P;
-  ak.K = d_K;
+  for (OzDens& q : dd) {
+    OzArgs& ax = q.ax;
+    OzArgs& ak = q.ak;
+    ax = OzArgs{};
+    ak = OzArgs{};
+    oz_plan(ax, s, q.Nt);
+    oz_plan(ak, sk, 128);
+    if (ax.stages < 2 || ak.stages < 2) { h->err = "mixed J/K: slice tiles do not fit in shared memory"; return MG_ERR_ARG; }
+    ax.err = ak.err = d_err;
+    ax.nrt = ld / 128; ax.nnt = q.nnt; ax.ld = ld; ax.n = n; ax.r = q.r; ax.eA = eA; ax.fB = q.fC; ax.X = Xf;
+    ax.xld = ld; ax.xmax = xmax;
+    ak.ld = ld; ak.n = n; ak.ntile = ntile; ak.nsub = q.nsub; ak.kblk = q.kblk; ak.ksub = q.ksub; ak.eX = q.eX;
+    ak.P = P; ak.K = q.K;
+  }
   const double one = 1.0, zero = 0.0;
-  if (cudaMemsetAsync(d_err, 0, sizeof(int), st) != cudaSuccess || cudaMemsetAsync(jrs, 0, 8 * nrs, st) != cudaSuccess ||
-      cudaMemsetAsync(d_K, 0, 8 * nn, st) != cudaSuccess) {
+  if (cudaMemsetAsync(d_err, 0, sizeof(int), st) != cudaSuccess ||
+      cudaMemsetAsync(jrs_all, 0, 8 * nrs * k, st) != cudaSuccess) {
     h->err = std::string("mixed J/K: clearing buffers: ") + cudaGetErrorString(cudaGetLastError());
     return MG_ERR_CUDA;
   }
-  if (const cublasStatus_t bs = cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, r, &one, d_C, n, d_C, n, &zero, D, n);
-      bs != CUBLAS_STATUS_SUCCESS) {
-    h->err = "mixed J/K: density product (cublasDgemm) failed, status " + std::to_string((int)bs);
-    return MG_ERR_CUDA;
+  for (int d = 0; d < k; ++d) {
+    OzDens& q = dd[d];
+    if (cudaMemsetAsync(q.K, 0, 8 * nn, st) != cudaSuccess) {
+      h->err = std::string("mixed J/K: clearing K: ") + cudaGetErrorString(cudaGetLastError());
+      return MG_ERR_CUDA;
+    }
+    // D = C C^T: the first density's is read by the L unpacking, the others are packed over rs
+    double* Dd = d == 0 ? D : Dt;
+    if (const cublasStatus_t bs = cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, q.r, &one, q.C, n, q.C, n, &zero, Dd, n);
+        bs != CUBLAS_STATUS_SUCCESS) {
+      h->err = "mixed J/K: density product (cublasDgemm) failed, status " + std::to_string((int)bs);
+      return MG_ERR_CUDA;
+    }
+    if (d > 0) {
+      k_pack_density<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, Dt, n, q.dw);
+      if (!launched("k_pack_density")) return MG_ERR_CUDA;
+    }
   }
   if (const cudaError_t e = cudaGetLastError(); e != cudaSuccess) {
-    h->err = std::string("mixed J/K: after the density product: ") + cudaGetErrorString(e);
+    h->err = std::string("mixed J/K: after the density products: ") + cudaGetErrorString(e);
     return MG_ERR_CUDA;
   }
   cudaMemsetAsync(inv, 0xFF, 4 * nn, st);
@@ -670,10 +819,12 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
   if (!launched("k_rs_inverse")) return MG_ERR_CUDA;
   const short* eL = oz_row_exponents(h, inv, ld, st);
   if (!eL) { h->err = "mixed J/K: row exponents could not be stored"; return MG_ERR_MEMORY; }
-  oz_with_slices(s, [&](auto S) {
-    k_oz_slice_c<decltype(S)::value><<<(npad + 7) / 8, 256, 0, st>>>(d_C, n, r, npad, ld, Nt, CS, fC);
-  });
-  if (!launched("k_oz_slice_c")) return MG_ERR_CUDA;
+  for (OzDens& q : dd) {
+    oz_with_slices(s, [&](auto S) {
+      k_oz_slice_c<decltype(S)::value><<<(q.npad + 7) / 8, 256, 0, st>>>(q.C, n, q.r, q.npad, ld, q.Nt, q.CS, q.fC);
+    });
+    if (!launched("k_oz_slice_c")) return MG_ERR_CUDA;
+  }
   for (int g0 = 0; g0 < nblocks; g0 += G) {
     const int gn = std::min(G, nblocks - g0);
     for (int bi = 0; bi < gn; ++bi) {
@@ -681,10 +832,7 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
       const int nv = std::min(nb, M - J0);
       const double* Lb = cho_vec_ptr(c, J0, nv, st, h);
       if (!Lb) { h->err = "vector block straddles storage blocks"; return MG_ERR_ARG; }
-      // a short last block: clear the columns of the missing vectors
-      if (nv < nb) cudaMemsetAsync(Xf, 0, 8 * (size_t)ld * kx, st);
       cudaMemsetAsync(V, 0, 8 * (size_t)nb, st);
-      cudaMemsetAsync(xmax, 0, 8 * (size_t)ld, st);
       oz_with_slices(s, [&](auto S) {
         k_oz_slice_l_blocks<decltype(S)::value>
             <<<dim3((ld + kOzChunk - 1) / kOzChunk, ld / kOzRows, nv), kOzChunk, 0, st>>>(
@@ -692,36 +840,56 @@ int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cuda
                 LS, eA, V);
       });
       if (!launched("k_oz_slice_l_blocks")) return MG_ERR_CUDA;
-      k_jacc64<<<nb256(nrs), 256, 0, st>>>(Lb, nrs, nv, V, jrs);
-      if (!launched("k_jacc64")) return MG_ERR_CUDA;
-      // X_J = L_J C for the block (the slice map covers nb vectors; nv <= nb of them are used)
-      ax.nJ = nv;
-      ax.nitems = ax.nrt * nv * nnt;
-      const int gx = std::min(ax.nitems, nsm);
-      oz_with_slices(s, [&](auto S) {
-        oz_gemm_kernel<false, decltype(S)::value><<<gx, kOzThreads, ax.stages * ax.stage_bytes + 1024, st>>>(map_l, map_c, ax);
-      });
-      if (!launched("oz_gemm_kernel<false>")) return MG_ERR_CUDA;
-      oz_with_slices(sk, [&](auto S) {
-        k_oz_slice_x<decltype(S)::value><<<nb256((int64_t)ld * (kblk / 32)), 256, 0, st>>>(
-            Xf, ld, n, kx, ld, kblk, xs_row, (int64_t)bi * kblk, xmax, XS, eX + (size_t)bi * ld);
-      });
-      if (!launched("k_oz_slice_x")) return MG_ERR_CUDA;
+      if (k == 1) {
+        k_jacc64<<<nb256(nrs), 256, 0, st>>>(Lb, nrs, nv, V, dd[0].jrs);
+        if (!launched("k_jacc64")) return MG_ERR_CUDA;
+      } else {
+        k_vmulti<<<nv, 256, 0, st>>>(Lb, nrs, nb, k - 1, dws, V);
+        if (!launched("k_vmulti")) return MG_ERR_CUDA;
+        k_jacc_multi<<<nb256(nrs), 256, 0, st>>>(Lb, nrs, nv, nb, k, V, jrs_all);
+        if (!launched("k_jacc_multi")) return MG_ERR_CUDA;
+      }
+      for (OzDens& q : dd) {
+        // a short last block: clear the columns of the missing vectors
+        if (nv < nb) cudaMemsetAsync(Xf, 0, 8 * (size_t)ld * q.kx, st);
+        cudaMemsetAsync(xmax, 0, 8 * (size_t)ld, st);
+        // X_J = L_J C for the block (the slice map covers nb vectors; nv <= nb of them are used)
+        OzArgs& ax = q.ax;
+        ax.nJ = nv;
+        ax.nitems = ax.nrt * nv * q.nnt;
+        const int gx = std::min(ax.nitems, nsm);
+        oz_with_slices(s, [&](auto S) {
+          oz_gemm_kernel<false, decltype(S)::value><<<gx, kOzThreads, ax.stages * ax.stage_bytes + 1024, st>>>(
+              map_l, q.map_c, ax);
+        });
+        if (!launched("oz_gemm_kernel<false>")) return MG_ERR_CUDA;
+        oz_with_slices(sk, [&](auto S) {
+          k_oz_slice_x<decltype(S)::value><<<nb256((int64_t)ld * (q.kblk / 32)), 256, 0, st>>>(
+              Xf, ld, n, q.kx, ld, q.kblk, q.xs_row, (int64_t)bi * q.kblk, xmax, q.XS, q.eX + (size_t)bi * ld);
+        });
+        if (!launched("k_oz_slice_x")) return MG_ERR_CUDA;
+      }
     }
-    // K += X X^T over the group (lower tiles)
-    ak.nblk = gn;
-    ak.nitems = ntile * gn * nsub;
-    const int gk = std::min(ak.nitems, nsm);
-    oz_with_slices(sk, [&](auto S) {
-      oz_gemm_kernel<true, decltype(S)::value><<<gk, kOzThreads, ak.stages * ak.stage_bytes + 1024, st>>>(map_x, map_x, ak);
-    });
-    if (!launched("oz_gemm_kernel<true>")) return MG_ERR_CUDA;
+    // K += X X^T over the group (lower tiles), per density
+    for (OzDens& q : dd) {
+      OzArgs& ak = q.ak;
+      ak.nblk = gn;
+      ak.nitems = ntile * gn * q.nsub;
+      const int gk = std::min(ak.nitems, nsm);
+      oz_with_slices(sk, [&](auto S) {
+        oz_gemm_kernel<true, decltype(S)::value><<<gk, kOzThreads, ak.stages * ak.stage_bytes + 1024, st>>>(
+            q.map_x, q.map_x, ak);
+      });
+      if (!launched("oz_gemm_kernel<true>")) return MG_ERR_CUDA;
+    }
   }
-  k_symmetrize_lower<<<nb256((int64_t)nn), 256, 0, st>>>(d_K, n);
-  if (!launched("k_symmetrize_lower")) return MG_ERR_CUDA;
-  cudaMemsetAsync(d_J, 0, 8 * nn, st);  // AO pairs without rows
-  k_unpack_sym<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, jrs, n, d_J);
-  if (!launched("k_unpack_sym")) return MG_ERR_CUDA;
+  for (OzDens& q : dd) {
+    k_symmetrize_lower<<<nb256((int64_t)nn), 256, 0, st>>>(q.K, n);
+    if (!launched("k_symmetrize_lower")) return MG_ERR_CUDA;
+    cudaMemsetAsync(q.J, 0, 8 * nn, st);  // AO pairs without rows
+    k_unpack_sym<<<nb256(nrs), 256, 0, st>>>(d_ra, d_rb, nrs, q.jrs, n, q.J);
+    if (!launched("k_unpack_sym")) return MG_ERR_CUDA;
+  }
   if (const cudaError_t e = cudaGetLastError(); e != cudaSuccess) {
     h->err = std::string("mixed J/K: ") + cudaGetErrorString(e);
     return MG_ERR_CUDA;

@@ -188,6 +188,11 @@ int cd_incore(Handle* h, double* d_X, int n, double thr, double* d_vec, int maxv
 int fock_accumulate(double* F, const double* J, const double* K, double factxi, int64_t n, cudaStream_t st);
 int jk_fp64(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block);
 int jk_mixed(Handle* h, const double* d_C, int r, double* d_J, double* d_K, cudaStream_t st, int block, int s, int sk);
+// J/K of k (1..8) densities over one pass of the vectors (jk.cu)
+int jk_mixed_batch(Handle* h, int k, const double* const* Cs, const int* rs, double* const* Js, double* const* Ks,
+                   cudaStream_t st, int block, int s, int sk);
+int jk_fp64_batch(Handle* h, int k, const double* const* Cs, const int* rs, double* const* Js, double* const* Ks,
+                  cudaStream_t st, int block);
 
 inline int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 inline int ncart_cum(int l) { return l <= 0 ? 0 : l * (l + 1) * (l + 2) / 6; }

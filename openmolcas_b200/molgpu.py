@@ -59,6 +59,8 @@ def lib():
                              C.c_void_p]
     L.mg_cho_jk.argtypes = [vp, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     L.mg_rys_roots.argtypes = [vp, C.c_int, C.c_int64, d, d, d]
+    L.mg_cho_jk_batch.argtypes = [vp, C.c_int, C.POINTER(C.c_void_p), i, C.POINTER(C.c_void_p),
+                                  C.POINTER(C.c_void_p), C.c_int, C.c_void_p]
     L.mg_cd_incore.argtypes = [vp, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_int, i, C.c_void_p]
     L.mg_choscf_lk.argtypes = [vp, C.c_void_p, C.c_double, C.c_void_p, C.c_int, i, C.c_void_p]
     L.mg_eri_work.argtypes = [vp, i32, C.c_int64, d, d]
@@ -237,6 +239,23 @@ class MolGpu:
         self._check(self.L.mg_cho_jk(self.h, C.c_void_p(Cc.data_ptr()), r, C.c_void_p(J.data_ptr()),
                                      C.c_void_p(K.data_ptr()), precision, _stream(self.device)), "mg_cho_jk")
         return J, K
+
+    def cho_jk_batch(self, Cfacs, precision: int = 0):
+        """CHO_LK_SCF for several densities D_i = C_i C_i^T at once (1..8; every
+        block of vectors is unpacked once): returns a list of (J, K)."""
+        dev = f"cuda:{self.device}"
+        n, k = self.nbf, len(Cfacs)
+        Cc = [Cf.to(device=dev, dtype=torch.float64).t().contiguous() for Cf in Cfacs]
+        for Cf in Cfacs:
+            if Cf.shape[0] != n:
+                raise MolGpuError(f"C must have {n} rows")
+        Js = [torch.empty((n, n), dtype=torch.float64, device=dev) for _ in range(k)]
+        Ks = [torch.empty((n, n), dtype=torch.float64, device=dev) for _ in range(k)]
+        ptrs = lambda ts: (C.c_void_p * k)(*[t.data_ptr() for t in ts])
+        rs = (C.c_int * k)(*[int(Cf.shape[1]) for Cf in Cfacs])
+        self._check(self.L.mg_cho_jk_batch(self.h, k, ptrs(Cc), rs, ptrs(Js), ptrs(Ks), precision,
+                                           _stream(self.device)), "mg_cho_jk_batch")
+        return list(zip(Js, Ks))
 
     def cd_incore(self, X: torch.Tensor, thr: float = 1e-6, maxvec: int | None = None):
         """CD_InCore (cholesky_util/cd_incore.F90:14): pivoted Cholesky vectors of

@@ -250,3 +250,19 @@ def test_scf065_energy_through_device_cholesky(scf065):
     assert np.array_equal(piv, ref["piv"])
     assert abs(E - Eo) < 1e-9
     assert abs(E - float(z["E_SCF"])) <= 10.0 ** -int(z["E_SCF_digits"])
+
+
+@pytest.mark.parametrize("prec", [MolGpu.PREC_FP64, MolGpu.PREC_MIXED])
+def test_jk_batch_equals_single_calls(setup, prec):
+    """mg_cho_jk_batch (three densities of different rank in one pass over the
+    vectors) equals one mg_cho_jk per density, J and K within 1e-13 of their
+    largest elements, both paths (not to the bit: the CTA tiles of K and the
+    Coulomb contractions are added with FP64 atomics, whose order varies from
+    call to call)."""
+    g = setup[1]
+    Cs = [torch.from_numpy(B.density_factor(g.nbf, rk, 10 + rk)) for rk in (3, 7, 12)]
+    batch = g.cho_jk_batch(Cs, precision=prec)
+    for Cf, (Jb, Kb) in zip(Cs, batch):
+        J, K = g.cho_jk(Cf, precision=prec)
+        assert float((Jb - J).abs().max()) < 1e-13 * float(J.abs().max())
+        assert float((Kb - K).abs().max()) < 1e-13 * float(K.abs().max())
