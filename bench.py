@@ -477,15 +477,7 @@ def run_gpu(args, rank, world):
 
 
 def grad_flops(g):
-    try:
-        from openmolcas_b200.molgpu import lib as mglib
-        import ctypes
-        f = mglib().mg_drvg1_flops
-        f.restype = ctypes.c_double
-        f.argtypes = [ctypes.c_void_p, ctypes.c_double]
-        return float(f(g.h, CUTINT))
-    except Exception:
-        return None
+    return float(g.drvg1_flops(CUTINT))
 
 
 CPU_SAMPLE_FACTOR = 100  # each CPU leg times at least 1/100 of its workload

@@ -64,6 +64,8 @@ def lib():
     L.mg_cd_incore.argtypes = [vp, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_int, i, C.c_void_p]
     L.mg_choscf_lk.argtypes = [vp, C.c_void_p, C.c_double, C.c_void_p, C.c_int, i, C.c_void_p]
     L.mg_eri_work.argtypes = [vp, i32, C.c_int64, d, d]
+    L.mg_drvg1_flops.restype = C.c_double
+    L.mg_drvg1_flops.argtypes = [vp, C.c_double]
     _lib = L
     return L
 
@@ -151,6 +153,14 @@ class MolGpu:
         self._check(self.L.mg_eri_work(self.h, _p(q, C.c_int32), q.shape[0], C.byref(pq), C.byref(fl)),
                     "mg_eri_work")
         return pq.value, fl.value
+
+    def drvg1_flops(self, cutint: float = 1e-12) -> float:
+        """Algorithmic FP64 flops of drvg1 at this Schwarz threshold (the
+        kernel's work model over its quartet plan)."""
+        f = self.L.mg_drvg1_flops(self.h, cutint)
+        if f < 0:
+            raise MolGpuError(f"mg_drvg1_flops: {self.L.mg_last_error(self.h).decode()}")
+        return f
 
     def rys_roots(self, nrys: int, T) -> tuple[np.ndarray, np.ndarray]:
         """vRysRW on the device: (u^2, weights), each len(T) x nrys."""

@@ -39,6 +39,8 @@
 //    (alaska/drvg1.F90, alaska_util/twoel_g.F90, rys_util/rysg1.F90,
 //    rys_util/rys2dg.F90, rys_util/assg1.F90) with the PGet1 2-PDM
 //    (integral_util/pget1.F90:66-106) and the 1/2 of alaska.F90:236.
+//  * Built a second time with -DOR_COUNT_FLOPS (_build/liboracle_count.so),
+//    the same loops tally the FP64 operations they execute (or_flops).
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -47,12 +49,49 @@
 #include <cstring>
 #include <string>
 #include <memory>
+#include <mutex>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
 
 namespace {
+
+// ------------------------------------------- FLOP tally (instrumented build)
+// With -DOR_COUNT_FLOPS every FP64 add, subtract, multiply, divide and square
+// root that the restated loops execute is tallied where it is written (a*b + c
+// counts 2; a product with a loop index counts 1), per stage; the default
+// build compiles the tally away.  Shell-pair data (make_pair) and the HRR
+// matrices (hrr_mtrx) are basis set-up and are not counted.
+enum FlopStage {
+  FS_PRIM,      // per primitive quartet: zeta + eta, rho, |PQ|^2, T, prefactor
+  FS_ROOTS,     // Rys roots and weights (table or asymptotic form)
+  FS_RYS2D,     // vCff2D + vRys2D coefficients and recursion
+  FS_RYSEF,     // [e0|f0] = Fact sum_r Ix Iy Iz
+  FS_CONTRACT,  // contraction with the general-contraction coefficients
+  FS_HRR,       // HRR + spherical transforms of the contracted block
+  FS_TRANSFER,  // gradient: 2D-level HRR transfers (HRR2Da/HRR2Db)
+  FS_ASSG1,     // gradient: derivative 2D factors, Assg1 products, Distg1
+  FS_PDM,       // gradient: PGet1 2-PDM, spherical -> Cartesian, de-contraction
+  FS_N
+};
+#ifdef OR_COUNT_FLOPS
+thread_local double t_flops[FS_N];
+double g_flops[FS_N];
+std::mutex g_flops_mu;
+#define OR_FLOPS(stage, n) (t_flops[stage] += (double)(n))
+// move this thread's tally into the total (at the end of each shell quartet)
+void flops_commit() {
+  std::lock_guard<std::mutex> lk(g_flops_mu);
+  for (int t = 0; t < FS_N; ++t) {
+    g_flops[t] += t_flops[t];
+    t_flops[t] = 0.0;
+  }
+}
+#else
+#define OR_FLOPS(stage, n) ((void)0)
+inline void flops_commit() {}
+#endif
 
 // ----------------------------------------------------------------- Rys table
 struct RysOrder {
@@ -105,17 +144,20 @@ inline void rys_rw(int n, double T, double* x, double* w) {
   if (T >= o.tmax) {
     double ai = 1.0 / T, si = std::sqrt(ai);
     for (int i = 0; i < n; ++i) { x[i] = o.hx[i] * ai; w[i] = o.hw[i] * si; }
+    OR_FLOPS(FS_ROOTS, 2 + 2 * n);
     return;
   }
   int k = (int)(T / o.h);
   if (k >= o.K) k = o.K - 1;
   double s = 2.0 * (T - k * o.h) / o.h - 1.0;
+  OR_FLOPS(FS_ROOTS, 6);
   const int D = g_rys.D;
   const double* c = &o.coef[(size_t)k * 2 * n * (D + 1)];
   for (int q = 0; q < 2 * n; ++q) {
     const double* cq = c + q * (D + 1);
     double acc = cq[D];
     for (int j = D - 1; j >= 0; --j) acc = acc * s + cq[j];
+    OR_FLOPS(FS_ROOTS, 2 * D);
     if (q < n) x[q] = acc; else w[q - n] = acc;
   }
 }
@@ -341,24 +383,31 @@ void rys2d(int nr, int imax, int jmax, double zeta, double eta, const double* P,
   G.nr = nr; G.ni = imax + 1; G.nj = jmax + 1;
   G.v.assign((size_t)3 * nr * G.ni * G.nj, 0.0);
   double zi = 1.0 / zeta, ei = 1.0 / eta, ze = zeta + eta, zei = 1.0 / ze;
+  OR_FLOPS(FS_RYS2D, 4);
   for (int r = 0; r < nr; ++r) {
     double U2 = u2[r] * zei;              // ModU2
     double B00 = 0.5 * U2;
     double B10 = 0.5 * (1.0 - U2 * eta) * zi;
     double B01 = 0.5 * (1.0 - U2 * zeta) * ei;
+    OR_FLOPS(FS_RYS2D, 10);
     for (int c = 0; c < 3; ++c) {
       double PAQP = P[c] - Ap[c] + eta * U2 * (Q[c] - P[c]);
       double QCPQ = Q[c] - Cp[c] - zeta * U2 * (Q[c] - P[c]);
+      OR_FLOPS(FS_RYS2D, 10);
       double I00 = (c == 2) ? w[r] : 1.0;
       G.at(c, r, 0, 0) = I00;
-      if (imax >= 1) G.at(c, r, 1, 0) = PAQP * I00;
-      for (int i = 1; i < imax; ++i) G.at(c, r, i + 1, 0) = PAQP * G.at(c, r, i, 0) + i * B10 * G.at(c, r, i - 1, 0);
+      if (imax >= 1) { G.at(c, r, 1, 0) = PAQP * I00; OR_FLOPS(FS_RYS2D, 1); }
+      for (int i = 1; i < imax; ++i) {
+        G.at(c, r, i + 1, 0) = PAQP * G.at(c, r, i, 0) + i * B10 * G.at(c, r, i - 1, 0);
+        OR_FLOPS(FS_RYS2D, 4);
+      }
       for (int j = 0; j < jmax; ++j)
         for (int i = 0; i <= imax; ++i) {
           double v = QCPQ * G.at(c, r, i, j);
           if (j >= 1) v += j * B01 * G.at(c, r, i, j - 1);
           if (i >= 1) v += i * B00 * G.at(c, r, i - 1, j);
           G.at(c, r, i, j + 1) = v;
+          OR_FLOPS(FS_RYS2D, 1 + (j >= 1 ? 3 : 0) + (i >= 1 ? 3 : 0));
         }
     }
   }
@@ -411,6 +460,7 @@ void eri_quartet(const Basis& bs, int iS, int jS, int kS, int lS, double* out, b
       double PQ2 = (P[0] - Q[0]) * (P[0] - Q[0]) + (P[1] - Q[1]) * (P[1] - Q[1]) + (P[2] - Q[2]) * (P[2] - Q[2]);
       double T = rho * PQ2;
       double Fact = pab.kappa[pp] * pcd.kappa[pq] * std::sqrt(tmp);
+      OR_FLOPS(FS_PRIM, 16);
       rys_rw(nr, T, x, w);
       rys2d(nr, emax, fmax, zeta, eta, P, Q, Ap, Cp, x, w, G);
       for (int ie = 0; ie < ne; ++ie)
@@ -419,20 +469,24 @@ void eri_quartet(const Basis& bs, int iS, int jS, int kS, int lS, double* out, b
           double s = 0;
           for (int r = 0; r < nr; ++r) s += G.at(0, r, E.x, F.x) * G.at(1, r, E.y, F.y) * G.at(2, r, E.z, F.z);
           ef[ie + (size_t)ne * jf] = absmode ? std::fabs(s * Fact) : s * Fact;
+          OR_FLOPS(FS_RYSEF, 3 * nr + 1);
         }
       for (int l4 = 0; l4 < d.nc; ++l4)
         for (int k3 = 0; k3 < c.nc; ++k3) {
           double ccd = c.c[ic + c.np * k3] * d.c[id + d.np * l4];
+          OR_FLOPS(FS_CONTRACT, 1);
           if (absmode) ccd = std::fabs(ccd);
           if (ccd == 0.0) continue;
           for (int j2 = 0; j2 < b.nc; ++j2)
             for (int i1 = 0; i1 < a.nc; ++i1) {
               double cf = a.c[ia + a.np * i1] * b.c[ib + b.np * j2] * ccd;
+              OR_FLOPS(FS_CONTRACT, 2);
               if (absmode) cf = std::fabs(cf);
               if (cf == 0.0) continue;
               int ijkl = i1 + a.nc * (j2 + b.nc * (k3 + c.nc * l4));
               double* ac = &acc[(size_t)ijkl * ne * nf];
               for (size_t t = 0; t < (size_t)ne * nf; ++t) ac[t] += cf * ef[t];
+              OR_FLOPS(FS_CONTRACT, 2 * ne * nf);
             }
         }
     }
@@ -447,14 +501,17 @@ void eri_quartet(const Basis& bs, int iS, int jS, int kS, int lS, double* out, b
         double s = 0;
         for (int ie = 0; ie < ne; ++ie) s += (absmode ? std::fabs(Hab[ie + (size_t)ne * sab]) : Hab[ie + (size_t)ne * sab]) * ac[ie + (size_t)ne * jf];
         tmpab[sab + (size_t)na * nb * jf] = s;
+        OR_FLOPS(FS_HRR, 2 * ne);
       }
     for (int scd = 0; scd < nc * nd; ++scd)
       for (int sab = 0; sab < na * nb; ++sab) {
         double s = 0;
         for (int jf = 0; jf < nf; ++jf) s += (absmode ? std::fabs(Hcd[jf + (size_t)nf * scd]) : Hcd[jf + (size_t)nf * scd]) * tmpab[sab + (size_t)na * nb * jf];
         out[ijkl + (size_t)nijkl * (sab + (size_t)na * nb * scd)] = s;
+        OR_FLOPS(FS_HRR, 2 * nf);
       }
   }
+  flops_commit();
 }
 
 // AO index of (shell, contracted k, spherical m): shells store functions
@@ -909,6 +966,7 @@ void grad_quartet(const Basis& bs, int iS, int jS, int kS, int lS, const double*
       double x = Dm[p * n + r] * Dm[q * n + s] + Dm[p * n + s] * Dm[q * n + r];
       if (Ds) x += Ds[p * n + r] * Ds[q * n + s] + Ds[p * n + s] * Ds[q * n + r];
       double g = coulfac * Dm[p * n + q] * Dm[r * n + s] - 0.25 * exfac * x;
+      OR_FLOPS(FS_PDM, 8 + (Ds ? 4 : 0));
       int ijkl = k1 + nc[0] * (k2 + nc[1] * (k3 + nc[2] * k4));
       Gs[ijkl + (size_t)nijkl * (ma + ns[0] * (mb + (size_t)ns[1] * (mc + (size_t)ns[2] * md)))] = g;
     }
@@ -917,12 +975,13 @@ void grad_quartet(const Basis& bs, int iS, int jS, int kS, int lS, const double*
   std::vector<double> Gc((size_t)nijkl * ncr4, 0.0);
   for (int md = 0; md < ns[3]; ++md) for (int mc = 0; mc < ns[2]; ++mc) for (int mb = 0; mb < ns[1]; ++mb) for (int ma = 0; ma < ns[0]; ++ma)
     for (int cd = 0; cd < ncr[3]; ++cd) { double sd = g_sph[l[3]][cd + (size_t)ncr[3] * md]; if (sd == 0) continue;
-    for (int cc = 0; cc < ncr[2]; ++cc) { double sc = g_sph[l[2]][cc + (size_t)ncr[2] * mc] * sd; if (sc == 0) continue;
-    for (int cb = 0; cb < ncr[1]; ++cb) { double sb = g_sph[l[1]][cb + (size_t)ncr[1] * mb] * sc; if (sb == 0) continue;
-    for (int ca = 0; ca < ncr[0]; ++ca) { double sa = g_sph[l[0]][ca + (size_t)ncr[0] * ma] * sb; if (sa == 0) continue;
+    for (int cc = 0; cc < ncr[2]; ++cc) { double sc = g_sph[l[2]][cc + (size_t)ncr[2] * mc] * sd; OR_FLOPS(FS_PDM, 1); if (sc == 0) continue;
+    for (int cb = 0; cb < ncr[1]; ++cb) { double sb = g_sph[l[1]][cb + (size_t)ncr[1] * mb] * sc; OR_FLOPS(FS_PDM, 1); if (sb == 0) continue;
+    for (int ca = 0; ca < ncr[0]; ++ca) { double sa = g_sph[l[0]][ca + (size_t)ncr[0] * ma] * sb; OR_FLOPS(FS_PDM, 1); if (sa == 0) continue;
       size_t cidx = ca + ncr[0] * (cb + (size_t)ncr[1] * (cc + (size_t)ncr[2] * cd));
       size_t sidx = ma + ns[0] * (mb + (size_t)ns[1] * (mc + (size_t)ns[2] * md));
       for (int ijkl = 0; ijkl < nijkl; ++ijkl) Gc[ijkl + (size_t)nijkl * cidx] += sa * Gs[ijkl + (size_t)nijkl * sidx];
+      OR_FLOPS(FS_PDM, 2 * nijkl);
     }}}}
   auto cl0 = cart_list(l[0]), cl1 = cart_list(l[1]), cl2 = cart_list(l[2]), cl3 = cart_list(l[3]);
   const double *A = S[0]->A, *B = S[1]->A, *C = S[2]->A, *D = S[3]->A;
@@ -952,10 +1011,12 @@ void grad_quartet(const Basis& bs, int iS, int jS, int kS, int lS, const double*
       bool nz = false;
       for (int k4 = 0; k4 < nc[3]; ++k4) for (int k3 = 0; k3 < nc[2]; ++k3) for (int k2 = 0; k2 < nc[1]; ++k2) for (int k1 = 0; k1 < nc[0]; ++k1) {
         double cf = S[0]->c[ia + S[0]->np * k1] * S[1]->c[ib + S[1]->np * k2] * S[2]->c[ic + S[2]->np * k3] * S[3]->c[id + S[3]->np * k4];
+        OR_FLOPS(FS_PDM, 3);
         if (cf == 0.0) continue;
         nz = true;
         int ijkl = k1 + nc[0] * (k2 + nc[1] * (k3 + nc[2] * k4));
         for (size_t t = 0; t < ncr4; ++t) Gp[t] += cf * Gc[ijkl + (size_t)nijkl * t];
+        OR_FLOPS(FS_PDM, 2 * ncr4);
       }
       if (!nz) continue;
       double P[3] = {pab.P[pp], pab.P[pp + pab.np], pab.P[pp + 2 * pab.np]};
@@ -963,6 +1024,7 @@ void grad_quartet(const Basis& bs, int iS, int jS, int kS, int lS, const double*
       double PQ2 = (P[0] - Q[0]) * (P[0] - Q[0]) + (P[1] - Q[1]) * (P[1] - Q[1]) + (P[2] - Q[2]) * (P[2] - Q[2]);
       double T = rho * PQ2;
       double Fact = pab.kappa[pp] * pcd.kappa[pq] * std::sqrt(tmp);
+      OR_FLOPS(FS_PRIM, 16);
       rys_rw(nr, T, x, w);
       rys2d(nr, emax, fmax, zeta, eta, P, Q, A, C, x, w, G);
       // 2D-level HRR (HRR2Da/HRR2Db): h(a,b,c,d) from G(e,f), e at A, f at C
@@ -974,20 +1036,27 @@ void grad_quartet(const Basis& bs, int iS, int jS, int kS, int lS, const double*
           for (int e = 0; e <= emax; ++e) for (int f = 0; f <= fmax; ++f) TB(e, 0, f) = G.at(c, r, e, f);
           for (int b = 1; b < nb1; ++b)
             for (int a = 0; a + b <= emax; ++a)
-              for (int f = 0; f <= fmax; ++f) TB(a, b, f) = TB(a + 1, b - 1, f) + AB[c] * TB(a, b - 1, f);
+              for (int f = 0; f <= fmax; ++f) {
+                TB(a, b, f) = TB(a + 1, b - 1, f) + AB[c] * TB(a, b - 1, f);
+                OR_FLOPS(FS_TRANSFER, 2);
+              }
           for (int a = 0; a < na1; ++a)
             for (int b = 0; b < nb1; ++b) {
               if (a + b > emax) continue;
               std::vector<double> tk((size_t)(fmax + 1) * nd1, 0.0);
               for (int f = 0; f <= fmax; ++f) tk[(size_t)f * nd1] = TB(a, b, f);
               for (int d = 1; d < nd1; ++d)
-                for (int cc = 0; cc + d <= fmax; ++cc) tk[(size_t)cc * nd1 + d] = tk[(size_t)(cc + 1) * nd1 + d - 1] + CD[c] * tk[(size_t)cc * nd1 + d - 1];
+                for (int cc = 0; cc + d <= fmax; ++cc) {
+                  tk[(size_t)cc * nd1 + d] = tk[(size_t)(cc + 1) * nd1 + d - 1] + CD[c] * tk[(size_t)cc * nd1 + d - 1];
+                  OR_FLOPS(FS_TRANSFER, 2);
+                }
               for (int cc = 0; cc < nc1; ++cc)
                 for (int d = 0; d < nd1; ++d) if (cc + d <= fmax) h(c, r, a, b, cc, d) = tk[(size_t)cc * nd1 + d];
             }
         }
       // Assg1: sum over Cartesian components of Gamma x derivative products
       double ex[3] = {2 * alp, 2 * bet, 2 * gam};
+      OR_FLOPS(FS_ASSG1, 3);
       for (int cd = 0; cd < ncr[3]; ++cd) for (int cc = 0; cc < ncr[2]; ++cc) for (int cb = 0; cb < ncr[1]; ++cb) for (int ca = 0; ca < ncr[0]; ++ca) {
         double g = Gp[ca + ncr[0] * (cb + (size_t)ncr[1] * (cc + (size_t)ncr[2] * cd))];
         if (g == 0.0) continue;
@@ -1000,11 +1069,13 @@ void grad_quartet(const Basis& bs, int iS, int jS, int kS, int lS, const double*
             dv[0][c] = ex[0] * h(c, r, ai[c] + 1, bi[c], ci[c], di[c]) - (ai[c] ? ai[c] * h(c, r, ai[c] - 1, bi[c], ci[c], di[c]) : 0.0);
             dv[1][c] = ex[1] * h(c, r, ai[c], bi[c] + 1, ci[c], di[c]) - (bi[c] ? bi[c] * h(c, r, ai[c], bi[c] - 1, ci[c], di[c]) : 0.0);
             dv[2][c] = ex[2] * h(c, r, ai[c], bi[c], ci[c] + 1, di[c]) - (ci[c] ? ci[c] * h(c, r, ai[c], bi[c], ci[c] - 1, di[c]) : 0.0);
+            OR_FLOPS(FS_ASSG1, 6 + (ai[c] ? 1 : 0) + (bi[c] ? 1 : 0) + (ci[c] ? 1 : 0));
           }
           for (int X = 0; X < 3; ++X) {
             gq[3 * X + 0] += g * Fact * dv[X][0] * v[1] * v[2];
             gq[3 * X + 1] += g * Fact * v[0] * dv[X][1] * v[2];
             gq[3 * X + 2] += g * Fact * v[0] * v[1] * dv[X][2];
+            OR_FLOPS(FS_ASSG1, 15);
           }
         }
       }
@@ -1018,7 +1089,9 @@ void grad_quartet(const Basis& bs, int iS, int jS, int kS, int lS, const double*
     grad[3 * at[1] + c] += scale * gq[3 + c];
     grad[3 * at[2] + c] += scale * gq[6 + c];
     grad[3 * at[3] + c] += scale * gd;
+    OR_FLOPS(FS_ASSG1, 10);
   }
+  flops_commit();
 }
 
 }  // namespace
@@ -1375,6 +1448,26 @@ static int grad_sampled_x(void* h, const double* D, const double* Ds, double cou
     for (int t = 0; t < 3 * na; ++t) grad[t] += gl[t];
   }
   return 0;
+}
+
+// Per-stage FP64 operation tally of the instrumented build (the FlopStage
+// order: primitive set-up, roots, 2D recursion, RysEF, contraction, HRR +
+// spherical, 2D transfers, Assg1 + Distg1, 2-PDM); returns the number of
+// stages, or -1 in the default build.  reset != 0 clears the tally.
+int or_flops(double* out, int reset) {
+#ifdef OR_COUNT_FLOPS
+  flops_commit();
+  std::lock_guard<std::mutex> lk(g_flops_mu);
+  for (int t = 0; t < FS_N; ++t) {
+    out[t] = g_flops[t];
+    if (reset) g_flops[t] = 0.0;
+  }
+  return FS_N;
+#else
+  (void)out;
+  (void)reset;
+  return -1;
+#endif
 }
 
 int or_num_threads() {

@@ -15,21 +15,28 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "liboracle.so")
+# the same restatement with its FP64 operation tally compiled in
+LIB_COUNT = os.path.join(HERE, "_build", "liboracle_count.so")
 TABLE = os.path.join(os.path.dirname(HERE), "openmolcas_b200", "rys", "rys_table.bin")
 
-_lib = None
+_libs = {}
+
+# stages of the operation tally, in or_flops order
+FLOP_STAGES = ("prim", "roots", "rys2d", "rysef", "contract", "hrr", "transfer", "assg1", "pdm")
 
 
 def build():
     subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB):
+def lib(counting: bool = False):
+    """The oracle library; counting=True: the build that tallies its FP64
+    operations (handles of one library cannot be used with the other)."""
+    if counting not in _libs:
+        path = LIB_COUNT if counting else LIB
+        if not os.path.exists(path):
             build()
-        L = C.CDLL(LIB)
+        L = C.CDLL(path)
         d, i, vp = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
         L.or_load_rys.argtypes = [C.c_char_p]
         L.or_rys_rw.argtypes = [C.c_int, C.c_int, d, d, d]
@@ -56,11 +63,12 @@ def lib():
         L.or_grad_sampled.argtypes = [vp, d, C.c_double, C.c_int, d, C.POINTER(C.c_int64)]
         L.or_grad_sampled_at.argtypes = [vp, d, C.c_double, C.c_int, C.c_int, d, C.POINTER(C.c_int64)]
         L.or_num_threads.restype = C.c_int
+        L.or_flops.argtypes = [d, C.c_int]
         rc = L.or_load_rys(TABLE.encode())
         if rc != 0:
             raise RuntimeError(f"oracle: cannot load Rys table ({rc})")
-        _lib = L
-    return _lib
+        _libs[counting] = L
+    return _libs[counting]
 
 
 def _p(a, t=C.c_double):
@@ -85,20 +93,30 @@ def sph_matrix(l):
 class Oracle:
     """One basis on the CPU oracle."""
 
-    def __init__(self, mol):
+    def __init__(self, mol, counting: bool = False):
+        self.L = lib(counting)
         self.mol = mol
         xyz, l, npr, nco, at, ex, cf = mol.flat()
         self._keep = (xyz, l, npr, nco, at, ex, cf)
-        self.h = lib().or_basis_create(len(l), _p(xyz), _p(l, C.c_int), _p(npr, C.c_int), _p(nco, C.c_int),
+        self.h = self.L.or_basis_create(len(l), _p(xyz), _p(l, C.c_int), _p(npr, C.c_int), _p(nco, C.c_int),
                                        _p(at, C.c_int), _p(ex), _p(cf))
-        self.nbf = lib().or_nbf(self.h)
+        self.nbf = self.L.or_nbf(self.h)
         self.nshell = len(l)
 
     def __del__(self):
         try:
-            lib().or_basis_free(self.h)
+            self.L.or_basis_free(self.h)
         except Exception:
             pass
+
+    def flops(self, reset: bool = True) -> dict:
+        """FP64 operations the counting build's loops executed since the last
+        reset, per stage (FLOP_STAGES); every handle of the build shares the
+        tally."""
+        out = np.zeros(len(FLOP_STAGES))
+        if self.L.or_flops(_p(out), int(reset)) != len(FLOP_STAGES):
+            raise RuntimeError("oracle: not the counting build (Oracle(mol, counting=True))")
+        return dict(zip(FLOP_STAGES, out.tolist()))
 
     def quartet_shape(self, i, j, k, l):
         sh = self.mol.shells
@@ -109,7 +127,7 @@ class Oracle:
         """(ij|kl) block in reference layout, returned as flat Fortran-order array."""
         shp = self.quartet_shape(i, j, k, l)
         out = np.empty(int(np.prod(shp)))
-        lib().or_eri_quartet(self.h, i, j, k, l, _p(out))
+        self.L.or_eri_quartet(self.h, i, j, k, l, _p(out))
         return out
 
     def eri_quartet_abs(self, i, j, k, l):
@@ -117,18 +135,18 @@ class Oracle:
         |primitive [e0|f0]|, |HRR|): the scale of FP64 rounding error."""
         shp = self.quartet_shape(i, j, k, l)
         out = np.empty(int(np.prod(shp)))
-        lib().or_eri_quartet_abs(self.h, i, j, k, l, _p(out))
+        self.L.or_eri_quartet_abs(self.h, i, j, k, l, _p(out))
         return out
 
     def schwarz(self):
         t = np.empty(self.nshell * self.nshell)
-        lib().or_schwarz(self.h, _p(t))
+        self.L.or_schwarz(self.h, _p(t))
         return t.reshape(self.nshell, self.nshell)
 
     def eri_full(self, cutint=0.0):
         n = self.nbf
         out = np.empty(n ** 4)
-        lib().or_eri_full(self.h, cutint, _p(out))
+        self.L.or_eri_full(self.h, cutint, _p(out))
         return out.reshape(n, n, n, n)
 
     def rs_compact(self, thrcom):
@@ -136,21 +154,21 @@ class Oracle:
         over (the shell pairs that survive the initial screening), without
         decomposing.  A decomposition sets it as well; before either, the rs
         list holds every AO pair."""
-        lib().or_rs_compact(self.h, thrcom)
+        self.L.or_rs_compact(self.h, thrcom)
 
     def rs_list(self):
         """The rs list in use (AO indices a >= b within each shell pair, shell-pair id)."""
-        n = lib().or_rs_count(self.h)
+        n = self.L.or_rs_count(self.h)
         a = np.empty(n, np.int32)
         b = np.empty(n, np.int32)
         sp = np.empty(n, np.int32)
-        lib().or_rs_list(self.h, _p(a, C.c_int), _p(b, C.c_int), _p(sp, C.c_int))
+        self.L.or_rs_list(self.h, _p(a, C.c_int), _p(b, C.c_int), _p(sp, C.c_int))
         return a, b, sp
 
     def eri_diag(self):
-        n = lib().or_rs_count(self.h)
+        n = self.L.or_rs_count(self.h)
         d = np.empty(n)
-        lib().or_eri_diag(self.h, _p(d))
+        self.L.or_eri_diag(self.h, _p(d))
         return d
 
     def cholesky(self, thrcom=1e-6, span=1e-2, minqual=50, maxqual=100, maxvec=None, mxshpr=1, ialqua=2):
@@ -165,12 +183,12 @@ class Oracle:
         pas = np.zeros(maxvec, np.int32)
         M = C.c_int(0)
         npass = C.c_int(0)
-        rc = lib().or_cholesky_x(self.h, thrcom, span, minqual, maxqual, mxshpr, ialqua, maxvec, C.byref(M),
+        rc = self.L.or_cholesky_x(self.h, thrcom, span, minqual, maxqual, mxshpr, ialqua, maxvec, C.byref(M),
                                  _p(piv, C.c_int), _p(pas, C.c_int), _p(L), C.byref(npass))
         if rc != 0:
             raise RuntimeError(f"oracle cholesky failed rc={rc}")
         m = M.value
-        nrs = lib().or_rs_count(self.h)  # the decomposition's rs list (screened shell pairs have no rows)
+        nrs = self.L.or_rs_count(self.h)  # the decomposition's rs list (screened shell pairs have no rows)
         return dict(L=L[: nrs * m].reshape(m, nrs).T.copy(), piv=piv[:m].copy(), pass_of=pas[:m].copy(),
                     M=m, npass=npass.value)
 
@@ -181,14 +199,14 @@ class Oracle:
         n = self.nbf
         J = np.empty(n * n)
         K = np.empty(n * n)
-        lib().or_cho_jk(self.h, _p(Lf), M, _p(Cf), Cf.shape[1], _p(J), _p(K))
+        self.L.or_cho_jk(self.h, _p(Lf), M, _p(Cf), Cf.shape[1], _p(J), _p(K))
         return J.reshape(n, n, order="F"), K.reshape(n, n, order="F")
 
     def grad(self, D, cutint=0.0, exfac=1.0, coulfac=1.0, DS=None):
         Dc = np.ascontiguousarray(D, dtype=np.float64)
         Ds = None if DS is None else np.ascontiguousarray(DS, dtype=np.float64)
         g = np.empty(3 * self.mol.natom)
-        lib().or_grad_x(self.h, _p(Dc), None if Ds is None else Ds.ctypes.data, coulfac, exfac, cutint, _p(g))
+        self.L.or_grad_x(self.h, _p(Dc), None if Ds is None else Ds.ctypes.data, coulfac, exfac, cutint, _p(g))
         return g.reshape(-1, 3)
 
 
@@ -209,7 +227,7 @@ def grad_sampled(orc, D, cutint, stride, offset=0):
     Dc = np.ascontiguousarray(D, dtype=np.float64)
     g = np.empty(3 * orc.mol.natom)
     nq = C.c_int64(0)
-    lib().or_grad_sampled_at(orc.h, _p(Dc), cutint, stride, offset % stride, _p(g), C.byref(nq))
+    orc.L.or_grad_sampled_at(orc.h, _p(Dc), cutint, stride, offset % stride, _p(g), C.byref(nq))
     return g.reshape(-1, 3), nq.value
 
 
