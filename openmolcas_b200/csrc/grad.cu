@@ -59,7 +59,8 @@ static size_t grad_group_smem(const DPair& P, const DPair& Q, int nijc, int nklc
                        ev2((ncart4 + 1) / 2);
   const size_t nt = (size_t)pab * pcd;
   const size_t w = std::min<size_t>(rw, NR);
-  const size_t gs = ncart4 | 1, st = w * 12 * n1d + 2;  // padded strides of Gp and F
+  // padded strides of Gp and F (the kernel's Gs, J4 and St)
+  const size_t gs = ncart4 | 1, j4 = 4 * n1d + 2, st = 3 * w * j4 + (w & 1 ? 0 : 2);
   const size_t tile = ev2(nt * ((size_t)NR * 10 + 5)) + ev2(nt * gs) + nt * st;
   return ev2(fixed + std::max(tile, (size_t)16 * 9));
 }

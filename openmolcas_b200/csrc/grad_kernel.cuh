@@ -49,7 +49,7 @@ GradFn grad_kernel_m1(int nab1, int ncd1);
 // components (component 0 is (LA, 0, 0), so the x records start LA before it).
 template <int LA>
 __device__ __forceinline__ void assg1_a_block(const double* __restrict__ F, const double* __restrict__ Gp,
-                                              const int* __restrict__ IX, int nt, int nrest, int St, int Gs, int n1d4,
+                                              const int* __restrict__ IX, int nt, int nrest, int St, int Gs, int J4,
                                               int nrw, int tid, int tpq, double* acc) {
   constexpr int NCA = (LA + 1) * (LA + 2) / 2;
   constexpr CartExp<LA> ce{};
@@ -66,9 +66,9 @@ __device__ __forceinline__ void assg1_a_block(const double* __restrict__ F, cons
     }
     if (!any) continue;
     const int pk = IX[abcd0];
-    const int bx = 4 * ((pk & 255) - LA), by = n1d4 + 4 * ((pk >> 8) & 255), bz = 2 * n1d4 + 4 * (pk >> 16);
+    const int bx = 4 * ((pk & 255) - LA), by = J4 + 4 * ((pk >> 8) & 255), bz = 2 * J4 + 4 * (pk >> 16);
     const double* Fb = F + (size_t)t * St;
-    for (int rl = 0; rl < nrw; ++rl, Fb += 3 * n1d4) {
+    for (int rl = 0; rl < nrw; ++rl, Fb += 3 * J4) {
       double2 X01[LA + 1], X23[LA + 1], Y01[LA + 1], Y23[LA + 1], Z01[LA + 1], Z23[LA + 1];
 #pragma unroll
       for (int k = 0; k <= LA; ++k) {
@@ -105,7 +105,10 @@ __device__ __forceinline__ void assg1_a_block(const double* __restrict__ F, cons
 // Per-group shared layout (doubles, every region starts on an even offset):
 //   hdr[8] (AB, CD, item) | Cab | Ccd | Y | union{ reduction | tile: cf | Gp | F | S }
 // F holds, per (quartet, root, direction), the 2D integral and its three
-// centre derivatives interleaved: F[(job * n1d + e1) * 4 + {0: I, 1: dA, 2: dB, 3: dC}].
+// centre derivatives interleaved: F[job * J4 + e1 * 4 + {0: I, 1: dA, 2: dB, 3: dC}],
+// J4 = 4 n1d + 2: a job stride of 2 mod 4 doubles shifts each job's 16-byte
+// records by an odd number of bank groups, so the jobs that a warp's lane
+// segments store at once fall in different banks.
 // Threads per CTA of a variant: 512 when one CTA fills the SM (128 registers
 // per thread), 256 otherwise.
 template <int MINB>
@@ -159,10 +162,11 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
   double* U0 = reinterpret_cast<double*>(IX) + ev2((ncart4 + 1) / 2);
   // padded strides: consecutive primitive quartets fall in different bank groups
   const int Gs = ncart4 | 1;                          // Gp row (odd)
-  const int St = RW * 12 * n1d + 2;                   // F block of one quartet (= 2 mod 4)
+  const int J4 = 4 * n1d + 2;                          // F record of one (root, direction) job
+  const int St = 3 * RW * J4 + (RW & 1 ? 0 : 2);       // F block of one quartet (= 2 mod 4)
   double* cf = U0;                                    // NT * CFT
   double* Gp = cf + ev2(NT * CFT);                    // [t][abcd] primitive 2-PDM, row stride Gs
-  double* F = Gp + ev2(NT * Gs);                      // [t][rl][dir][e1][4], quartet stride St
+  double* F = Gp + ev2(NT * Gs);                      // [t][rl][dir][e1][4], job stride J4, quartet stride St
   double* Gam = Gg;                                   // [il][abcd] (global scratch)
   double* Tmp = Gg + ev2(nc * ncart4);                // stage-0 temp (global scratch)
   if (tid < 3) {
@@ -397,7 +401,6 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
           const int lane = tid & 31;
           const int seg = lane / NI, e = lane - seg * NI;  // seg >= JPW: spare lanes
           const int lup = (lane + 31) & 31, ldn = (lane + 1) & 31;
-          const int n1d4 = 4 * n1d;
           for (int jb = (tid >> 5) * JPW; jb < njobs; jb += (tpq >> 5) * JPW) {  // warp-uniform trip count
             const bool valid = seg < JPW && jb + seg < njobs;
             const int job = min(jb + seg, njobs - 1);
@@ -424,7 +427,7 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
             const double cdv = hdr[3 + d], abv = hdr[d];
             const double* ex = cf + t * CFT + NR * 10;
             const double e2a = ex[0], e2b = ex[1], e2c = ex[2];
-            double2* Fo = reinterpret_cast<double2*>(F + (size_t)t * St + (size_t)(job - 3 * nrw * t) * n1d4);
+            double2* Fo = reinterpret_cast<double2*>(F + (size_t)t * St + (size_t)(job - 3 * nrw * t) * J4);
             const bool wr = valid && e <= la;
 #pragma unroll
             for (int m = 0; m < NJ; ++m) {  // ket level: L[c] = V[e][c][m]
@@ -475,20 +478,19 @@ __global__ void __launch_bounds__(GradThreads<MINB>::value, MINB) grad_kernel(co
         //      la = 0, which puts B first in the component order with unit stride)
         const int lblk = la > 0 ? la : lb;
         if (lblk == 1) {
-          assg1_a_block<1>(F, Gp, IX, nt, ncart4 / 3, St, Gs, 4 * n1d, nrw, tid, tpq, acc);
+          assg1_a_block<1>(F, Gp, IX, nt, ncart4 / 3, St, Gs, J4, nrw, tid, tpq, acc);
         } else if (lblk == 2) {
-          assg1_a_block<2>(F, Gp, IX, nt, ncart4 / 6, St, Gs, 4 * n1d, nrw, tid, tpq, acc);
+          assg1_a_block<2>(F, Gp, IX, nt, ncart4 / 6, St, Gs, J4, nrw, tid, tpq, acc);
         } else {
           const FDiv fnt = fdiv(nt);
-          const int n1d4 = 4 * n1d;
           for (int w = tid; w < nt * ncart4; w += tpq) {
             const int abcd = fq(w, fnt), t = w - abcd * nt;
             const double gm = Gp[t * Gs + abcd];
             if (gm == 0.0) continue;
             const int pk = IX[abcd];
-            const int i0 = 4 * (pk & 255), i1 = n1d4 + 4 * ((pk >> 8) & 255), i2 = 2 * n1d4 + 4 * (pk >> 16);
+            const int i0 = 4 * (pk & 255), i1 = J4 + 4 * ((pk >> 8) & 255), i2 = 2 * J4 + 4 * (pk >> 16);
             const double* Fb = F + (size_t)t * St;
-            for (int rl = 0; rl < nrw; ++rl, Fb += 3 * n1d4) {
+            for (int rl = 0; rl < nrw; ++rl, Fb += 3 * J4) {
               const double2 x01 = *reinterpret_cast<const double2*>(Fb + i0);
               const double2 x23 = *reinterpret_cast<const double2*>(Fb + i0 + 2);
               const double2 y01 = *reinterpret_cast<const double2*>(Fb + i1);
