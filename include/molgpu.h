@@ -199,6 +199,28 @@ int mg_drvg1_x(mg_handle* h, const double* d_D, const double* d_DS, double coulf
  * no reference counterpart).  Negative on error. */
 double mg_drvg1_flops(mg_handle* h, double cutint);
 
+/* Gradient tile tuning (no reference counterpart; the knobs of the
+ * project's autotuner, openmolcas_b200/autotune.py, whose table
+ * grad_tiles.json the Python layer applies at handle creation).  The
+ * gradient runs one persistent kernel per class (nab1, ncd1) = (la+lb+1,
+ * lc+ld+1); each CTA is split into groups of tpq threads that take work
+ * items, and each group's shared memory holds a tile of primitive quartets
+ * (bra x ket) and the 2D records of some roots at a time.
+ * mg_grad_set_tile: tpq = the first group size tried (128, 256, 512; 0 =
+ * the planner's choice), order = the dimension the planner shrinks first
+ * when the tile does not fit (0 ket primitives, 1 roots per wave, 2 bra
+ * primitives).  Takes effect at the next gradient (re-plan).
+ * mg_grad_profile(h, 1): later gradients launch their classes one after
+ * another on the caller's stream with an event pair around each;
+ * mg_grad_class_times then returns the classes of the last one (key =
+ * nab1 * 8 + ncd1, kernel milliseconds; waits for them) and their count.
+ * mg_grad_plan_info: the current plan's tile per class (group size,
+ * primitive-quartet tile pab x pcd, roots per wave); returns the count. */
+int mg_grad_set_tile(mg_handle* h, int nab1, int ncd1, int tpq, int order);
+int mg_grad_profile(mg_handle* h, int enable);
+int mg_grad_class_times(mg_handle* h, int* keys, double* ms, int maxn);
+int mg_grad_plan_info(mg_handle* h, int* keys, int* tpq, int* pab, int* pcd, int* rw, int maxn);
+
 /* ---------------------------------------------------------------------
  * Rys roots and weights (replaces vRysRW, rys_util/vrysrw.F90:15, and the
  * RysNN table evaluation, rys22.F90:36-47, at the unit-test level): for the n

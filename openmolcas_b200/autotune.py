@@ -1,0 +1,134 @@
+"""Tile autotuner of the two-electron gradient (mg_drvg1).
+
+The gradient runs one persistent kernel per shell-quartet class (la+lb+1,
+lc+ld+1).  How each class tiles its work -- threads per work-item group and
+which dimension of the primitive-quartet tile (ket primitives, roots per
+wave, bra primitives) shrinks first to fit shared memory -- is chosen by the
+planner from a fixed rule.  This tool measures instead: every candidate
+(group size 128/256/512 x shrink order 0/1/2) is applied to all classes, the
+gradient runs profiled (classes one after another on one stream, an event
+pair around each kernel), and each class keeps the candidate with the
+shortest kernel time if it beats the planner's own choice by more than the
+margin.  The result is written to grad_tiles.json, which MolGpu applies at
+handle creation (mg_grad_set_tile per class).
+
+    python -m openmolcas_b200.autotune [--cfg c4] [--reps 2] [--margin 0.02] [--out PATH]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+import torch
+
+from openmolcas_b200 import basis as B
+from openmolcas_b200.molgpu import GRAD_TILES, MolGpu
+
+CANDIDATES = [(tpq, order) for tpq in (128, 256, 512) for order in (0, 1, 2)]
+CUTINT = 1e-12
+
+
+def _class_times(g, D, reps):
+    """Per-class minimum kernel milliseconds over `reps` profiled gradients
+    (after one unprofiled-timing warm-up that also re-plans)."""
+    g.drvg1(D, CUTINT)
+    torch.cuda.synchronize()
+    best = {}
+    for _ in range(reps):
+        g.drvg1(D, CUTINT)
+        for k, t in g.grad_class_times().items():
+            best[k] = min(best.get(k, float("inf")), t)
+    return best, g.grad_plan_info()
+
+
+def _set_all(g, tpq, order):
+    for a in range(1, 8):
+        for b in range(1, 8):
+            g.set_grad_tile(a, b, tpq, order)
+
+
+def _gradient_ms(g, D, reps):
+    """Mean device milliseconds of the normal (multi-stream) gradient."""
+    g.grad_profile(False)
+    g.drvg1(D, CUTINT)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.drvg1(D, CUTINT)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return float(np.mean(ms))
+
+
+def tune(cfg="c4", reps=2, margin=0.02, device=0, log=print):
+    mol = B.config_molecule(cfg)
+    c = B.CONFIGS[cfg]
+    g = MolGpu(mol, device, grad_tiles=None)
+    Cm = B.density_factor(g.nbf, c["rank"] or 40, c["seed"])
+    D = torch.from_numpy(Cm @ Cm.T).to(f"cuda:{device}")
+    t0 = time.time()
+    g.grad_profile(True)
+    _set_all(g, 0, 0)
+    base, base_plan = _class_times(g, D, reps)
+    log(f"planner: {sum(base.values()):.1f} ms over {len(base)} classes")
+    runs = {}
+    for tpq, order in CANDIDATES:
+        _set_all(g, tpq, order)
+        runs[(tpq, order)] = _class_times(g, D, reps)
+        log(f"tpq {tpq} order {order}: {sum(runs[(tpq, order)][0].values()):.1f} ms")
+    classes = {}
+    for k, tb in sorted(base.items()):
+        (tpq, order), (tt, plan) = min(((cand, (r[0][k], r[1][k])) for cand, r in runs.items()),
+                                       key=lambda x: x[1][0])
+        if tt < (1.0 - margin) * tb:
+            classes[f"{k[0]},{k[1]}"] = {"tpq": tpq, "order": order, "tile": list(plan), "ms": round(tt, 3),
+                                         "planner_tile": list(base_plan[k]), "planner_ms": round(tb, 3)}
+    # check: the table against the planner, profiled and in the normal launch
+    _set_all(g, 0, 0)
+    for key, t in classes.items():
+        a, b = (int(x) for x in key.split(","))
+        g.set_grad_tile(a, b, t["tpq"], t["order"])
+    tuned, _ = _class_times(g, D, reps)
+    ms_tuned = _gradient_ms(g, D, max(reps, 3))
+    _set_all(g, 0, 0)
+    ms_planner = _gradient_ms(g, D, max(reps, 3))
+    table = {
+        "workload": f"{cfg}: {mol.natom} atoms, {g.nbf} bf, Schwarz {CUTINT}; per-class kernel time, minimum of "
+                    f"{reps} profiled gradients per candidate",
+        "device": torch.cuda.get_device_name(device),
+        "candidates": [list(x) for x in CANDIDATES],
+        "margin": margin,
+        "profiled_ms": {"planner": round(sum(base.values()), 2), "tuned": round(sum(tuned.values()), 2)},
+        "gradient_ms": {"planner": round(ms_planner, 2), "tuned": round(ms_tuned, 2)},
+        "tuning_seconds": round(time.time() - t0, 1),
+        "classes": classes,
+    }
+    g.close()
+    return table
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--cfg", default="c4")
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--margin", type=float, default=0.02)
+    ap.add_argument("--out", default=GRAD_TILES)
+    args = ap.parse_args(argv)
+    table = tune(args.cfg, args.reps, args.margin, log=lambda m: print(m, file=sys.stderr, flush=True))
+    with open(args.out, "w") as f:
+        json.dump(table, f, indent=1)
+        f.write("\n")
+    print(json.dumps({k: table[k] for k in ("profiled_ms", "gradient_ms", "tuning_seconds")}
+                     | {"classes_changed": len(table["classes"])}))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

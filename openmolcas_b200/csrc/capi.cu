@@ -204,6 +204,7 @@ int mg_destroy(mg_handle* H) {
     if (h->eri_events[k]) cudaEventDestroy(h->eri_events[k]);
   }
   if (h->eri_fork) cudaEventDestroy(h->eri_fork);
+  for (cudaEvent_t e : h->grad_ev) cudaEventDestroy(e);
   if (h->ws.ptr) cudaFree(h->ws.ptr);
   delete H;
   return 0;
@@ -653,6 +654,59 @@ int mg_rys_roots(mg_handle* H, int nrys, int64_t n, const double* T, double* x, 
   cudaFree(d);
   if (rc) h->err = "mg_rys_roots: evaluation failed";
   return rc;
+}
+
+int mg_grad_set_tile(mg_handle* H, int nab1, int ncd1, int tpq, int order) {
+  if (!H) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  if (nab1 < 1 || nab1 > 7 || ncd1 < 1 || ncd1 > 7 || (tpq != 0 && tpq != 128 && tpq != 256 && tpq != 512) ||
+      order < 0 || order > 2) {
+    h->err = "mg_grad_set_tile: class 1..7 x 1..7, tpq 0/128/256/512, order 0..2";
+    return MG_ERR_ARG;
+  }
+  h->grad_tpq[nab1 * 8 + ncd1] = tpq;
+  h->grad_order[nab1 * 8 + ncd1] = order;
+  if (h->grad) h->grad->cutint = -1;  // re-plan at the next gradient
+  return 0;
+}
+
+int mg_grad_profile(mg_handle* H, int enable) {
+  if (!H) return MG_ERR_ARG;
+  H->h.grad_profile = enable != 0;
+  H->h.grad_ev_used = 0;
+  return 0;
+}
+
+int mg_grad_class_times(mg_handle* H, int* keys, double* ms, int maxn) {
+  if (!H || (maxn > 0 && (!keys || !ms))) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  const int n = std::min(maxn, h->grad_ev_used);
+  for (int k = 0; k < n; ++k) {
+    float t = 0.f;
+    if (cudaEventSynchronize(h->grad_ev[2 * k + 1]) != cudaSuccess ||
+        cudaEventElapsedTime(&t, h->grad_ev[2 * k], h->grad_ev[2 * k + 1]) != cudaSuccess) {
+      h->err = "mg_grad_class_times: no profiled gradient to read";
+      return MG_ERR_CUDA;
+    }
+    keys[k] = h->grad_ev_key[k];
+    ms[k] = t;
+  }
+  return h->grad_ev_used;
+}
+
+int mg_grad_plan_info(mg_handle* H, int* keys, int* tpq, int* pab, int* pcd, int* rw, int maxn) {
+  if (!H || (maxn > 0 && (!keys || !tpq || !pab || !pcd || !rw))) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  if (!h->grad || h->grad->cutint < 0) return 0;
+  const std::vector<GradClass>& cl = h->grad->classes;
+  for (int k = 0; k < std::min<int>(maxn, (int)cl.size()); ++k) {
+    keys[k] = cl[k].nab1 * 8 + cl[k].ncd1;
+    tpq[k] = cl[k].tpq;
+    pab[k] = cl[k].pab;
+    pcd[k] = cl[k].pcd;
+    rw[k] = cl[k].rw;
+  }
+  return (int)cl.size();
 }
 
 double mg_drvg1_flops(mg_handle* H, double cutint) {

@@ -163,17 +163,24 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
     GradClass c;
     c.tpq = 0;
     // one 512-thread CTA per SM (128 registers per thread; measured faster than
-    // 2 or 3 smaller CTAs whose register budgets spill); groups of tpq threads
+    // 2 or 3 smaller CTAs whose register budgets spill); groups of tpq threads.
+    // The class's tile choice (mg_grad_set_tile, written by the autotuner) may set
+    // the first group size tried and the order in which the tile shrinks:
+    // 0 ket primitives, bra primitives, roots per wave; 1 roots first; 2 bra first.
     {
       const size_t cta = kCtaLimit / 8 - kGTabD;
       const int nthr = GradThreads<1>::value;
-      for (int tpq = wmax <= 512 ? 128 : 256; tpq <= nthr && !c.tpq; tpq *= 2) {
+      const int order = h->grad_order[key];
+      const int tpq0 = h->grad_tpq[key] ? h->grad_tpq[key] : (wmax <= 512 ? 128 : 256);
+      for (int tpq = tpq0; tpq <= nthr && !c.tpq; tpq *= 2) {
         const int groups = nthr / tpq;
         const size_t gb = (cta / groups) & ~(size_t)1;
         int pab = std::max(1, std::min(m.npab, 16)), pcd = std::max(1, std::min(m.npcd, 8)), rw = NRc;
         size_t need = worst(pab, pcd, rw);
         while (need > gb && (pab > 1 || pcd > 1 || rw > 1)) {
-          if (pcd > 1) pcd = (pcd + 1) / 2;
+          if (order == 1 && rw > 1) --rw;
+          else if (order == 2 && pab > 1) pab = (pab + 1) / 2;
+          else if (pcd > 1) pcd = (pcd + 1) / 2;
           else if (pab > 1) pab = (pab + 1) / 2;
           else --rw;
           need = worst(pab, pcd, rw);
@@ -260,7 +267,18 @@ int grad_run(Handle* h, const GradPlan& plan, const double* d_D, const double* d
   int rc = side_streams_fork(h, st);
   if (rc) return rc;
   // largest classes first; the scratch region follows the stream (classes on one
-  // stream run one after another)
+  // stream run one after another).  Profiled: every class on the caller's stream,
+  // between its own pair of events.
+  if (h->grad_profile) {
+    const size_t need = 2 * plan.classes.size();
+    while (h->grad_ev.size() < need) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) { h->err = "gradient profiling events"; return MG_ERR_CUDA; }
+      h->grad_ev.push_back(e);
+    }
+    h->grad_ev_key.assign(plan.classes.size(), 0);
+    h->grad_ev_used = (int)plan.classes.size();
+  }
   std::vector<int> order(plan.classes.size());
   for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
   std::stable_sort(order.begin(), order.end(),
@@ -270,14 +288,19 @@ int grad_run(Handle* h, const GradPlan& plan, const double* d_D, const double* d
     const GradClass& c = plan.classes[ci];
     GradFn k = grad_kernel_m1(c.nab1, c.ncd1);
     if (!k) { h->err = "gradient class out of range"; return MG_ERR_ARG; }
-    const int sk = (int)(pos % MG_ERI_STREAMS);
+    const int sk = h->grad_profile ? 0 : (int)(pos % MG_ERI_STREAMS);
+    const cudaStream_t ks = h->grad_profile ? st : h->eri_streams[sk];
     GradArgs a{plan.d_items + c.begin, c.count, h->d_pairs, h->d_prim, h->tot_np, h->d_coef, d_D, h->nbf,
                plan.d_tab, d_grad, plan.d_scratch + plan.scratch_stride * sk, c.scr, plan.d_counters + ci, c.tpq,
                c.gsm, c.pab, c.pcd, c.rw, d_DS, coulfac, 0.25 * exfac};
-    k<<<(unsigned)c.grid, c.tpq * c.groups, sizeof(double) * (kGTabD + (size_t)c.gsm * c.groups),
-        h->eri_streams[sk]>>>(a, ra);
+    if (h->grad_profile) {
+      h->grad_ev_key[pos] = c.nab1 * 8 + c.ncd1;
+      cudaEventRecord(h->grad_ev[2 * pos], ks);
+    }
+    k<<<(unsigned)c.grid, c.tpq * c.groups, sizeof(double) * (kGTabD + (size_t)c.gsm * c.groups), ks>>>(a, ra);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (cudaGetLastError() != cudaSuccess) { h->err = "gradient kernel launch failed"; return MG_ERR_CUDA; }
+    if (h->grad_profile) cudaEventRecord(h->grad_ev[2 * pos + 1], ks);
   }
   side_streams_join(h, st);
   return 0;

@@ -120,6 +120,16 @@ struct Handle {
   size_t lk_cap = 0;
   double* d_dcd = nullptr;         // density copy and its Cholesky vectors of mg_choscf_lk (2 nbf^2)
   size_t dcd_cap = 0;
+  // gradient tile choices per class key (nab1 * 8 + ncd1): threads per group
+  // (0 = the planner's) and the order in which the tile shrinks to fit
+  int grad_tpq[64] = {};
+  int grad_order[64] = {};
+  // profiled gradients: classes one after another on the caller's stream, an
+  // event pair around each (grad_ev[2k], grad_ev[2k + 1] for class key grad_ev_key[k])
+  bool grad_profile = false;
+  std::vector<cudaEvent_t> grad_ev;
+  std::vector<int> grad_ev_key;
+  int grad_ev_used = 0;
 };
 
 struct GradItem {

@@ -10,6 +10,7 @@ without the library or a CUDA device the calls raise.
 from __future__ import annotations
 
 import ctypes as C
+import json
 import os
 
 import numpy as np
@@ -18,6 +19,8 @@ import torch
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmolgpu.so")
 RYS_TABLE = os.path.join(HERE, "rys", "rys_table.bin")
+# gradient tile table written by openmolcas_b200/autotune.py
+GRAD_TILES = os.path.join(HERE, "grad_tiles.json")
 
 _lib = None
 
@@ -66,6 +69,10 @@ def lib():
     L.mg_eri_work.argtypes = [vp, i32, C.c_int64, d, d]
     L.mg_drvg1_flops.restype = C.c_double
     L.mg_drvg1_flops.argtypes = [vp, C.c_double]
+    L.mg_grad_set_tile.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.mg_grad_profile.argtypes = [vp, C.c_int]
+    L.mg_grad_class_times.argtypes = [vp, i, d, C.c_int]
+    L.mg_grad_plan_info.argtypes = [vp, i, i, i, i, i, C.c_int]
     _lib = L
     return L
 
@@ -87,7 +94,9 @@ class ChoCfg(C.Structure):
 class MolGpu:
     """One basis set resident on one GPU (the handle of the C ABI)."""
 
-    def __init__(self, mol, device: int = 0):
+    def __init__(self, mol, device: int = 0, grad_tiles: str | None = GRAD_TILES):
+        """grad_tiles: the gradient tile table to apply (the autotuner's JSON;
+        None or a missing file: the planner's own choices)."""
         if not torch.cuda.is_available():
             raise MolGpuError("molgpu needs a CUDA device (no CPU fallback)")
         self.mol = mol
@@ -104,6 +113,11 @@ class MolGpu:
         self.nbf = self.L.mg_nbf(self.h)
         self.natom = self.L.mg_natom(self.h)
         self.nshell = len(l)
+        if grad_tiles and os.path.exists(grad_tiles):
+            with open(grad_tiles) as f:
+                for key, t in json.load(f)["classes"].items():
+                    nab1, ncd1 = (int(x) for x in key.split(","))
+                    self.set_grad_tile(nab1, ncd1, t["tpq"], t["order"])
 
     def _check(self, rc, what):
         if rc != 0:
@@ -161,6 +175,34 @@ class MolGpu:
         if f < 0:
             raise MolGpuError(f"mg_drvg1_flops: {self.L.mg_last_error(self.h).decode()}")
         return f
+
+    def set_grad_tile(self, nab1: int, ncd1: int, tpq: int = 0, order: int = 0):
+        """Tile choice of gradient class (la+lb+1, lc+ld+1): first group size
+        tried (0 = the planner's) and the dimension shrunk first (0 ket
+        primitives, 1 roots per wave, 2 bra primitives)."""
+        self._check(self.L.mg_grad_set_tile(self.h, nab1, ncd1, tpq, order), "mg_grad_set_tile")
+
+    def grad_profile(self, enable: bool = True):
+        """Later gradients run their classes one after another on the current
+        stream, each timed with its own event pair."""
+        self._check(self.L.mg_grad_profile(self.h, int(enable)), "mg_grad_profile")
+
+    def grad_class_times(self) -> dict:
+        """Kernel milliseconds per class (nab1, ncd1) of the last profiled gradient."""
+        keys, ms = np.zeros(64, dtype=np.int32), np.zeros(64)
+        n = self.L.mg_grad_class_times(self.h, _p(keys, C.c_int), _p(ms), 64)
+        if n < 0:
+            self._check(n, "mg_grad_class_times")
+        return {(int(k) // 8, int(k) % 8): float(t) for k, t in zip(keys[:n], ms[:n])}
+
+    def grad_plan_info(self) -> dict:
+        """Tile of every class of the current gradient plan: (tpq, pab, pcd, rw)."""
+        a = [np.zeros(64, dtype=np.int32) for _ in range(5)]
+        n = self.L.mg_grad_plan_info(self.h, *[_p(x, C.c_int) for x in a], 64)
+        if n < 0:
+            self._check(n, "mg_grad_plan_info")
+        return {(int(k) // 8, int(k) % 8): (int(t), int(pa), int(pc), int(r))
+                for k, t, pa, pc, r in zip(*[x[:n] for x in a])}
 
     def rys_roots(self, nrys: int, T) -> tuple[np.ndarray, np.ndarray]:
         """vRysRW on the device: (u^2, weights), each len(T) x nrys."""
