@@ -83,7 +83,7 @@ int build_eri_items(Handle* h, const int32_t* q4, int64_t nq, const int64_t* off
     c.ncd = key % 8;
     c.begin = items.size();
     c.count = v.size();
-    c.plan = eri_plan(c.nab, c.ncd, st[key]);
+    c.plan = eri_plan(c.nab, c.ncd, st[key], h->eri_tpq[key], h->eri_order[key]);
     c.work = st[key].work;
     if (c.plan.PAB < 1) {
       h->err = "mg_eri_quartets: class does not fit in shared memory";
@@ -120,14 +120,31 @@ int run_eri_items(Handle* h, const std::vector<EriItem>& items, const std::vecto
   std::vector<int> order(classes.size());
   for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return classes[a].work > classes[b].work; });
+  // profiled (mg_eri_profile): every class on the caller's stream between its own events
+  if (h->eri_profile) {
+    while (h->eri_ev.size() < 2 * classes.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) { h->err = "ERI profiling events"; return MG_ERR_CUDA; }
+      h->eri_ev.push_back(e);
+    }
+    h->eri_ev_key.assign(classes.size(), 0);
+    h->eri_ev_plan.assign(classes.size(), ClassPlan{});
+    h->eri_ev_used = (int)classes.size();
+  }
   for (size_t k = 0; k < order.size(); ++k) {
     const int ci = order[k];
     const EriClass& c = classes[ci];
-    if (eri_launch_class(h, d_items + c.begin, c.count, c.nab, c.ncd, c.plan, d_out, h->d_eri_counters + ci,
-                         h->eri_streams[k % MG_ERI_STREAMS])) {
+    const cudaStream_t ks = h->eri_profile ? st : h->eri_streams[k % MG_ERI_STREAMS];
+    if (h->eri_profile) {
+      h->eri_ev_key[k] = c.nab * 8 + c.ncd;
+      h->eri_ev_plan[k] = c.plan;
+      cudaEventRecord(h->eri_ev[2 * k], ks);
+    }
+    if (eri_launch_class(h, d_items + c.begin, c.count, c.nab, c.ncd, c.plan, d_out, h->d_eri_counters + ci, ks)) {
       h->err = std::string("ERI kernel launch failed: ") + cudaGetErrorString(cudaGetLastError());
       return MG_ERR_CUDA;
     }
+    if (h->eri_profile) cudaEventRecord(h->eri_ev[2 * k + 1], ks);
   }
   side_streams_join(h, st);
   return 0;
@@ -205,6 +222,7 @@ int mg_destroy(mg_handle* H) {
   }
   if (h->eri_fork) cudaEventDestroy(h->eri_fork);
   for (cudaEvent_t e : h->grad_ev) cudaEventDestroy(e);
+  for (cudaEvent_t e : h->eri_ev) cudaEventDestroy(e);
   if (h->ws.ptr) cudaFree(h->ws.ptr);
   delete H;
   return 0;
@@ -692,6 +710,46 @@ int mg_grad_class_times(mg_handle* H, int* keys, double* ms, int maxn) {
     ms[k] = t;
   }
   return h->grad_ev_used;
+}
+
+int mg_eri_set_tile(mg_handle* H, int nab, int ncd, int tpq, int order) {
+  if (!H) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  if (nab < 0 || nab > 7 || ncd < 0 || ncd > 7 || (tpq != 0 && tpq != 64 && tpq != 128 && tpq != 256 && tpq != 512) ||
+      order < 0 || order > 1) {
+    h->err = "mg_eri_set_tile: class 0..7 x 0..7, tpq 0/64/128/256/512, order 0..1";
+    return MG_ERR_ARG;
+  }
+  h->eri_tpq[nab * 8 + ncd] = tpq;
+  h->eri_order[nab * 8 + ncd] = order;
+  return 0;
+}
+
+int mg_eri_profile(mg_handle* H, int enable) {
+  if (!H) return MG_ERR_ARG;
+  H->h.eri_profile = enable != 0;
+  H->h.eri_ev_used = 0;
+  return 0;
+}
+
+int mg_eri_class_times(mg_handle* H, int* keys, double* ms, int* tpq, int* pab, int* pcd, int maxn) {
+  if (!H || (maxn > 0 && (!keys || !ms || !tpq || !pab || !pcd))) return MG_ERR_ARG;
+  Handle* h = &H->h;
+  const int n = std::min(maxn, h->eri_ev_used);
+  for (int k = 0; k < n; ++k) {
+    float t = 0.f;
+    if (cudaEventSynchronize(h->eri_ev[2 * k + 1]) != cudaSuccess ||
+        cudaEventElapsedTime(&t, h->eri_ev[2 * k], h->eri_ev[2 * k + 1]) != cudaSuccess) {
+      h->err = "mg_eri_class_times: no profiled ERI batch to read";
+      return MG_ERR_CUDA;
+    }
+    keys[k] = h->eri_ev_key[k];
+    ms[k] = t;
+    tpq[k] = h->eri_ev_plan[k].tpq;
+    pab[k] = h->eri_ev_plan[k].PAB;
+    pcd[k] = h->eri_ev_plan[k].PCD;
+  }
+  return h->eri_ev_used;
 }
 
 int mg_grad_plan_info(mg_handle* H, int* keys, int* tpq, int* pab, int* pcd, int* rw, int maxn) {

@@ -65,19 +65,22 @@ static size_t eri_group_smem(int nab, int ncd, const ClassStats& cs, int pab, in
          std::max(tile, ev2s(cs.max_tmp));
 }
 
-ClassPlan eri_plan(int nab, int ncd, const ClassStats& cs) {
+// tpq0: the first group size tried (0: from the widest stage); order: the tile
+// dimension shrunk first when it does not fit (0 ket primitives, 1 bra)
+ClassPlan eri_plan(int nab, int ncd, const ClassStats& cs, int tpq0, int order) {
   const int NR = (nab + ncd) / 2 + 1;
   ClassPlan pl{0, 0, 0, 0, 0};
   const size_t budget = (227 * 1024) / 8 - kETabD;  // one CTA per SM
   int pab = std::max(1, std::min(cs.max_npab, 32));
   int pcd = std::max(1, std::min(cs.max_npcd, 8));
   const int width = std::max({cs.max_acc, pab * pcd * cs.max_nef / 2, pab * pcd * NR * 3 * 8});
-  for (int tpq = width <= 96 ? 64 : width <= 384 ? 128 : 256; tpq <= kEriThreads; tpq *= 2) {
+  for (int tpq = tpq0 ? tpq0 : width <= 96 ? 64 : width <= 384 ? 128 : 256; tpq <= kEriThreads; tpq *= 2) {
     const int groups = kEriThreads / tpq;
     const size_t gbudget = (budget / groups) & ~(size_t)1;
     int a = pab, c = pcd;
     while (eri_group_smem(nab, ncd, cs, a, c) > gbudget && (a > 1 || c > 1)) {
-      if (c > 1) c = (c + 1) / 2;
+      if (order == 1 && a > 1) a = (a + 1) / 2;
+      else if (c > 1) c = (c + 1) / 2;
       else a = (a + 1) / 2;
     }
     if (eri_group_smem(nab, ncd, cs, a, c) <= gbudget) {

@@ -130,6 +130,15 @@ struct Handle {
   std::vector<cudaEvent_t> grad_ev;
   std::vector<int> grad_ev_key;
   int grad_ev_used = 0;
+  // the same for the ERI classes (key nab * 8 + ncd; order 0 ket primitives
+  // shrink first, 1 bra primitives), with each profiled class's plan
+  int eri_tpq[64] = {};
+  int eri_order[64] = {};
+  bool eri_profile = false;
+  std::vector<cudaEvent_t> eri_ev;
+  std::vector<int> eri_ev_key;
+  std::vector<ClassPlan> eri_ev_plan;
+  int eri_ev_used = 0;
 };
 
 struct GradItem {
@@ -217,7 +226,7 @@ int setup_pairs(Handle* h);
 void* ws_get(Handle* h, size_t bytes, cudaStream_t st);
 
 // ERI work lists (capi.cu) and launchers (eri.cu)
-ClassPlan eri_plan(int nab, int ncd, const ClassStats& cs);
+ClassPlan eri_plan(int nab, int ncd, const ClassStats& cs, int tpq0 = 0, int order = 0);
 int eri_launch_class(Handle* h, const EriItem* d_items, int nitems, int nab, int ncd, const ClassPlan& pl, double* out,
                      int* d_counter, cudaStream_t st);
 int build_eri_items(Handle* h, const int32_t* q4, int64_t nq, const int64_t* offsets, std::vector<EriItem>& items,

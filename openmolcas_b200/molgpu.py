@@ -19,8 +19,9 @@ import torch
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmolgpu.so")
 RYS_TABLE = os.path.join(HERE, "rys", "rys_table.bin")
-# gradient tile table written by openmolcas_b200/autotune.py
+# tile tables written by openmolcas_b200/autotune.py
 GRAD_TILES = os.path.join(HERE, "grad_tiles.json")
+ERI_TILES = os.path.join(HERE, "eri_tiles.json")
 
 _lib = None
 
@@ -73,6 +74,9 @@ def lib():
     L.mg_grad_profile.argtypes = [vp, C.c_int]
     L.mg_grad_class_times.argtypes = [vp, i, d, C.c_int]
     L.mg_grad_plan_info.argtypes = [vp, i, i, i, i, i, C.c_int]
+    L.mg_eri_set_tile.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.mg_eri_profile.argtypes = [vp, C.c_int]
+    L.mg_eri_class_times.argtypes = [vp, i, d, i, i, i, C.c_int]
     _lib = L
     return L
 
@@ -94,8 +98,8 @@ class ChoCfg(C.Structure):
 class MolGpu:
     """One basis set resident on one GPU (the handle of the C ABI)."""
 
-    def __init__(self, mol, device: int = 0, grad_tiles: str | None = GRAD_TILES):
-        """grad_tiles: the gradient tile table to apply (the autotuner's JSON;
+    def __init__(self, mol, device: int = 0, grad_tiles: str | None = GRAD_TILES, eri_tiles: str | None = ERI_TILES):
+        """grad_tiles, eri_tiles: the tile tables to apply (the autotuner's JSON;
         None or a missing file: the planner's own choices)."""
         if not torch.cuda.is_available():
             raise MolGpuError("molgpu needs a CUDA device (no CPU fallback)")
@@ -118,6 +122,11 @@ class MolGpu:
                 for key, t in json.load(f)["classes"].items():
                     nab1, ncd1 = (int(x) for x in key.split(","))
                     self.set_grad_tile(nab1, ncd1, t["tpq"], t["order"])
+        if eri_tiles and os.path.exists(eri_tiles):
+            with open(eri_tiles) as f:
+                for key, t in json.load(f)["classes"].items():
+                    nab, ncd = (int(x) for x in key.split(","))
+                    self.set_eri_tile(nab, ncd, t["tpq"], t["order"])
 
     def _check(self, rc, what):
         if rc != 0:
@@ -194,6 +203,26 @@ class MolGpu:
         if n < 0:
             self._check(n, "mg_grad_class_times")
         return {(int(k) // 8, int(k) % 8): float(t) for k, t in zip(keys[:n], ms[:n])}
+
+    def set_eri_tile(self, nab: int, ncd: int, tpq: int = 0, order: int = 0):
+        """Tile choice of ERI class (la+lb, lc+ld): first group size tried (0 =
+        the planner's) and the dimension shrunk first (0 ket, 1 bra primitives)."""
+        self._check(self.L.mg_eri_set_tile(self.h, nab, ncd, tpq, order), "mg_eri_set_tile")
+
+    def eri_profile(self, enable: bool = True):
+        """Later ERI batches run their classes one after another on the
+        current stream, each timed with its own event pair."""
+        self._check(self.L.mg_eri_profile(self.h, int(enable)), "mg_eri_profile")
+
+    def eri_class_times(self) -> dict:
+        """(nab, ncd) -> (kernel ms, (tpq, pab, pcd)) of the last profiled ERI batch."""
+        a = [np.zeros(64, dtype=np.int32) for _ in range(4)]
+        ms = np.zeros(64)
+        n = self.L.mg_eri_class_times(self.h, _p(a[0], C.c_int), _p(ms), *[_p(x, C.c_int) for x in a[1:]], 64)
+        if n < 0:
+            self._check(n, "mg_eri_class_times")
+        return {(int(k) // 8, int(k) % 8): (float(t), (int(tq), int(pa), int(pc)))
+                for k, t, tq, pa, pc in zip(a[0][:n], ms[:n], a[1][:n], a[2][:n], a[3][:n])}
 
     def grad_plan_info(self) -> dict:
         """Tile of every class of the current gradient plan: (tpq, pab, pcd, rw)."""

@@ -10,8 +10,8 @@ import pytest
 import torch
 
 from openmolcas_b200 import basis as B
-from openmolcas_b200.autotune import CANDIDATES
-from openmolcas_b200.molgpu import GRAD_TILES
+from openmolcas_b200.autotune import CANDIDATES, ERI_CANDIDATES
+from openmolcas_b200.molgpu import ERI_TILES, GRAD_TILES
 
 
 def _setup():
@@ -53,14 +53,39 @@ def test_profiled_gradient_times_every_class():
     assert g.grad_class_times() == {}
 
 
-def test_committed_tile_table_is_valid():
-    if not os.path.exists(GRAD_TILES):
+@pytest.mark.gpu
+def test_every_eri_tile_choice_gives_the_same_integrals():
+    """Every class of the s..f test molecule under each ERI candidate, also
+    profiled (classes one after another, timed per class)."""
+    from openmolcas_b200.molgpu import MolGpu, unique_quartets
+    mol = B.small_molecule(3, seed=5)
+    g = MolGpu(mol, eri_tiles=None)
+    q = unique_quartets(len(mol.shells))
+    ref, _ = g.eri_quartets(q)
+    ref = ref.cpu().numpy()
+    scale = np.abs(ref).max()
+    plans = set()
+    g.eri_profile(True)
+    for tpq, order in ERI_CANDIDATES:
+        for a in range(8):
+            for b in range(8):
+                g.set_eri_tile(a, b, tpq, order)
+        got, _ = g.eri_quartets(q)
+        times = g.eri_class_times()
+        plans.add(tuple(sorted((k, pl) for k, (_, pl) in times.items())))
+        assert all(t > 0 for t, _ in times.values()) and len(times) > 1
+        assert np.abs(got.cpu().numpy() - ref).max() < 1e-11 * max(1.0, scale), (tpq, order)
+    assert len(plans) > 1
+
+
+@pytest.mark.parametrize("path,cands,lo", [(GRAD_TILES, CANDIDATES, 1), (ERI_TILES, ERI_CANDIDATES, 0)])
+def test_committed_tile_tables_are_valid(path, cands, lo):
+    if not os.path.exists(path):
         pytest.skip("no tuned table: the planner's choices apply")
-    with open(GRAD_TILES) as f:
+    with open(path) as f:
         table = json.load(f)
-    assert table["classes"], table
     for key, t in table["classes"].items():
         a, b = (int(x) for x in key.split(","))
-        assert 1 <= a <= 7 and 1 <= b <= 7
-        assert (t["tpq"], t["order"]) in CANDIDATES
+        assert lo <= a <= 7 and lo <= b <= 7
+        assert (t["tpq"], t["order"]) in cands
         assert t["ms"] < t["planner_ms"]
