@@ -209,7 +209,8 @@ double mg_drvg1_flops(mg_handle* h, double cutint);
  * mg_grad_set_tile: tpq = the first group size tried (128, 256, 512; 0 =
  * the planner's choice), order = the dimension the planner shrinks first
  * when the tile does not fit (0 ket primitives, 1 roots per wave, 2 bra
- * primitives).  Takes effect at the next gradient (re-plan).
+ * primitives; 3..5 the same with the tile starting from 32 x 16 primitive
+ * pairs instead of 16 x 8).  Takes effect at the next gradient (re-plan).
  * mg_grad_profile(h, 1): later gradients launch their classes one after
  * another on the caller's stream with an event pair around each;
  * mg_grad_class_times then returns the classes of the last one (key =

@@ -29,7 +29,9 @@ import torch
 from openmolcas_b200 import basis as B
 from openmolcas_b200.molgpu import ERI_TILES, GRAD_TILES, MolGpu, unique_quartets
 
-CANDIDATES = [(tpq, order) for tpq in (128, 256, 512) for order in (0, 1, 2)]
+# gradient: group size x shrink order (0 ket primitives, 1 roots per wave, 2 bra
+# primitives; 3..5 the same from the larger 32 x 16 tile caps)
+CANDIDATES = [(tpq, order) for tpq in (128, 256, 512) for order in range(6)]
 ERI_CANDIDATES = [(tpq, order) for tpq in (64, 128, 256, 512) for order in (0, 1)]
 CUTINT = 1e-12
 ERI_SAMPLE = 2_000_000  # the seeded quartet sample of the ERI throughput benchmark

@@ -677,13 +677,15 @@ int mg_rys_roots(mg_handle* H, int nrys, int64_t n, const double* T, double* x, 
 int mg_grad_set_tile(mg_handle* H, int nab1, int ncd1, int tpq, int order) {
   if (!H) return MG_ERR_ARG;
   Handle* h = &H->h;
+  // order + 3: the same shrink order with the larger tile caps (32 x 16)
   if (nab1 < 1 || nab1 > 7 || ncd1 < 1 || ncd1 > 7 || (tpq != 0 && tpq != 128 && tpq != 256 && tpq != 512) ||
-      order < 0 || order > 2) {
-    h->err = "mg_grad_set_tile: class 1..7 x 1..7, tpq 0/128/256/512, order 0..2";
+      order < 0 || order > 5) {
+    h->err = "mg_grad_set_tile: class 1..7 x 1..7, tpq 0/128/256/512, order 0..5";
     return MG_ERR_ARG;
   }
   h->grad_tpq[nab1 * 8 + ncd1] = tpq;
-  h->grad_order[nab1 * 8 + ncd1] = order;
+  h->grad_order[nab1 * 8 + ncd1] = order % 3;
+  h->grad_cap[nab1 * 8 + ncd1] = order / 3;
   if (h->grad) h->grad->cutint = -1;  // re-plan at the next gradient
   return 0;
 }

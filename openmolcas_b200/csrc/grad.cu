@@ -171,13 +171,21 @@ int grad_build(Handle* h, double cutint, GradPlan& plan) {
       const size_t cta = kCtaLimit / 8 - kGTabD;
       const int nthr = GradThreads<1>::value;
       const int order = h->grad_order[key];
+      const int cab = h->grad_cap[key] ? 32 : 16, ccd = h->grad_cap[key] ? 16 : 8;
       const int tpq0 = h->grad_tpq[key] ? h->grad_tpq[key] : (wmax <= 512 ? 128 : 256);
+      // a tile fits when its shared memory is within the group's share and every
+      // run-time loop extent x divisor of the kernel stays below 2^32
+      auto div_ok = [&](int a, int c, int rw) {
+        for (const GradItem& it : v)
+          if (grad_div_bound(h->pairs[it.p], h->pairs[it.q], it.i1 - it.i0, a, c, rw) >= 4294967296.0) return false;
+        return true;
+      };
       for (int tpq = tpq0; tpq <= nthr && !c.tpq; tpq *= 2) {
         const int groups = nthr / tpq;
         const size_t gb = (cta / groups) & ~(size_t)1;
-        int pab = std::max(1, std::min(m.npab, 16)), pcd = std::max(1, std::min(m.npcd, 8)), rw = NRc;
+        int pab = std::max(1, std::min(m.npab, cab)), pcd = std::max(1, std::min(m.npcd, ccd)), rw = NRc;
         size_t need = worst(pab, pcd, rw);
-        while (need > gb && (pab > 1 || pcd > 1 || rw > 1)) {
+        while ((need > gb || !div_ok(pab, pcd, rw)) && (pab > 1 || pcd > 1 || rw > 1)) {
           if (order == 1 && rw > 1) --rw;
           else if (order == 2 && pab > 1) pab = (pab + 1) / 2;
           else if (pcd > 1) pcd = (pcd + 1) / 2;

@@ -124,6 +124,7 @@ struct Handle {
   // (0 = the planner's) and the order in which the tile shrinks to fit
   int grad_tpq[64] = {};
   int grad_order[64] = {};
+  int grad_cap[64] = {};  // tile caps: 0 = 16 bra x 8 ket primitive pairs, 1 = 32 x 16
   // profiled gradients: classes one after another on the caller's stream, an
   // event pair around each (grad_ev[2k], grad_ev[2k + 1] for class key grad_ev_key[k])
   bool grad_profile = false;

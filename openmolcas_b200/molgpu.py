@@ -188,7 +188,8 @@ class MolGpu:
     def set_grad_tile(self, nab1: int, ncd1: int, tpq: int = 0, order: int = 0):
         """Tile choice of gradient class (la+lb+1, lc+ld+1): first group size
         tried (0 = the planner's) and the dimension shrunk first (0 ket
-        primitives, 1 roots per wave, 2 bra primitives)."""
+        primitives, 1 roots per wave, 2 bra primitives; 3..5 the same
+        starting from 32 x 16 primitive pairs instead of 16 x 8)."""
         self._check(self.L.mg_grad_set_tile(self.h, nab1, ncd1, tpq, order), "mg_grad_set_tile")
 
     def grad_profile(self, enable: bool = True):
