@@ -106,10 +106,14 @@ def rhf(jk: Callable[[torch.Tensor], tuple], h: torch.Tensor, S: torch.Tensor, n
 
 def uhf(jk: Callable[[torch.Tensor], tuple], h: torch.Tensor, S: torch.Tensor, nalpha: int, nbeta: int,
         enuc: float, C0: Optional[tuple] = None, e_conv: float = 1e-10, d_conv: float = 1e-8, maxiter: int = 200,
-        ndiis: int = 8, lindep: float = 1e-9) -> dict:
+        ndiis: int = 8, lindep: float = 1e-9, jk_batch: Optional[Callable[[list], list]] = None) -> dict:
     """Unrestricted SCF (the reference's ``UHF`` keyword of &SCF): separate
     alpha and beta orbitals, F_s = h + J[D_a + D_b] - K[D_s], two jk calls per
-    iteration, one DIIS over both spin commutators.
+    iteration, one DIIS over both spin commutators.  jk_batch, when given,
+    takes the list of occupied factors and returns their (J, K) in one call
+    (MolGpu.cho_jk_batch: one pass over the Cholesky vectors for both spins,
+    the two-density CHO_LK_SCF call of scf/choscf_drv.F90:433); jk is then
+    not called.
 
     E = 1/2 tr((D_a + D_b) h) + 1/2 tr(D_a F_a) + 1/2 tr(D_b F_b) + enuc; its
     two-electron part equals 1/2 tr(D J[D]) - 1/4 (tr(D K[D]) + tr(DS K[DS]))
@@ -142,17 +146,18 @@ def uhf(jk: Callable[[torch.Tensor], tuple], h: torch.Tensor, S: torch.Tensor, n
     e_old = None
     converged = False
     for it in range(1, maxiter + 1):
-        Ds, Ks = [], []
+        Ds, Ks = [], [torch.zeros_like(h), torch.zeros_like(h)]
         J = torch.zeros_like(h)
+        occ = []
         for s in range(2):
             Co = Cs[s][:, :nocc[s]]
             Ds.append(Co @ Co.T)
             if nocc[s] > 0:
-                Js, Kk = jk(Co)
-                J = J + Js.to(dev, dt)
-                Ks.append(Kk.to(dev, dt))
-            else:
-                Ks.append(torch.zeros_like(h))
+                occ.append((s, Co))
+        res = jk_batch([Co for _, Co in occ]) if jk_batch is not None else [jk(Co) for _, Co in occ]
+        for (s, _), (Js, Kk) in zip(occ, res):
+            J = J + Js.to(dev, dt)
+            Ks[s] = Kk.to(dev, dt)
         Fs = [h + J - Ks[s] for s in range(2)]
         E = float(0.5 * torch.sum((Ds[0] + Ds[1]) * h) + 0.5 * torch.sum(Ds[0] * Fs[0])
                   + 0.5 * torch.sum(Ds[1] * Fs[1])) + enuc

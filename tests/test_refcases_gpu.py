@@ -137,3 +137,41 @@ def test_symmetric_case_device_drvg1_with_d_shells_against_reference(symgrad):
     err = np.abs(G[z["grad_atom"], z["grad_comp"]] - z["GRAD"]).max()
     print(f"{mol.name} device: max |grad - GRAD| = {err:.1e}")
     assert err <= 10.0 ** -int(z["GRAD_digits"])
+
+
+def test_uhf_over_device_batched_jk_862(grad862):
+    """Open-shell UHF (the water cation of test 862's basis and geometry, 5
+    alpha and 4 beta electrons) over mg_cho_drv (ThrCom 1e-9) with both spins'
+    J and K from one mg_cho_jk_batch call per iteration: equal to the same
+    loop with two mg_cho_jk calls and to the loop over the oracle's vectors
+    (1e-8 Eh), within 1e-6 Eh of UHF over exact integrals (the decomposition
+    error), and the mixed-precision batch within 1e-8 Eh of the FP64 one."""
+    mol = grad862["mol"]
+    S, T, V = oneint.one_electron(mol)
+    enuc = oneint.nuclear_repulsion(mol)
+    h, Sm = torch.from_numpy(T + V), torch.from_numpy(S)
+    o = O.Oracle(mol)
+    kw = dict(e_conv=1e-12, d_conv=1e-10)
+    r0 = scf.uhf(exact_jk(o.eri_full()), h, Sm, 5, 4, enuc, **kw)
+    g = MolGpu(mol)
+    g.cho_drv(thrcom=1e-9)
+    dev = torch.device("cuda", g.device)
+    hd, Sd = h.to(dev), Sm.to(dev)
+    fp64 = MolGpu.PREC_FP64
+    r1 = scf.uhf(None, hd, Sd, 5, 4, enuc, jk_batch=lambda Cs: g.cho_jk_batch(Cs, precision=fp64), **kw)
+    r2 = scf.uhf(lambda Cf: g.cho_jk(Cf, precision=fp64), hd, Sd, 5, 4, enuc, **kw)
+    r3 = scf.uhf(None, hd, Sd, 5, 4, enuc, jk_batch=lambda Cs: g.cho_jk_batch(Cs, precision=MolGpu.PREC_MIXED), **kw)
+    L = o.cholesky(thrcom=1e-9)["L"]
+
+    def jk(Cf):
+        J, K = o.cho_jk(L, Cf.numpy())
+        return torch.from_numpy(J), torch.from_numpy(K)
+
+    r4 = scf.uhf(jk, h, Sm, 5, 4, enuc, **kw)
+    print(f"UHF 862 cation: exact {r0['energy']:.12f}, device batch {r1['energy']:.12f}, two calls "
+          f"{r2['energy']:.12f}, mixed batch {r3['energy']:.12f}, oracle vectors {r4['energy']:.12f}")
+    assert all(r["converged"] for r in (r0, r1, r2, r3, r4))
+    assert abs(r1["energy"] - r2["energy"]) < 1e-10
+    assert abs(r1["energy"] - r4["energy"]) < 1e-8
+    assert abs(r1["energy"] - r0["energy"]) < 1e-6
+    assert abs(r3["energy"] - r1["energy"]) < 1e-8
