@@ -37,9 +37,28 @@ CUTINT = 1e-12
 ERI_SAMPLE = 2_000_000  # the seeded quartet sample of the ERI throughput benchmark
 
 
+def pick(base, base_plan, runs, margin):
+    """Per-class choice: `base` maps a class to the planner's time, `runs`
+    maps each candidate to (times, plans) per class.  A class takes the
+    candidate with the shortest time when that beats the planner's by more
+    than `margin` (a fraction); the entry records the candidate, the tile it
+    produced and both times.  Classes a candidate did not time are skipped
+    for that candidate."""
+    classes = {}
+    for k, tb in sorted(base.items()):
+        timed = [(r[0][k], cand, r[1][k]) for cand, r in runs.items() if k in r[0]]
+        if not timed:
+            continue
+        tt, (tpq, order), plan = min(timed, key=lambda x: x[0])
+        if tt < (1.0 - margin) * tb:
+            classes[f"{k[0]},{k[1]}"] = {"tpq": tpq, "order": order, "tile": list(plan), "ms": round(tt, 3),
+                                         "planner_tile": list(base_plan[k]), "planner_ms": round(tb, 3)}
+    return classes
+
+
 def _class_times(g, D, reps):
     """Per-class minimum kernel milliseconds over `reps` profiled gradients
-    (after one unprofiled-timing warm-up that also re-plans)."""
+    (after one more profiled gradient that re-plans and warms up)."""
     g.drvg1(D, CUTINT)
     torch.cuda.synchronize()
     best = {}
@@ -88,13 +107,7 @@ def tune(cfg="c4", reps=2, margin=0.02, device=0, log=print):
         _set_all(g, tpq, order)
         runs[(tpq, order)] = _class_times(g, D, reps)
         log(f"tpq {tpq} order {order}: {sum(runs[(tpq, order)][0].values()):.1f} ms")
-    classes = {}
-    for k, tb in sorted(base.items()):
-        (tpq, order), (tt, plan) = min(((cand, (r[0][k], r[1][k])) for cand, r in runs.items()),
-                                       key=lambda x: x[1][0])
-        if tt < (1.0 - margin) * tb:
-            classes[f"{k[0]},{k[1]}"] = {"tpq": tpq, "order": order, "tile": list(plan), "ms": round(tt, 3),
-                                         "planner_tile": list(base_plan[k]), "planner_ms": round(tb, 3)}
+    classes = pick(base, base_plan, runs, margin)
     # check: the table against the planner, profiled and in the normal launch
     _set_all(g, 0, 0)
     for key, t in classes.items():
@@ -173,13 +186,7 @@ def tune_eri(cfg="c2", sample=400_000, reps=2, margin=0.02, device=0, log=print)
         _set_all_eri(g, tpq, order)
         runs[(tpq, order)] = _eri_batch(g, sel, out, reps)
         log(f"ERI tpq {tpq} order {order}: {sum(runs[(tpq, order)][0].values()):.1f} ms")
-    classes = {}
-    for k, tb in sorted(base.items()):
-        (tpq, order), (tt, plan) = min(((cand, (r[0][k], r[1][k])) for cand, r in runs.items()),
-                                       key=lambda x: x[1][0])
-        if tt < (1.0 - margin) * tb:
-            classes[f"{k[0]},{k[1]}"] = {"tpq": tpq, "order": order, "tile": list(plan), "ms": round(tt, 3),
-                                         "planner_tile": list(base_plan[k]), "planner_ms": round(tb, 3)}
+    classes = pick(base, base_plan, runs, margin)
     _set_all_eri(g, 0, 0)
     for key, t in classes.items():
         a, b = (int(x) for x in key.split(","))

@@ -89,3 +89,24 @@ def test_committed_tile_tables_are_valid(path, cands, lo):
         assert lo <= a <= 7 and lo <= b <= 7
         assert (t["tpq"], t["order"]) in cands
         assert t["ms"] < t["planner_ms"]
+
+
+def test_pick_keeps_only_clear_wins():
+    """The tuner's per-class choice on made-up timings: the fastest candidate
+    wins only when it beats the planner by more than the margin, and a class
+    one candidate did not time is judged on the others."""
+    from openmolcas_b200.autotune import pick
+    base = {(3, 3): 100.0, (4, 4): 50.0, (2, 2): 10.0}
+    plan = {(3, 3): (128, 8, 1, 3), (4, 4): (256, 4, 1, 4), (2, 2): (128, 16, 2, 2)}
+    runs = {
+        (256, 1): ({(3, 3): 90.0, (4, 4): 49.5, (2, 2): 11.0},
+                   {(3, 3): (256, 16, 2, 1), (4, 4): (256, 8, 1, 1), (2, 2): (256, 16, 4, 1)}),
+        (512, 0): ({(3, 3): 95.0, (2, 2): 9.0},
+                   {(3, 3): (512, 8, 2, 3), (2, 2): (512, 16, 8, 2)}),
+    }
+    got = pick(base, plan, runs, 0.02)
+    assert set(got) == {"3,3", "2,2"}  # (4,4): 1 % better only
+    assert got["3,3"]["tpq"] == 256 and got["3,3"]["order"] == 1 and got["3,3"]["tile"] == [256, 16, 2, 1]
+    assert got["3,3"]["ms"] == 90.0 and got["3,3"]["planner_ms"] == 100.0
+    assert got["2,2"]["tpq"] == 512 and got["2,2"]["planner_tile"] == [128, 16, 2, 2]
+    assert pick(base, plan, runs, 0.2) == {}
