@@ -223,7 +223,8 @@ int mg_grad_class_times(mg_handle* h, int* keys, double* ms, int maxn);
 int mg_grad_plan_info(mg_handle* h, int* keys, int* tpq, int* pab, int* pcd, int* rw, int maxn);
 /* The same for the ERI classes (nab, ncd) = (la+lb, lc+ld) of mg_eri_quartets
  * (and the Cholesky columns): tpq 0, 64, 128, 256 or 512; order 0 shrinks the
- * ket primitives of the tile first, 1 the bra primitives.  Effective from the
+ * ket primitives of the tile first, 1 the bra primitives (+ 2: the tile starts
+ * from 64 x 16 primitive pairs instead of 32 x 8).  Effective from the
  * next batch.  mg_eri_class_times reports the last profiled batch's classes
  * with their plan (group size, pab x pcd tile). */
 int mg_eri_set_tile(mg_handle* h, int nab, int ncd, int tpq, int order);

@@ -32,7 +32,8 @@ from openmolcas_b200.molgpu import ERI_TILES, GRAD_TILES, MolGpu, unique_quartet
 # gradient: group size x shrink order (0 ket primitives, 1 roots per wave, 2 bra
 # primitives; 3..5 the same from the larger 32 x 16 tile caps)
 CANDIDATES = [(tpq, order) for tpq in (128, 256, 512) for order in range(6)]
-ERI_CANDIDATES = [(tpq, order) for tpq in (64, 128, 256, 512) for order in (0, 1)]
+# ERIs: group size x order = shrink order (0 ket, 1 bra primitives) + 2 (64 x 16 tile caps)
+ERI_CANDIDATES = [(tpq, order) for tpq in (64, 128, 256, 512) for order in range(4)]
 CUTINT = 1e-12
 ERI_SAMPLE = 2_000_000  # the seeded quartet sample of the ERI throughput benchmark
 

@@ -718,8 +718,8 @@ int mg_eri_set_tile(mg_handle* H, int nab, int ncd, int tpq, int order) {
   if (!H) return MG_ERR_ARG;
   Handle* h = &H->h;
   if (nab < 0 || nab > 7 || ncd < 0 || ncd > 7 || (tpq != 0 && tpq != 64 && tpq != 128 && tpq != 256 && tpq != 512) ||
-      order < 0 || order > 1) {
-    h->err = "mg_eri_set_tile: class 0..7 x 0..7, tpq 0/64/128/256/512, order 0..1";
+      order < 0 || order > 3) {
+    h->err = "mg_eri_set_tile: class 0..7 x 0..7, tpq 0/64/128/256/512, order 0..3";
     return MG_ERR_ARG;
   }
   h->eri_tpq[nab * 8 + ncd] = tpq;

@@ -66,19 +66,29 @@ static size_t eri_group_smem(int nab, int ncd, const ClassStats& cs, int pab, in
 }
 
 // tpq0: the first group size tried (0: from the widest stage); order: the tile
-// dimension shrunk first when it does not fit (0 ket primitives, 1 bra)
+// dimension shrunk first when it does not fit (0 ket primitives, 1 bra; + 2:
+// the tile starts from 64 x 16 primitive pairs instead of 32 x 8)
 ClassPlan eri_plan(int nab, int ncd, const ClassStats& cs, int tpq0, int order) {
   const int NR = (nab + ncd) / 2 + 1;
   ClassPlan pl{0, 0, 0, 0, 0};
   const size_t budget = (227 * 1024) / 8 - kETabD;  // one CTA per SM
-  int pab = std::max(1, std::min(cs.max_npab, 32));
-  int pcd = std::max(1, std::min(cs.max_npcd, 8));
+  const bool big = order >= 2;
+  order %= 2;
+  int pab = std::max(1, std::min(cs.max_npab, big ? 64 : 32));
+  int pcd = std::max(1, std::min(cs.max_npcd, big ? 16 : 8));
   const int width = std::max({cs.max_acc, pab * pcd * cs.max_nef / 2, pab * pcd * NR * 3 * 8});
+  // the kernel's multiply-high divisions are exact below 2^32: largest loop
+  // extent x divisor of a tile a x c
+  auto bound = [&](int a, int c) {
+    const double nt = (double)a * c;
+    return std::max({nt * cs.max_nef * nt, (double)cs.max_nij * c * cs.max_nef * cs.max_nef,
+                     (double)cs.max_acc * cs.max_nef, (double)cs.max_tmp * cs.max_nf, (double)cs.max_tmp * cs.max_nc});
+  };
   for (int tpq = tpq0 ? tpq0 : width <= 96 ? 64 : width <= 384 ? 128 : 256; tpq <= kEriThreads; tpq *= 2) {
     const int groups = kEriThreads / tpq;
     const size_t gbudget = (budget / groups) & ~(size_t)1;
     int a = pab, c = pcd;
-    while (eri_group_smem(nab, ncd, cs, a, c) > gbudget && (a > 1 || c > 1)) {
+    while ((eri_group_smem(nab, ncd, cs, a, c) > gbudget || bound(a, c) >= 4294967296.0) && (a > 1 || c > 1)) {
       if (order == 1 && a > 1) a = (a + 1) / 2;
       else if (c > 1) c = (c + 1) / 2;
       else a = (a + 1) / 2;
@@ -89,12 +99,7 @@ ClassPlan eri_plan(int nab, int ncd, const ClassStats& cs, int tpq0, int order) 
       pl.PCD = c;
       pl.gsm = (int)eri_group_smem(nab, ncd, cs, a, c);
       pl.smem = 8 * ((size_t)pl.gsm * groups + kETabD);
-      // the kernel's multiply-high divisions are exact below 2^32
-      const double nt = (double)a * c;
-      const double bound = std::max({nt * cs.max_nef * nt, (double)cs.max_nij * c * cs.max_nef * cs.max_nef,
-                                     (double)cs.max_acc * cs.max_nef, (double)cs.max_tmp * cs.max_nf,
-                                     (double)cs.max_tmp * cs.max_nc});
-      if (bound >= 4294967296.0) pl.PAB = 0;
+      if (bound(a, c) >= 4294967296.0) pl.PAB = 0;
       return pl;
     }
   }

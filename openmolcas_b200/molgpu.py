@@ -207,7 +207,8 @@ class MolGpu:
 
     def set_eri_tile(self, nab: int, ncd: int, tpq: int = 0, order: int = 0):
         """Tile choice of ERI class (la+lb, lc+ld): first group size tried (0 =
-        the planner's) and the dimension shrunk first (0 ket, 1 bra primitives)."""
+        the planner's) and the dimension shrunk first (0 ket, 1 bra primitives;
+        + 2: starting from 64 x 16 primitive pairs instead of 32 x 8)."""
         self._check(self.L.mg_eri_set_tile(self.h, nab, ncd, tpq, order), "mg_eri_set_tile")
 
     def eri_profile(self, enable: bool = True):
